@@ -1,0 +1,66 @@
+"""In-tree build of the native libraries (sm_100a CUDA and host C++).
+
+    python -m gpu_cdt_refine_b200.build
+
+libgqm_b200.so : refine.cu (kernels, driver, C ABI) + legacy.cpp (C++ drop-in)
+libgqm_host.so : cdt_build.cpp + synth.cpp + certify.cpp
+
+Every floating-point operation of the refiner is rounded on its own:
+nvcc -fmad=false and gcc -ffp-contract=off, the same arithmetic as the
+reference built with -fmad=false.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+INC = os.path.join(os.path.dirname(HERE), "include")
+NVCC = os.environ.get("NVCC", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
+def _stale(out, srcs):
+    if not os.path.exists(out):
+        return True
+    t = os.path.getmtime(out)
+    return any(os.path.getmtime(s) > t for s in srcs)
+
+
+def build_host(force=False):
+    out = os.path.join(HERE, "libgqm_host.so")
+    srcs = [os.path.join(CSRC, f) for f in ("cdt_build.cpp", "synth.cpp", "certify.cpp")]
+    deps = srcs + [os.path.join(CSRC, "predicates.h")]
+    if force or _stale(out, deps):
+        _run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-ffp-contract=off", "-I" + INC, "-o", out] + srcs)
+    return out
+
+
+def build_cuda(force=False, extra=None):
+    out = os.path.join(HERE, "libgqm_b200.so")
+    srcs = [os.path.join(CSRC, "refine.cu"), os.path.join(CSRC, "legacy.cpp")]
+    deps = srcs + [os.path.join(CSRC, f) for f in ("kernels.cuh", "gqm_device.cuh", "predicates.h")] + [
+        os.path.join(INC, "gqm_refine.h"), os.path.join(INC, "gqm_triangulateio.h")]
+    if force or _stale(out, deps):
+        cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
+                               "-Xcompiler", "-ffp-contract=off", "-shared", "-I" + INC, "-o", out] + srcs
+        if extra:
+            cmd[1:1] = extra
+        _run(cmd)
+    return out
+
+
+def build(force=False):
+    build_host(force)
+    build_cuda(force)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)

@@ -1,0 +1,39 @@
+"""Exact certificate of a refined CDT (csrc/certify.cpp)."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _native
+from .cdtio import CDT
+
+
+class _Cert(ctypes.Structure):
+    _fields_ = [("not_ccw", ctypes.c_longlong), ("bad_neighbors", ctypes.c_longlong),
+                ("open_boundary", ctypes.c_longlong), ("non_delaunay", ctypes.c_longlong),
+                ("segments_missing", ctypes.c_longlong), ("input_points_moved", ctypes.c_longlong),
+                ("triangles_below_theta", ctypes.c_longlong), ("euler_defect", ctypes.c_longlong),
+                ("min_angle_deg", ctypes.c_double), ("theta", ctypes.c_double),
+                ("max_segment_deviation", ctypes.c_double)]
+
+
+def certify(out: CDT, inp: CDT, theta: float) -> dict:
+    """Check `out` (a refinement of `inp`) and return the certificate fields.
+
+    ``ok`` is True when the mesh is a valid constrained Delaunay triangulation
+    that preserves every input point and segment.  The angle fields report the
+    quality separately (``triangles_below_theta``, ``min_angle_deg``).
+    """
+    lib = _native.host()
+    dp, ip = ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)
+    lib.gqm_certify.argtypes = [ctypes.c_int, dp, ctypes.c_int, ip, ip, ctypes.c_int, ip, ctypes.c_int, dp,
+                                ctypes.c_int, ip, ctypes.c_double, ctypes.POINTER(_Cert)]
+    c = _Cert()
+    rc = lib.gqm_certify(out.numberofpoints, _native.dptr(out.pointlist), out.numberoftriangles,
+                         _native.iptr(out.trianglelist), _native.iptr(out.neighborlist), out.numberofsegments,
+                         _native.iptr(out.segmentlist), inp.numberofpoints, _native.dptr(inp.pointlist),
+                         inp.numberofsegments, _native.iptr(inp.segmentlist), float(theta), ctypes.byref(c))
+    d = {k: getattr(c, k) for k, _ in _Cert._fields_}
+    d["ok"] = rc == 0
+    return d

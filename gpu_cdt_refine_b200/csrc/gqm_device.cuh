@@ -1,0 +1,125 @@
+// Device-side mesh layout and per-element helpers of the B200 refiner.
+//
+// Layout (structure of arrays, resident in HBM for the whole refinement):
+//   pts   double2[Pcap]   vertex coordinates (one 128-bit load each)
+//   ps    uint8[Pcap]     point flags: DELETED | STEINER | SEGSPLIT | NEW
+//   pred  uint8[Pcap]     "redundant" flag (set concurrently by many threads)
+//   tv    int4[Tcap]      triangle vertices (x, y, z), w unused
+//   tn    int4[Tcap]      oriented neighbours (tri << 2 | edge), -1 boundary
+//   tsg   int4[Tcap]      subsegment on each edge, -1 if none
+//   tst   uint8[Tcap]     NOTNULL | BAD | CHECK
+//   tflip uint8[Tcap]     flip-flop marker (set concurrently)
+//   tfo   uint8[Tcap]     flip orientation code, 15 = none
+//   tmark int[Tcap]       ownership marker (atomicMin) / flipBy
+//   s2t   uint64[Scap]    subsegment -> oriented triangle, tagged with the
+//                         launch epoch in the high word (see s2t_store)
+//   s2seg int[Scap], enc int[Scap], segs int2[S_in]
+// Edge i of a triangle joins vertices i+1 and i+2 and faces vertex i; an
+// oriented triangle (t << 2 | i) names edge i of t (GPU_Refine/refine.cu:95-113).
+// Flags the reference keeps in one byte (GPU_Refine/refine.h:36-205) are split
+// across separate byte arrays so that concurrent writers never share a byte.
+#pragma once
+#include <cstdint>
+
+#include "predicates.h"
+
+namespace gqm {
+
+constexpr int kMaxInt = 2147483647;
+constexpr int kCavityCap = 50;  // MyList capacity, GPU_Refine/refine.h:30
+
+enum : uint8_t { PS_DELETED = 1, PS_STEINER = 2, PS_SEGSPLIT = 4, PS_NEW = 8 };
+enum : uint8_t { TS_NOTNULL = 1, TS_BAD = 2, TS_CHECK = 4 };
+
+struct Mesh {
+  double2 *pts;
+  uint8_t *ps, *pred;
+  int4 *tv, *tn, *tsg;
+  uint8_t *tst, *tflip, *tfo, *flip0;
+  int *tmark;
+  int *tpos;  // winner-slot of each triangle during a flip step
+  unsigned long long *s2t;
+  int *s2seg, *enc;
+  const int2 *segs;
+  int *err;  // first error code raised on the device
+  double gc2;  // cos^2(theta), computed on the device as the reference does
+  int mode;    // 1 Ruppert, 0 Chew
+};
+
+__device__ __forceinline__ int dtri(int o) { return o >= 0 ? (o >> 2) : -1; }
+__device__ __forceinline__ int dori(int o) { return o & 3; }
+__device__ __forceinline__ int etri(int t, int o) { return t >= 0 ? ((t << 2) | o) : -1; }
+__device__ __forceinline__ int negate_idx(int i) { return -i - 3; }
+__device__ __forceinline__ int m3(int i) { return i >= 3 ? i - 3 : i; }
+
+__device__ __forceinline__ int comp(const int4 &v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+__device__ __forceinline__ void setc(int4 &v, int i, int x) {
+  if (i == 0)
+    v.x = x;
+  else if (i == 1)
+    v.y = x;
+  else
+    v.z = x;
+}
+// single-component stores into an int4 row
+__device__ __forceinline__ void st1(int4 *a, int t, int i, int x) { reinterpret_cast<int *>(a + t)[i] = x; }
+__device__ __forceinline__ int ld1(const int4 *a, int t, int i) { return reinterpret_cast<const int *>(a + t)[i]; }
+
+__device__ __forceinline__ int s2t_get(const Mesh &M, int s) { return (int)(uint32_t)M.s2t[s]; }
+// Rule for concurrent writers of one subsegment's entry within a launch: the
+// largest oriented triangle wins; a value from an earlier launch always loses.
+__device__ __forceinline__ void s2t_store(const Mesh &M, int s, int v, uint32_t epoch) {
+  atomicMax(M.s2t + s, ((unsigned long long)epoch << 32) | (uint32_t)v);
+}
+
+__device__ __forceinline__ void raise_err(const Mesh &M, int code) { atomicCAS(M.err, 0, code); }
+
+// ---------------------------------------------------------------------------
+// Predicates with the reference's effective arithmetic (PRED = 0) or exact
+// (PRED = 1).  Orientation: cuda_fast / cuda_ccw.  Incircle: the
+// "cuda_inCircle, then cuda_inCircle_exact if 0" pattern used by every caller.
+// ---------------------------------------------------------------------------
+template <int PRED>
+__device__ __forceinline__ double orient(double2 a, double2 b, double2 c) {
+  if (PRED == 0) return gqm_orient_ref(a.x, a.y, b.x, b.y, c.x, c.y);
+  return gqm_orient_exact(a.x, a.y, b.x, b.y, c.x, c.y);
+}
+template <int PRED>
+__device__ __noinline__ double incircle_slow(double2 a, double2 b, double2 c, double2 d) {
+  if (PRED == 0) return gqm_incircle_zero_fallback_ref(a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y);
+  return gqm_incircle_exact(a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y);
+}
+template <int PRED>
+__device__ __forceinline__ double incircle(double2 a, double2 b, double2 c, double2 d) {
+  if (PRED == 0) {
+    double r = gqm_incircle_det_ref(a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y);
+    if (r != 0) return r;
+    return incircle_slow<0>(a, b, c, d);
+  }
+  // exact: filter then exact expansion
+  double adx = a.x - d.x, bdx = b.x - d.x, cdx = c.x - d.x;
+  double ady = a.y - d.y, bdy = b.y - d.y, cdy = c.y - d.y;
+  double bdxcdy = bdx * cdy, cdxbdy = cdx * bdy, alift = adx * adx + ady * ady;
+  double cdxady = cdx * ady, adxcdy = adx * cdy, blift = bdx * bdx + bdy * bdy;
+  double adxbdy = adx * bdy, bdxady = bdx * ady, clift = cdx * cdx + cdy * cdy;
+  double det = alift * (bdxcdy - cdxbdy) + blift * (cdxady - adxcdy) + clift * (adxbdy - bdxady);
+  double perm = (fabs(bdxcdy) + fabs(cdxbdy)) * alift + (fabs(cdxady) + fabs(adxcdy)) * blift +
+                (fabs(adxbdy) + fabs(bdxady)) * clift;
+  double eb = (10.0 + 96.0 * GQM_EPS) * GQM_EPS * perm;
+  if (det > eb || -det > eb) return det;
+  return incircle_slow<1>(a, b, c, d);
+}
+
+// checkseg4encroach, GPU_Refine/refine.cu:115-139 (goodcoss squared once).
+__device__ __forceinline__ bool encroached(double2 o, double2 d, double2 a, double gc2, int mode) {
+  double dot = (o.x - a.x) * (d.x - a.x) + (o.y - a.y) * (d.y - a.y);
+  if (dot < 0.0) {
+    if (mode || dot * dot >= (2.0 * gc2 - 1.0) * (2.0 * gc2 - 1.0) *
+                                   ((o.x - a.x) * (o.x - a.x) + (o.y - a.y) * (o.y - a.y)) *
+                                   ((d.x - a.x) * (d.x - a.x) + (d.y - a.y) * (d.y - a.y)))
+      return true;
+  }
+  return false;
+}
+
+}  // namespace gqm

@@ -1,0 +1,853 @@
+// Host driver of the B200 refiner and the C ABI of include/gqm_refine.h.
+//
+// The driver reproduces the control flow of GPU_Refine_Quality
+// (GPU_Refine/refine.cu:6500-7139): split encroached subsegments, then rounds
+// of {mark bad triangles, split them, split encroached subsegments} until no
+// bad triangle remains, then compact.  The reference's host bookkeeping of
+// free slots (refine.cu:149-197, 3408-3444, 3545-3562, 5259-5296, 5354-5368)
+// is reproduced exactly, because the slot a new point or triangle receives
+// decides later conflicts.  Physical device buffers are allocated once, larger
+// than the reference's logical capacity, and the logical capacity is tracked
+// separately.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/gqm_refine.h"
+#include "kernels.cuh"
+
+namespace gqm {
+
+// ============================================================================
+// Ordered stream compaction: out[k] = map(i) for the k-th i in [lo, hi) with
+// pred(i), in ascending i.  Three launches: per-block counts, one-block scan,
+// per-block ordered emit (warp ballots).  No spin waits.
+// ============================================================================
+constexpr int kCompactThreads = 256;
+constexpr int kMaxCompactBlocks = 2048;
+
+template <class F>
+__global__ void k_cnt(F f, int lo, int hi, int chunk, int *bc) {
+  int b0 = lo + blockIdx.x * chunk, b1 = min(hi, b0 + chunk);
+  int c = 0;
+  for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) c += f(i) ? 1 : 0;
+  __shared__ int red[32];
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) bc[blockIdx.x] = v;
+  }
+}
+// exclusive scan of bc[0..nb) in place (one block of 1024 threads); total at *total
+__global__ void k_scan(int *bc, int nb, int *total) {
+  __shared__ int sh[1024];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nb; base += 1024) {
+    int i = base + threadIdx.x;
+    int v = (i < nb) ? bc[i] : 0;
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = 1; o < 1024; o <<= 1) {
+      int t = (threadIdx.x >= o) ? sh[threadIdx.x - o] : 0;
+      __syncthreads();
+      sh[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < nb) bc[i] = carry + sh[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += sh[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+template <class F, class Mp>
+__global__ void k_emit(F f, Mp m, int lo, int hi, int chunk, const int *bc, int *out) {
+  __shared__ int wsum[32];
+  __shared__ int base;
+  int b0 = lo + blockIdx.x * chunk, b1 = min(hi, b0 + chunk);
+  if (threadIdx.x == 0) base = bc[blockIdx.x];
+  __syncthreads();
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int s = b0; s < b1; s += blockDim.x) {
+    int i = s + threadIdx.x;
+    bool p = (i < b1) && f(i);
+    unsigned bal = __ballot_sync(0xffffffffu, p);
+    if (lane == 0) wsum[warp] = __popc(bal);
+    __syncthreads();
+    int off = 0, tot = 0;
+    for (int w = 0; w < nw; ++w) {
+      int c = wsum[w];
+      if (w < warp) off += c;
+      tot += c;
+    }
+    if (p) out[base + off + __popc(bal & ((1u << lane) - 1))] = m(i);
+    __syncthreads();
+    if (threadIdx.x == 0) base += tot;
+    __syncthreads();
+  }
+}
+
+// predicates and maps for the compactions
+struct Ident {
+  __device__ int operator()(int i) const { return i; }
+};
+struct ValueOf {
+  const int *a;
+  __device__ int operator()(int i) const { return a[i]; }
+};
+struct PNotNullFlag {
+  const uint8_t *tst, *flag;
+  __device__ bool operator()(int i) const { return (tst[i] & TS_NOTNULL) && flag[i]; }
+};
+struct PWinner {
+  const uint8_t *tst, *tfo;
+  __device__ bool operator()(int i) const { return (tst[i] & TS_NOTNULL) && tfo[i] != 15; }
+};
+struct PNeg {
+  const int *a;
+  __device__ bool operator()(int i) const { return a[i] < 0; }
+};
+struct PNonNeg {
+  const int *a;
+  __device__ bool operator()(int i) const { return a[i] >= 0; }
+};
+struct PBad {
+  const uint8_t *tst;
+  __device__ bool operator()(int i) const { return (tst[i] & (TS_NOTNULL | TS_BAD)) == (TS_NOTNULL | TS_BAD); }
+};
+struct PTriNull {
+  const uint8_t *tst;
+  __device__ bool operator()(int i) const { return !(tst[i] & TS_NOTNULL); }
+};
+struct PTriLive {
+  const uint8_t *tst;
+  __device__ bool operator()(int i) const { return (tst[i] & TS_NOTNULL) != 0; }
+};
+struct PPtDeleted {
+  const uint8_t *ps;
+  __device__ bool operator()(int i) const { return (ps[i] & PS_DELETED) != 0; }
+};
+struct PPtLive {
+  const uint8_t *ps;
+  __device__ bool operator()(int i) const { return !(ps[i] & PS_DELETED); }
+};
+
+__global__ void k_fill(int *a, int n, int v) { GS_LOOP(i, n) a[i] = v; }
+__global__ void k_copy(int *dst, const int *src, const int *dn) {
+  int n = *dn;
+  GS_LOOP(i, n) dst[i] = src[i];
+}
+__global__ void k_set_count(int *dst, int v) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *dst = v;
+}
+
+// ============================================================================
+// Refiner
+// ============================================================================
+struct Refiner {
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  int device = 0;
+  Mesh M{};
+  // physical capacities
+  long pphys = 0, tphys = 0, sphys = 0;
+  // reference logical state
+  long pcap = 0, tcap = 0;
+  int last_point = 0, last_triangle = 0, last_subseg = 0, nseg_in = 0;
+  int pointblock = 0, triblock = 0, nempty_p = 0, nempty_t = 0, lenp = 0, lent = 0;
+  uint32_t epoch = 1;
+  // per-triangle scratch (capacity tphys)
+  int *emptyt = nullptr, *bad = nullptr, *imark = nullptr, *ilist = nullptr, *sinks = nullptr, *wl = nullptr;
+  int *act = nullptr, *win = nullptr, *neg = nullptr, *ll = nullptr, *sl = nullptr, *newidx = nullptr;
+  int *tail = nullptr;
+  double2 *center = nullptr;
+  // per-point scratch (capacity pphys)
+  int *emptyp = nullptr, *pnew = nullptr;
+  // per-subsegment scratch (capacity sphys)
+  int *enclist = nullptr, *encl2 = nullptr, *smark = nullptr, *mids = nullptr, *snap = nullptr;
+  int2 *segs = nullptr;
+  // counters and small buffers
+  int *dcount = nullptr;  // [16] list sizes on the device
+  int *hcount = nullptr;  // pinned mirror
+  int *bc = nullptr;      // compaction block counts
+  unsigned long long *dctr = nullptr;  // [4] event counters
+  double *dgc = nullptr;
+  int *dinput = nullptr;  // staging for host inputs
+  size_t dinput_bytes = 0;
+  // options
+  int pred_mode = 0, mode = 1, offcenter = 1, offconstant = 0;
+  double theta = 20.0;
+  long long max_rounds = 1000000;
+  gqm_stats stats{};
+  int status = 0;
+  // result sizes
+  int out_np = 0, out_nt = 0, out_ns = 0;
+  bool have_result = false;
+
+  enum { C_LIST0 = 0, C_LIST1, C_LIST2, C_LIST3, C_LIST4, C_LIST5, C_MISC };
+
+  ~Refiner() { release(); }
+
+  template <class T>
+  static cudaError_t dalloc(T **p, size_t n) {
+    *p = nullptr;
+    return cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(n, 1));
+  }
+  // grow a device array to n elements, keeping its first `keep` elements
+  template <class T>
+  cudaError_t regrow(T **p, size_t keep, size_t n) {
+    T *q = nullptr;
+    cudaError_t e = dalloc(&q, n);
+    if (e != cudaSuccess) return e;
+    if (*p && keep) cudaMemcpyAsync(q, *p, sizeof(T) * keep, cudaMemcpyDeviceToDevice, st);
+    if (*p) {
+      cudaStreamSynchronize(st);
+      cudaFree(*p);
+    }
+    *p = q;
+    return cudaSuccess;
+  }
+
+  void release() {
+    void *ptrs[] = {M.pts, M.ps, M.pred, M.tv, M.tn, M.tsg, M.tst, M.tflip, M.tfo, M.flip0, M.tmark, M.tpos,
+                    M.s2t, M.s2seg, M.enc, M.err, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
+                    newidx, tail, center, emptyp, pnew, enclist, encl2, smark, mids, snap, segs, dcount, bc,
+                    dctr, dgc, dinput};
+    for (void *p : ptrs)
+      if (p) cudaFree(p);
+    if (hcount) cudaFreeHost(hcount);
+    hcount = nullptr;
+    M = Mesh{};
+    emptyt = bad = imark = ilist = sinks = wl = act = win = neg = ll = sl = newidx = tail = nullptr;
+    center = nullptr;
+    emptyp = pnew = enclist = encl2 = smark = mids = snap = nullptr;
+    segs = nullptr;
+    dcount = bc = nullptr;
+    dctr = nullptr;
+    dgc = nullptr;
+    dinput = nullptr;
+    dinput_bytes = 0;
+    pphys = tphys = sphys = 0;
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    ev0 = ev1 = nullptr;
+    if (st) cudaStreamDestroy(st);
+    st = nullptr;
+  }
+
+  int setup(int dev) {
+    device = dev;
+    if (cudaSetDevice(dev) != cudaSuccess) return GQM_ERR_NO_DEVICE;
+    if (!st && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return GQM_ERR_CUDA;
+    if (!ev0) cudaEventCreate(&ev0);
+    if (!ev1) cudaEventCreate(&ev1);
+    if (!dcount) {
+      if (dalloc(&dcount, 16) || dalloc(&bc, kMaxCompactBlocks + 1) || dalloc(&dctr, 4) || dalloc(&dgc, 2) ||
+          dalloc(&M.err, 1))
+        return GQM_ERR_MEMORY;
+      if (cudaMallocHost((void **)&hcount, sizeof(int) * 16) != cudaSuccess) return GQM_ERR_MEMORY;
+    }
+    return GQM_OK;
+  }
+
+  static int grid_for(long n, int threads = 256) {
+    long g = (n + threads - 1) / threads;
+    if (g < 1) g = 1;
+    if (g > 148L * 64) g = 148L * 64;
+    return (int)g;
+  }
+#define LAUNCH(kernel, n, ...)                                              \
+  do {                                                                      \
+    kernel<<<grid_for(n), 256, 0, st>>>(__VA_ARGS__);                       \
+    stats.kernel_launches++;                                                \
+  } while (0)
+
+  // Ordered compaction over [lo, hi) into out; the count lands in dcount[slot].
+  template <class F, class Mp>
+  void compact(F f, Mp m, int lo, int hi, int *out, int slot) {
+    int n = hi - lo;
+    if (n <= 0) {
+      k_set_count<<<1, 32, 0, st>>>(dcount + slot, 0);
+      stats.kernel_launches++;
+      return;
+    }
+    int chunk = std::max(4 * kCompactThreads, (n + kMaxCompactBlocks - 1) / kMaxCompactBlocks);
+    chunk = (chunk + kCompactThreads - 1) / kCompactThreads * kCompactThreads;
+    int nb = (n + chunk - 1) / chunk;
+    k_cnt<<<nb, kCompactThreads, 0, st>>>(f, lo, hi, chunk, bc);
+    k_scan<<<1, 1024, 0, st>>>(bc, nb, dcount + slot);
+    k_emit<<<nb, kCompactThreads, 0, st>>>(f, m, lo, hi, chunk, bc, out);
+    stats.kernel_launches += 3;
+  }
+  int fetch(int slot) {
+    cudaMemcpyAsync(hcount + slot, dcount + slot, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    stats.host_syncs++;
+    return hcount[slot];
+  }
+  int check_device_error() {
+    int e = 0;
+    cudaMemcpyAsync(hcount + C_MISC, M.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaError_t ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) return GQM_ERR_CUDA;
+    e = hcount[C_MISC];
+    return e;
+  }
+
+  // ---- capacity management ----
+  int alloc_points(long n) {
+    long old = pphys;
+    if (n <= old) return GQM_OK;
+    if (regrow(&M.pts, old, n) || regrow(&M.ps, old, n) || regrow(&M.pred, old, n) || regrow(&emptyp, 0, n) ||
+        regrow(&pnew, old, n))
+      return GQM_ERR_MEMORY;
+    // new slots are deleted points
+    if (n > old) {
+      cudaMemsetAsync(M.ps + old, PS_DELETED, n - old, st);
+      cudaMemsetAsync(M.pred + old, 0, n - old, st);
+      cudaMemsetAsync(M.pts + old, 0, sizeof(double2) * (n - old), st);
+    }
+    pphys = n;
+    return GQM_OK;
+  }
+  int alloc_tris(long n) {
+    long old = tphys;
+    if (n <= old) return GQM_OK;
+    if (regrow(&M.tv, old, n) || regrow(&M.tn, old, n) || regrow(&M.tsg, old, n) || regrow(&M.tst, old, n) ||
+        regrow(&M.tflip, old, n) || regrow(&M.tfo, old, n) || regrow(&M.flip0, old, n) ||
+        regrow(&M.tmark, old, n) || regrow(&M.tpos, old, n) || regrow(&emptyt, 0, n) || regrow(&bad, old, n) ||
+        regrow(&imark, old, n) || regrow(&ilist, old, n) || regrow(&sinks, old, n) || regrow(&wl, old, n) ||
+        regrow(&act, old, n) || regrow(&win, old, n) || regrow(&neg, old, n) || regrow(&ll, 2 * old, 2 * n) ||
+        regrow(&sl, 6 * old, 6 * n) || regrow(&newidx, 0, n) || regrow(&tail, 0, n) || regrow(&center, old, n))
+      return GQM_ERR_MEMORY;
+    if (n > old) {
+      cudaMemsetAsync(M.tst + old, 0, n - old, st);
+      cudaMemsetAsync(M.tflip + old, 0, n - old, st);
+      cudaMemsetAsync(M.tfo + old, 0, n - old, st);
+      cudaMemsetAsync(M.tsg + old, 0xff, sizeof(int4) * (n - old), st);
+      cudaMemsetAsync(M.tpos + old, 0xff, sizeof(int) * (n - old), st);
+    }
+    tphys = n;
+    return GQM_OK;
+  }
+  int alloc_subsegs(long n) {
+    long old = sphys;
+    if (n <= old) return GQM_OK;
+    if (regrow(&M.s2t, old, n) || regrow(&M.s2seg, old, n) || regrow(&M.enc, old, n) || regrow(&enclist, old, n) ||
+        regrow(&encl2, old, n) || regrow(&smark, old, n) || regrow(&mids, old, n) || regrow(&snap, old, n))
+      return GQM_ERR_MEMORY;
+    // new subsegment entries start at epoch 0 so that the first tagged store wins
+    cudaMemsetAsync(M.s2t + old, 0, sizeof(unsigned long long) * (n - old), st);
+    sphys = n;
+    return GQM_OK;
+  }
+
+  // updateEmptyPoints / updateEmptyTriangles (refine.cu:149-197)
+  int refresh_points() {
+    compact(PPtDeleted{M.ps}, Ident{}, 0, (int)pcap, emptyp, C_MISC);
+    lenp = fetch(C_MISC);
+    return lenp;
+  }
+  int refresh_tris() {
+    compact(PTriNull{M.tst}, Ident{}, 0, (int)tcap, emptyt, C_MISC);
+    lent = fetch(C_MISC);
+    return lent;
+  }
+  // growth steps of refine.cu:3408-3444 / 5259-5296
+  int ensure_slots(int npts, int ntris) {
+    if (npts > nempty_p) {
+      nempty_p = refresh_points();
+      long num = 0;
+      while (npts > nempty_p + num * pointblock) num++;
+      if (num) {
+        long ncap = pcap + num * pointblock;
+        if (ncap > pphys) {
+          int rc = alloc_points(std::max(ncap, pphys + pphys / 2));
+          if (rc) return rc;
+        }
+        pcap = ncap;
+        nempty_p = refresh_points();
+      }
+    }
+    if (ntris > nempty_t) {
+      nempty_t = refresh_tris();
+      long num = 0;
+      while (ntris > nempty_t + num * triblock) num++;
+      if (num) {
+        long ncap = tcap + num * triblock;
+        if (ncap > tphys) {
+          int rc = alloc_tris(std::max(ncap, tphys + tphys / 2));
+          if (rc) return rc;
+        }
+        tcap = ncap;
+        nempty_t = refresh_tris();
+      }
+    }
+    return GQM_OK;
+  }
+  // slot bookkeeping after an insertion batch (refine.cu:3545-3559, 5354-5368)
+  void consume_slots(int npts, int ntris) {
+    int slot_after = (int)(pcap - last_point);
+    int slot_before = nempty_p - slot_after;
+    if (slot_before < npts) last_point += npts - slot_before;
+    nempty_p -= npts;
+    slot_after = (int)(tcap - last_triangle);
+    slot_before = nempty_t - slot_after;
+    if (slot_before < ntris) last_triangle += ntris - slot_before;
+    nempty_t -= ntris;
+  }
+  const int *pslots() const { return emptyp + (lenp - nempty_p); }
+  const int *tslots() const { return emptyt + (lent - nempty_t); }
+
+  // ---- flip-flop (refine.cu:2328-2490) ----
+  int flip_flop(int ntri) {
+    long long steps = 0;
+    for (;;) {
+      compact(PNotNullFlag{M.tst, M.tflip}, Ident{}, 0, ntri, act, C_LIST3);
+      int nact = fetch(C_LIST3);
+      if (nact == 0) break;
+      if (++steps > 64 * max_rounds) return GQM_ERR_ROUND_LIMIT;
+      stats.flip_steps++;
+      LAUNCH(k_flip_init, ntri, M, ntri);
+      if (pred_mode)
+        LAUNCH(k_check_flip<1>, nact, M, act, dcount + C_LIST3);
+      else
+        LAUNCH(k_check_flip<0>, nact, M, act, dcount + C_LIST3);
+      LAUNCH(k_flip_winner, nact, M, act, dcount + C_LIST3);
+      compact(PWinner{M.tst, M.tfo}, Ident{}, 0, ntri, win, C_LIST4);
+      int bound = nact;  // winners are active triangles
+      LAUNCH(k_init_link, bound, M, win, dcount + C_LIST4, ll);
+      uint32_t ep = ++epoch;
+      LAUNCH(k_phase1, bound, M, win, dcount + C_LIST4, sl, ep);
+      LAUNCH(k_phase2, bound, M, win, dcount + C_LIST4, ll, sl);
+      LAUNCH(k_phase3, bound, M, win, dcount + C_LIST4, sl);
+      compact(PNeg{M.tmark}, Ident{}, 0, ntri, neg, C_LIST5);
+      LAUNCH(k_mark_red_steiner, 2 * nact, M, neg, dcount + C_LIST5);
+    }
+    return GQM_OK;
+  }
+
+  // ---- splitEncsegs (refine.cu:3180-3778) ----
+  int split_encsegs() {
+    long long outer = 0;
+    for (;;) {
+      compact(PNonNeg{M.enc}, Ident{}, 0, last_subseg, enclist, C_LIST0);
+      int nenc = fetch(C_LIST0);
+      if (nenc == 0) break;
+      if (++outer > max_rounds) return GQM_ERR_ROUND_LIMIT;
+      // delete free Steiner points inside diametral circles
+      LAUNCH(k_copy, nenc, smark, enclist, dcount + C_LIST0);
+      int nmark = nenc;
+      long long inner = 0;
+      for (;;) {
+        compact(PNonNeg{smark}, ValueOf{smark}, 0, nmark, mids, C_LIST1);
+        int ndel = fetch(C_LIST1);
+        if (ndel == 0) break;
+        if (++inner > max_rounds) return GQM_ERR_ROUND_LIMIT;
+        nmark = ndel;
+        LAUNCH(k_mark_redundant, ndel, M, smark, mids, dcount + C_LIST1);
+        int rc = flip_flop(last_triangle);
+        if (rc) return rc;
+      }
+      int rc = ensure_slots(nenc, 2 * nenc);
+      if (rc) return rc;
+      if (last_subseg + nenc > sphys) {
+        rc = alloc_subsegs(std::max<long>(last_subseg + nenc, sphys + sphys / 2));
+        if (rc) return rc;
+      }
+      LAUNCH(k_fill, nenc, M.enc + last_subseg, nenc, -1);
+      LAUNCH(k_copy, nenc, smark, enclist, dcount + C_LIST0);
+      long long mid_iter = 0;
+      for (;;) {
+        compact(PNonNeg{smark}, Ident{}, 0, nenc, mids, C_LIST1);
+        int nmid = fetch(C_LIST1);
+        if (nmid == 0) break;
+        if (++mid_iter > 64 * max_rounds) return GQM_ERR_ROUND_LIMIT;
+        LAUNCH(k_reset_mid, nmid, M, mids, dcount + C_LIST1, smark);
+        LAUNCH(k_mark_mid, nmid, M, mids, dcount + C_LIST1, smark);
+        LAUNCH(k_mid_snapshot, nmid, M, mids, dcount + C_LIST1, smark, snap);
+        uint32_t ep = ++epoch;
+        LAUNCH(k_insert_mid, nmid, M, mids, dcount + C_LIST1, smark, snap, pslots(), tslots(), last_subseg, ep,
+               dctr + 1);
+        LAUNCH(k_update_mid_nbrs, nmid, M, mids, dcount + C_LIST1, smark, enclist);
+      }
+      consume_slots(nenc, 2 * nenc);
+      last_subseg += nenc;
+      rc = flip_flop(last_triangle);
+      if (rc) return rc;
+    }
+    return GQM_OK;
+  }
+
+  // ---- splitTriangles (refine.cu:5107-5547) ----
+  int split_triangles(int nbad) {
+    int *dn = dcount + C_LIST2;  // number of bad triangles
+    LAUNCH(k_copy, nbad, imark, bad, dn);
+    LAUNCH(k_copy, nbad, ilist, bad, dn);
+    LAUNCH(k_circumcenter, nbad, M, bad, dn, (double)offconstant, offcenter, center);
+    LAUNCH(k_fill, last_triangle, M.tmark, last_triangle, kMaxInt);
+    if (pred_mode)
+      LAUNCH(k_locate<1>, nbad, M, bad, dn, center, sinks);
+    else
+      LAUNCH(k_locate<0>, nbad, M, bad, dn, center, sinks);
+    LAUNCH(k_remove_losers, nbad, M, bad, dn, sinks, imark);
+    LAUNCH(k_fill, last_triangle, M.tmark, last_triangle, kMaxInt);
+    if (pred_mode) {
+      LAUNCH(k_cavity_mark<1>, nbad, M, dn, sinks, center, imark, ilist);
+      LAUNCH(k_cavity_check<1>, nbad, M, dn, sinks, center, imark, ilist);
+    } else {
+      LAUNCH(k_cavity_mark<0>, nbad, M, dn, sinks, center, imark, ilist);
+      LAUNCH(k_cavity_check<0>, nbad, M, dn, sinks, center, imark, ilist);
+    }
+    compact(PNonNeg{imark}, Ident{}, 0, nbad, wl, C_LIST1);
+    int nst = fetch(C_LIST1);
+    int *dw = dcount + C_LIST1;
+    LAUNCH(k_fill, last_subseg, encl2, last_subseg, -1);
+    LAUNCH(k_mark_onsegs, nst, M, wl, dw, sinks, encl2);
+    int rc = ensure_slots(nst, 2 * nst);
+    if (rc) return rc;
+    LAUNCH(k_reset_steiner, nst, M, wl, dw, sinks);
+    uint32_t ep = ++epoch;
+    LAUNCH(k_insert_steiner, nst, M, wl, dw, sinks, center, pslots(), tslots(), ep, dctr + 0);
+    LAUNCH(k_update_steiner_nbrs, nst, M, wl, dw, sinks);
+    consume_slots(nst, 2 * nst);
+    rc = flip_flop(last_triangle);
+    if (rc) return rc;
+    LAUNCH(k_onsegs_to_enc, last_subseg, M, encl2, last_subseg);
+    return GQM_OK;
+  }
+
+  // ---- output compaction (refine.cu:5758-6428) ----
+  int compact_output() {
+    // triangles
+    compact(PTriLive{M.tst}, Ident{}, 0, last_triangle, tail, C_MISC);
+    int newn = fetch(C_MISC);
+    LAUNCH(k_newidx_init, last_triangle, M, newidx, last_triangle, newn, M.tst, (uint8_t)TS_NOTNULL, false);
+    if (newn < last_triangle) {
+      compact(PTriNull{M.tst}, Ident{}, 0, newn, emptyt, C_LIST0);
+      compact(PTriLive{M.tst}, Ident{}, newn, last_triangle, tail, C_LIST1);
+      LAUNCH(k_compact_tris_move, last_triangle - newn, M, tail, emptyt, dcount + C_LIST1, newidx);
+      LAUNCH(k_fix_nbrs, newn, M, newidx, newn);
+      LAUNCH(k_fix_s2t, last_subseg, M, newidx, last_subseg);
+    }
+    int ntri = newn;
+    // points
+    compact(PPtLive{M.ps}, Ident{}, 0, last_point, pnew, C_MISC);
+    int newp = fetch(C_MISC);
+    LAUNCH(k_newidx_init, last_point, M, pnew, last_point, newp, M.ps, (uint8_t)PS_DELETED, true);
+    if (newp < last_point) {
+      compact(PPtDeleted{M.ps}, Ident{}, 0, newp, emptyp, C_LIST0);
+      compact(PPtLive{M.ps}, Ident{}, newp, last_point, tail, C_LIST1);
+      LAUNCH(k_compact_pts_move, last_point - newp, M, tail, emptyp, dcount + C_LIST1, pnew);
+      LAUNCH(k_fix_tri_vertices, ntri, M, pnew, ntri);
+    }
+    out_np = newp;
+    out_nt = ntri;
+    out_ns = last_subseg;
+    return GQM_OK;
+  }
+
+  // ---- the whole refinement ----
+  int run(const gqm_cdt_in *in, bool on_device, const gqm_options *opt) {
+    int rc = setup(opt->device);
+    if (rc) return rc;
+    have_result = false;
+    stats = gqm_stats{};
+    status = 0;
+    theta = opt->theta;
+    mode = opt->mode ? 1 : 0;
+    pred_mode = opt->predicates ? 1 : 0;
+    max_rounds = opt->max_rounds > 0 ? opt->max_rounds : 1000000;
+    offcenter = 0;
+    double offc = 0.0;
+    if (opt->insert_policy == GQM_OFFCENTER) {  // refine.cu:6555-6567
+      offcenter = 1;
+      double cg = cos(theta * GQM_PI / 180);
+      offc = 0.475 * sqrt((1.0 + cg) / (1.0 - cg));
+    }
+    offconstant = (int)offc;  // splitTriangles takes an int (refine.cu:5132)
+    int np = in->numberofpoints, nt = in->numberoftriangles, ns = in->numberofsegments;
+    nseg_in = ns;
+    pointblock = (int)(np * 0.5);
+    triblock = 2 * pointblock;
+    pcap = np + pointblock;
+    tcap = nt + triblock;
+    rc = alloc_points(std::max<long>(pcap + 3L * pointblock, pphys));
+    if (rc) return rc;
+    rc = alloc_tris(std::max<long>(tcap + 4L * triblock, tphys));
+    if (rc) return rc;
+    rc = alloc_subsegs(std::max<long>(4L * ns + 1024, sphys));
+    if (rc) return rc;
+    // inputs
+    const double *dpts;
+    const int *dtri_in, *dnbr_in, *dseg_in;
+    size_t need = sizeof(double) * 2 * np + sizeof(int) * (6L * nt + 2L * ns) + 256;
+    if (!on_device) {
+      if (need > dinput_bytes) {
+        if (dinput) cudaFree(dinput);
+        dinput = nullptr;
+        if (cudaMalloc((void **)&dinput, need) != cudaSuccess) return GQM_ERR_MEMORY;
+        dinput_bytes = need;
+      }
+      char *base = (char *)dinput;
+      double *p0 = (double *)base;
+      int *t0 = (int *)(base + sizeof(double) * 2 * np);
+      int *n0 = t0 + 3L * nt;
+      int *s0 = n0 + 3L * nt;
+      cudaMemcpyAsync(p0, in->pointlist, sizeof(double) * 2 * np, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(t0, in->trianglelist, sizeof(int) * 3 * nt, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(n0, in->neighborlist, sizeof(int) * 3 * nt, cudaMemcpyHostToDevice, st);
+      if (ns) cudaMemcpyAsync(s0, in->segmentlist, sizeof(int) * 2 * ns, cudaMemcpyHostToDevice, st);
+      dpts = p0;
+      dtri_in = t0;
+      dnbr_in = n0;
+      dseg_in = s0;
+    } else {
+      dpts = in->pointlist;
+      dtri_in = in->trianglelist;
+      dnbr_in = in->neighborlist;
+      dseg_in = in->segmentlist;
+    }
+    cudaEventRecord(ev0, st);
+    if (segs) cudaFree(segs);
+    segs = nullptr;
+    if (dalloc(&segs, ns + 1)) return GQM_ERR_MEMORY;
+    if (ns) cudaMemcpyAsync(segs, dseg_in, sizeof(int2) * ns, cudaMemcpyDeviceToDevice, st);
+    M.segs = segs;
+    cudaMemsetAsync(M.s2t, 0, sizeof(unsigned long long) * sphys, st);
+    cudaMemsetAsync(M.err, 0, sizeof(int), st);
+    cudaMemsetAsync(dctr, 0, sizeof(unsigned long long) * 4, st);
+    // cos^2(theta) on the device, as the reference evaluates it
+    k_goodcos<<<1, 32, 0, st>>>(theta, dgc);
+    double hgc[2];
+    cudaMemcpyAsync(hgc, dgc, sizeof(double) * 2, cudaMemcpyDeviceToHost, st);
+    cudaStreamSynchronize(st);
+    M.gc2 = hgc[0];
+    M.mode = mode;
+    stats.goodcos2 = hgc[0];
+    LAUNCH(k_init_points, pphys, M, (const double2 *)dpts, np, (int)pphys);
+    LAUNCH(k_init_tris, tphys, M, dtri_in, dnbr_in, nt, (int)tphys);
+    // initSubsegs via a hash of segment endpoints
+    {
+      unsigned hsz = 1;
+      while (hsz < 2u * (unsigned)ns + 16) hsz <<= 1;
+      unsigned long long *keys = nullptr;
+      int *vals = nullptr, *s2ti = nullptr;
+      if (dalloc(&keys, hsz) || dalloc(&vals, hsz) || dalloc(&s2ti, ns + 1)) return GQM_ERR_MEMORY;
+      cudaMemsetAsync(keys, 0xff, sizeof(unsigned long long) * hsz, st);
+      cudaMemsetAsync(s2ti, 0xff, sizeof(int) * (ns + 1), st);
+      LAUNCH(k_seg_hash_insert, ns, segs, ns, keys, vals, hsz - 1);
+      LAUNCH(k_init_subsegs, nt, M, nt, keys, vals, hsz - 1, s2ti);
+      LAUNCH(k_pack_s2t, ns, M, s2ti, ns);
+      cudaStreamSynchronize(st);
+      cudaFree(keys);
+      cudaFree(vals);
+      cudaFree(s2ti);
+    }
+    last_point = np;
+    last_triangle = nt;
+    last_subseg = ns;
+    nempty_p = refresh_points();
+    nempty_t = refresh_tris();
+    LAUNCH(k_mark_all_encsegs, ns, M, ns);
+    rc = split_encsegs();
+    int rounds = 0;
+    while (rc == 0) {
+      LAUNCH(k_mark_bad, last_triangle, M, last_triangle);
+      compact(PBad{M.tst}, Ident{}, 0, last_triangle, bad, C_LIST2);
+      int nbad = fetch(C_LIST2);
+      int derr = check_device_error();
+      if (derr) {
+        rc = derr;
+        break;
+      }
+      if (nbad == 0) break;
+      if (rounds >= max_rounds) {
+        rc = GQM_ERR_ROUND_LIMIT;
+        break;
+      }
+      stats.bad_total += nbad;
+      rc = split_triangles(nbad);
+      if (rc) break;
+      rc = split_encsegs();
+      if (rc) break;
+      LAUNCH(k_points_old, last_point, M, last_point);
+      rounds++;
+    }
+    stats.rounds = rounds;
+    if (rc == 0) rc = check_device_error();
+    if (rc == 0) rc = compact_output();
+    cudaEventRecord(ev1, st);
+    cudaError_t ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) rc = GQM_ERR_CUDA;
+    if (rc == 0) {
+      int derr = check_device_error();
+      if (derr) rc = derr;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    stats.device_ms = ms;
+    unsigned long long hc[4];
+    cudaMemcpy(hc, dctr, sizeof(hc), cudaMemcpyDeviceToHost);
+    stats.steiner_inserted = (long long)hc[0];
+    stats.midpoints_inserted = (long long)hc[1];
+    stats.exact_fallbacks = (long long)hc[2];
+    have_result = (rc == 0);
+    status = rc;
+    return rc;
+  }
+
+  int result(gqm_cdt_out *out) {
+    if (!have_result) return GQM_ERR_ARGUMENT;
+    memset(out, 0, sizeof(*out));
+    int np = out_np, nt = out_nt, ns = out_ns;
+    int *dtri = nullptr, *dnbr = nullptr, *dseg = nullptr;
+    uint8_t *dts = nullptr, *dps = nullptr;
+    if (dalloc(&dtri, 3L * nt) || dalloc(&dnbr, 3L * nt) || dalloc(&dseg, 2L * ns) || dalloc(&dts, nt) ||
+        dalloc(&dps, np))
+      return GQM_ERR_MEMORY;
+    LAUNCH(k_emit_output, std::max(nt, ns), M, nt, ns, dtri, dnbr, dseg, dts);
+    LAUNCH(k_emit_pstatus, np, M, np, dps);
+    out->numberofpoints = np;
+    out->numberoftriangles = nt;
+    out->numberofsegments = ns;
+    out->pointlist = (double *)malloc(sizeof(double) * 2 * (size_t)np + 16);
+    out->trianglelist = (int *)malloc(sizeof(int) * 3 * (size_t)nt + 16);
+    out->neighborlist = (int *)malloc(sizeof(int) * 3 * (size_t)nt + 16);
+    out->segmentlist = (int *)malloc(sizeof(int) * 2 * (size_t)ns + 16);
+    out->pstatus = (unsigned char *)malloc((size_t)np + 16);
+    out->tstatus = (unsigned char *)malloc((size_t)nt + 16);
+    cudaMemcpyAsync(out->pointlist, M.pts, sizeof(double) * 2 * (size_t)np, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->trianglelist, dtri, sizeof(int) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->neighborlist, dnbr, sizeof(int) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->segmentlist, dseg, sizeof(int) * 2 * (size_t)ns, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->pstatus, dps, (size_t)np, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out->tstatus, dts, (size_t)nt, cudaMemcpyDeviceToHost, st);
+    cudaError_t ce = cudaStreamSynchronize(st);
+    cudaFree(dtri);
+    cudaFree(dnbr);
+    cudaFree(dseg);
+    cudaFree(dts);
+    cudaFree(dps);
+    return ce == cudaSuccess ? GQM_OK : GQM_ERR_CUDA;
+  }
+};
+
+}  // namespace gqm
+
+struct gqm_context {
+  gqm::Refiner r;
+};
+
+extern "C" {
+
+void gqm_default_options(gqm_options *o) {
+  o->theta = 20.0;
+  o->insert_policy = GQM_OFFCENTER;
+  o->mode = GQM_RUPPERT;
+  o->predicates = GQM_PRED_REFERENCE;
+  o->device = 0;
+  o->max_rounds = 0;
+}
+
+static int validate(const gqm_cdt_in *in, const gqm_options *opt) {
+  if (!in || !opt) return GQM_ERR_ARGUMENT;
+  if (in->numberofpoints < 3 || in->numberoftriangles < 1 || in->numberofsegments < 0) return GQM_ERR_ARGUMENT;
+  if (!in->pointlist || !in->trianglelist || !in->neighborlist) return GQM_ERR_ARGUMENT;
+  if (in->numberofsegments > 0 && !in->segmentlist) return GQM_ERR_ARGUMENT;
+  if (!(opt->theta > 0.0 && opt->theta < 60.0)) return GQM_ERR_ARGUMENT;
+  return GQM_OK;
+}
+
+int gqm_context_create(int device, gqm_context **ctx) {
+  if (!ctx) return GQM_ERR_ARGUMENT;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= device || device < 0) return GQM_ERR_NO_DEVICE;
+  *ctx = new gqm_context();
+  int rc = (*ctx)->r.setup(device);
+  if (rc) {
+    delete *ctx;
+    *ctx = nullptr;
+  }
+  return rc;
+}
+void gqm_context_destroy(gqm_context *ctx) { delete ctx; }
+int gqm_context_run(gqm_context *ctx, const gqm_cdt_in *in, int in_on_device, const gqm_options *opt,
+                    gqm_stats *stats) {
+  if (!ctx) return GQM_ERR_ARGUMENT;
+  int rc = validate(in, opt);
+  if (rc) return rc;
+  rc = ctx->r.run(in, in_on_device != 0, opt);
+  if (stats) *stats = ctx->r.stats;
+  return rc;
+}
+int gqm_context_result(gqm_context *ctx, gqm_cdt_out *out) {
+  if (!ctx || !out) return GQM_ERR_ARGUMENT;
+  return ctx->r.result(out);
+}
+int gqm_context_result_sizes(gqm_context *ctx, int *np, int *nt, int *ns) {
+  if (!ctx || !ctx->r.have_result) return GQM_ERR_ARGUMENT;
+  if (np) *np = ctx->r.out_np;
+  if (nt) *nt = ctx->r.out_nt;
+  if (ns) *ns = ctx->r.out_ns;
+  return GQM_OK;
+}
+void *gqm_context_stream(gqm_context *ctx) { return ctx ? (void *)ctx->r.st : nullptr; }
+
+int gqm_refine(const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt, gqm_stats *stats) {
+  if (!out) return GQM_ERR_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  gqm_options def;
+  if (!opt) {
+    gqm_default_options(&def);
+    opt = &def;
+  }
+  int rc = validate(in, opt);
+  if (rc) return rc;
+  gqm_context *ctx = nullptr;
+  rc = gqm_context_create(opt->device, &ctx);
+  if (rc) return rc;
+  rc = gqm_context_run(ctx, in, 0, opt, stats);
+  if (rc == GQM_OK) rc = gqm_context_result(ctx, out);
+  gqm_context_destroy(ctx);
+  return rc;
+}
+
+void gqm_free_result(gqm_cdt_out *out) {
+  if (!out) return;
+  free(out->pointlist);
+  free(out->trianglelist);
+  free(out->neighborlist);
+  free(out->segmentlist);
+  free(out->pstatus);
+  free(out->tstatus);
+  memset(out, 0, sizeof(*out));
+}
+
+const char *gqm_status_string(int s) {
+  switch (s) {
+    case GQM_OK: return "ok";
+    case GQM_ERR_ARGUMENT: return "invalid argument";
+    case GQM_ERR_ROUND_LIMIT: return "refinement loop exceeded max_rounds";
+    case GQM_ERR_WALK_LIMIT: return "point location walk did not end";
+    case GQM_ERR_FAN_LIMIT: return "vertex fan walk did not close";
+    case GQM_ERR_TOPOLOGY: return "mesh inconsistency";
+    case GQM_ERR_CAVITY: return "cavity walk exceeded its bound";
+    case GQM_ERR_CUDA: return "CUDA runtime error";
+    case GQM_ERR_NO_DEVICE: return "no CUDA device";
+    case GQM_ERR_MEMORY: return "device allocation failed";
+    default: return "unknown status";
+  }
+}
+int gqm_version(void) { return 100; }
+
+}  // extern "C"

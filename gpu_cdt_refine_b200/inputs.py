@@ -1,0 +1,112 @@
+"""Synthetic PSLG workloads and their constrained Delaunay triangulations.
+
+The workloads follow the five benchmark configurations of this project
+(plain small, plain large clustered, adversarial structure, batched domains,
+learned placement).  Points and segments come from the seeded generators in
+csrc/synth.cpp and the CDT from csrc/cdt_build.cpp; everything is
+deterministic for a given seed.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _native
+from .cdtio import CDT
+
+
+def build_cdt(points: np.ndarray, segments: np.ndarray) -> CDT:
+    """CDT with the convex hull enclosed by segments (Triangle "pzQnc")."""
+    lib = _native.host()
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 2)
+    seg = np.ascontiguousarray(segments, dtype=np.int32).reshape(-1, 2)
+    res = _native.CdtResult()
+    rc = lib.gqm_cdt_build(pts.shape[0], _native.dptr(pts), seg.shape[0], _native.iptr(seg), res)
+    if rc != 0:
+        raise ValueError(f"CDT construction failed with status {rc}")
+    try:
+        t, s = res.numberoftriangles, res.numberofsegments
+        tri = np.ctypeslib.as_array(res.trianglelist, shape=(t * 3,)).copy()
+        nbr = np.ctypeslib.as_array(res.neighborlist, shape=(t * 3,)).copy()
+        sg = np.ctypeslib.as_array(res.segmentlist, shape=(s * 2,)).copy()
+    finally:
+        lib.gqm_cdt_free(res)
+    return CDT(pts.copy(), tri, nbr, sg)
+
+
+def uniform_points(n: int, lo: float, hi: float, seed: int) -> np.ndarray:
+    xy = np.empty(2 * n, np.float64)
+    m = _native.host().gqm_synth_uniform(n, lo, hi, seed, _native.dptr(xy))
+    return xy[:2 * m].reshape(m, 2)
+
+
+def cluster_points(n: int, k: int, L: float, smin: float, smax: float, bg: float, seed: int) -> np.ndarray:
+    xy = np.empty(2 * n, np.float64)
+    m = _native.host().gqm_synth_clusters(n, k, L, smin, smax, bg, seed, _native.dptr(xy))
+    return xy[:2 * m].reshape(m, 2)
+
+
+def pick_segments(points: np.ndarray, nseg: int, seed: int, max_gap: int = 8,
+                  max_tries: int | None = None) -> np.ndarray:
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    out = np.empty(2 * max(nseg, 1), np.int32)
+    tries = max_tries if max_tries is not None else 200 * nseg + 1000
+    m = _native.host().gqm_pick_segments(pts.shape[0], _native.dptr(pts), nseg, max_gap, seed, tries,
+                                         _native.iptr(out))
+    return out[:2 * m].reshape(m, 2)
+
+
+def filter_segments(points: np.ndarray, cand: np.ndarray, nseg: int) -> np.ndarray:
+    pts = np.ascontiguousarray(points, dtype=np.float64)
+    c = np.ascontiguousarray(cand, dtype=np.int32).reshape(-1, 2)
+    out = np.empty(2 * max(nseg, 1), np.int32)
+    m = _native.host().gqm_filter_segments(pts.shape[0], _native.dptr(pts), c.shape[0], _native.iptr(c), nseg,
+                                           _native.iptr(out))
+    return out[:2 * m].reshape(m, 2)
+
+
+def grid_circle_points(g: int, sp: float, jit: float, nc: int, per: int, cxy: float, r0: float, r1: float,
+                       seed: int):
+    n = g * g + nc * per
+    xy = np.empty(2 * n, np.float64)
+    cid = np.empty(n, np.int32)
+    m = _native.host().gqm_synth_grid_circles(g, sp, jit, nc, per, cxy, r0, r1, seed, _native.dptr(xy),
+                                              _native.iptr(cid))
+    return xy[:2 * m].reshape(m, 2), cid[:m]
+
+
+# --- the benchmark workloads -------------------------------------------------
+
+def plain_small(seed: int = 20261204, n: int = 10_000, nseg: int = 500) -> CDT:
+    """10,000 points uniform in [0,1000]^2 with 500 random nearby-pair segments."""
+    pts = uniform_points(n, 0.0, 1000.0, seed)
+    seg = pick_segments(pts, nseg, seed + 1)
+    return build_cdt(pts, seg)
+
+
+def clustered(seed: int = 20261205, n: int = 2_000_000, nseg: int = 100_000) -> CDT:
+    """64 isotropic Gaussians (centres U[0,1e4]^2, sigma log-U[5,200]) + 10% uniform."""
+    pts = cluster_points(n, 64, 1.0e4, 5.0, 200.0, 0.10, seed)
+    seg = pick_segments(pts, nseg, seed + 1)
+    return build_cdt(pts, seg)
+
+
+def adversarial(seed: int = 20261206, g: int = 700, nc: int = 200, nseg: int = 20_000,
+                per: int | None = None) -> CDT:
+    """Jittered g x g grid plus nc concentric circles; chords along the circles."""
+    n_grid = g * g
+    if per is None:
+        per = max(3, n_grid // nc + (n_grid % nc > 0))  # about as many circle points as grid points
+    sp = 1.0
+    c = (g - 1) * sp / 2.0
+    pts, cid = grid_circle_points(g, sp, 1e-9, nc, per, c, 0.05 * g * sp, 0.45 * g * sp, seed)
+    cand = []
+    for k in range(nc):
+        idx = np.nonzero(cid == k)[0]
+        ang = np.arctan2(pts[idx, 1] - c, pts[idx, 0] - c)
+        idx = idx[np.argsort(ang)]
+        cand.append(np.stack([idx[0:-1:2], idx[1::2]], axis=1))
+    cand = np.concatenate(cand, axis=0)
+    rng = np.random.default_rng(seed + 1)
+    cand = cand[rng.permutation(cand.shape[0])]
+    seg = filter_segments(pts, cand, nseg)
+    return build_cdt(pts, seg)

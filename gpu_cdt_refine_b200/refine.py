@@ -1,0 +1,225 @@
+"""Python host side of the refiner, mirroring the reference's interface.
+
+``GPU_Refine_Quality(input, theta, insertpolicy, deletepolicy, mode,
+debug_iter)`` has the argument meaning of GPU_Refine/refine.h:385-386 and
+returns the refined CDT (plus the PStatus / TStatus debug bytes when asked).
+It calls the sm_100a library through the C ABI of include/gqm_refine.h; there
+is no CPU fallback: without the library or a GPU it raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _native
+from .cdtio import CDT
+
+Circumcenter, Offcenter = 0, 1
+Strict, Connected, Orthogonal, noDeletion, DeleteFromDT, noPriority = range(6)
+PRED_REFERENCE, PRED_EXACT = 0, 1
+
+
+class CdtIn(ctypes.Structure):
+    _fields_ = [("numberofpoints", ctypes.c_int), ("pointlist", ctypes.c_void_p),
+                ("numberoftriangles", ctypes.c_int), ("trianglelist", ctypes.c_void_p),
+                ("neighborlist", ctypes.c_void_p), ("numberofsegments", ctypes.c_int),
+                ("segmentlist", ctypes.c_void_p)]
+
+
+class CdtOut(ctypes.Structure):
+    _fields_ = [("numberofpoints", ctypes.c_int), ("pointlist", ctypes.POINTER(ctypes.c_double)),
+                ("numberoftriangles", ctypes.c_int), ("trianglelist", ctypes.POINTER(ctypes.c_int)),
+                ("neighborlist", ctypes.POINTER(ctypes.c_int)), ("numberofsegments", ctypes.c_int),
+                ("segmentlist", ctypes.POINTER(ctypes.c_int)), ("pstatus", ctypes.POINTER(ctypes.c_ubyte)),
+                ("tstatus", ctypes.POINTER(ctypes.c_ubyte))]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("theta", ctypes.c_double), ("insert_policy", ctypes.c_int), ("mode", ctypes.c_int),
+                ("predicates", ctypes.c_int), ("device", ctypes.c_int), ("max_rounds", ctypes.c_longlong)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("rounds", ctypes.c_int), ("flip_steps", ctypes.c_longlong),
+                ("steiner_inserted", ctypes.c_longlong), ("midpoints_inserted", ctypes.c_longlong),
+                ("bad_total", ctypes.c_longlong), ("host_syncs", ctypes.c_longlong),
+                ("kernel_launches", ctypes.c_longlong), ("exact_fallbacks", ctypes.c_longlong),
+                ("goodcos2", ctypes.c_double), ("device_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class RefineError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"{msg} (status {status})")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The sm_100a library; raises when it is missing (no fallback path)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_native.CUDA_LIB):
+            raise RuntimeError(f"{_native.CUDA_LIB} is missing: run `python -m gpu_cdt_refine_b200.build`")
+        L = ctypes.CDLL(_native.CUDA_LIB)
+        L.gqm_default_options.argtypes = [ctypes.POINTER(Options)]
+        L.gqm_refine.argtypes = [ctypes.POINTER(CdtIn), ctypes.POINTER(CdtOut), ctypes.POINTER(Options),
+                                 ctypes.POINTER(Stats)]
+        L.gqm_refine.restype = ctypes.c_int
+        L.gqm_free_result.argtypes = [ctypes.POINTER(CdtOut)]
+        L.gqm_status_string.argtypes = [ctypes.c_int]
+        L.gqm_status_string.restype = ctypes.c_char_p
+        L.gqm_context_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.gqm_context_create.restype = ctypes.c_int
+        L.gqm_context_destroy.argtypes = [ctypes.c_void_p]
+        L.gqm_context_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(CdtIn), ctypes.c_int,
+                                      ctypes.POINTER(Options), ctypes.POINTER(Stats)]
+        L.gqm_context_run.restype = ctypes.c_int
+        L.gqm_context_result.argtypes = [ctypes.c_void_p, ctypes.POINTER(CdtOut)]
+        L.gqm_context_result.restype = ctypes.c_int
+        L.gqm_context_result_sizes.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int),
+                                               ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
+        L.gqm_context_result_sizes.restype = ctypes.c_int
+        L.gqm_context_stream.argtypes = [ctypes.c_void_p]
+        L.gqm_context_stream.restype = ctypes.c_void_p
+        L.gqm_version.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def make_options(theta=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0,
+                 max_rounds=0) -> Options:
+    o = Options()
+    lib().gqm_default_options(ctypes.byref(o))
+    o.theta = float(theta)
+    o.insert_policy = int(insertpolicy)
+    o.mode = 1 if mode else 0
+    o.predicates = int(predicates)
+    o.device = int(device)
+    o.max_rounds = int(max_rounds)
+    return o
+
+
+def _cdt_in(cdt: CDT, keep):
+    arrs = [np.ascontiguousarray(cdt.pointlist, np.float64), np.ascontiguousarray(cdt.trianglelist, np.int32),
+            np.ascontiguousarray(cdt.neighborlist, np.int32), np.ascontiguousarray(cdt.segmentlist, np.int32)]
+    keep.extend(arrs)
+    return CdtIn(arrs[0].shape[0], arrs[0].ctypes.data, arrs[1].shape[0], arrs[1].ctypes.data, arrs[2].ctypes.data,
+                 arrs[3].shape[0], arrs[3].ctypes.data)
+
+
+def _take(out: CdtOut, with_status=False):
+    np_, nt_, ns_ = out.numberofpoints, out.numberoftriangles, out.numberofsegments
+    res = CDT(np.ctypeslib.as_array(out.pointlist, shape=(2 * np_,)).copy() if np_ else np.zeros(0),
+              np.ctypeslib.as_array(out.trianglelist, shape=(3 * nt_,)).copy() if nt_ else np.zeros(0, np.int32),
+              np.ctypeslib.as_array(out.neighborlist, shape=(3 * nt_,)).copy() if nt_ else np.zeros(0, np.int32),
+              np.ctypeslib.as_array(out.segmentlist, shape=(2 * ns_,)).copy() if ns_ else np.zeros(0, np.int32))
+    if not with_status:
+        return res
+    ps = np.ctypeslib.as_array(out.pstatus, shape=(np_,)).copy() if np_ else np.zeros(0, np.uint8)
+    ts = np.ctypeslib.as_array(out.tstatus, shape=(nt_,)).copy() if nt_ else np.zeros(0, np.uint8)
+    return res, ps, ts
+
+
+def refine(cdt: CDT, theta=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0,
+           max_rounds=0, with_status=False):
+    """Refine a CDT on the GPU; returns (CDT, stats dict) or (CDT, ps, ts, stats)."""
+    L = lib()
+    keep = []
+    cin = _cdt_in(cdt, keep)
+    out = CdtOut()
+    st = Stats()
+    opt = make_options(theta, insertpolicy, mode, predicates, device, max_rounds)
+    rc = L.gqm_refine(ctypes.byref(cin), ctypes.byref(out), ctypes.byref(opt), ctypes.byref(st))
+    if rc != 0:
+        raise RefineError(rc, L.gqm_status_string(rc).decode())
+    try:
+        got = _take(out, with_status)
+    finally:
+        L.gqm_free_result(ctypes.byref(out))
+    if with_status:
+        return (*got, st.as_dict())
+    return got, st.as_dict()
+
+
+def GPU_Refine_Quality(input: CDT, theta: float, insertpolicy=Offcenter, deletepolicy=Connected, mode=1,
+                       debug_iter=-1, ps_debug=False, ts_debug=False):
+    """Drop-in for the reference entry point (GPU_Refine/refine.h:385-386).
+
+    `deletepolicy` and `debug_iter` are accepted and ignored, as in the
+    reference.  Returns the refined CDT, or (CDT, pstatus, tstatus) when
+    `ps_debug` or `ts_debug` is true.
+    """
+    del deletepolicy, debug_iter
+    want = bool(ps_debug or ts_debug)
+    r = refine(input, theta, insertpolicy, mode, with_status=want)
+    if want:
+        return r[0], r[1], r[2]
+    return r[0]
+
+
+class Context:
+    """Reusable device context (gqm_context): buffers persist between runs."""
+
+    def __init__(self, device=0):
+        self._lib = lib()
+        self._h = ctypes.c_void_p()
+        rc = self._lib.gqm_context_create(int(device), ctypes.byref(self._h))
+        if rc != 0:
+            raise RefineError(rc, self._lib.gqm_status_string(rc).decode())
+
+    def close(self):
+        if self._h:
+            self._lib.gqm_context_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return int(self._lib.gqm_context_stream(self._h) or 0)
+
+    def run_device(self, np_, nt_, ns_, d_points, d_tris, d_nbrs, d_segs, opt: Options) -> dict:
+        """Refine inputs that already live in device memory (raw pointers)."""
+        cin = CdtIn(np_, d_points, nt_, d_tris, d_nbrs, ns_, d_segs)
+        st = Stats()
+        rc = self._lib.gqm_context_run(self._h, ctypes.byref(cin), 1, ctypes.byref(opt), ctypes.byref(st))
+        if rc != 0:
+            raise RefineError(rc, self._lib.gqm_status_string(rc).decode())
+        return st.as_dict()
+
+    def run_host(self, cdt: CDT, opt: Options) -> dict:
+        keep = []
+        cin = _cdt_in(cdt, keep)
+        st = Stats()
+        rc = self._lib.gqm_context_run(self._h, ctypes.byref(cin), 0, ctypes.byref(opt), ctypes.byref(st))
+        if rc != 0:
+            raise RefineError(rc, self._lib.gqm_status_string(rc).decode())
+        return st.as_dict()
+
+    def sizes(self):
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        rc = self._lib.gqm_context_result_sizes(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c))
+        if rc != 0:
+            raise RefineError(rc, "no result")
+        return a.value, b.value, c.value
+
+    def result(self, with_status=False):
+        out = CdtOut()
+        rc = self._lib.gqm_context_result(self._h, ctypes.byref(out))
+        if rc != 0:
+            raise RefineError(rc, self._lib.gqm_status_string(rc).decode())
+        try:
+            return _take(out, with_status)
+        finally:
+            self._lib.gqm_free_result(ctypes.byref(out))

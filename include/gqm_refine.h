@@ -1,0 +1,124 @@
+/* gqm_refine.h - C ABI of the B200 constrained-Delaunay quality refiner.
+ *
+ * Every entry point takes plain pointers and sizes and returns a status code
+ * (GQM_OK == 0, negative on error); none of them exits the process.
+ *
+ * Reference interface replaced (chenzhenghai/GPU_CDT_Refine):
+ *   void GPU_Refine_Quality(triangulateio *input, triangulateio *result,
+ *        double theta, InsertPolicy insertpolicy, DeletePolicy deletepolicy,
+ *        int mode, int debug_iter, PStatus **ps_debug, TStatus **ts_debug);
+ *   declared at GPU_Refine/refine.h:385-386, defined at
+ *   GPU_Refine/refine.cu:6500-7139.
+ * The C++ drop-in with that exact signature is in gqm_triangulateio.h and
+ * forwards to gqm_refine() below.
+ */
+#ifndef GQM_REFINE_H
+#define GQM_REFINE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define GQM_OK 0
+#define GQM_ERR_ARGUMENT (-1)     /* null pointer or inconsistent sizes */
+#define GQM_ERR_ROUND_LIMIT (-2)  /* a refinement loop exceeded options.max_rounds */
+#define GQM_ERR_WALK_LIMIT (-3)   /* a point-location walk did not end */
+#define GQM_ERR_FAN_LIMIT (-4)    /* a vertex fan walk did not close */
+#define GQM_ERR_TOPOLOGY (-5)     /* mesh inconsistency found on the device */
+#define GQM_ERR_CAVITY (-6)       /* cavity walk exceeded its bound */
+#define GQM_ERR_CUDA (-10)        /* a CUDA runtime call failed */
+#define GQM_ERR_NO_DEVICE (-11)   /* no CUDA device */
+#define GQM_ERR_MEMORY (-12)      /* device allocation failed */
+
+/* InsertPolicy (GPU_Refine/refine.h:32) */
+#define GQM_CIRCUMCENTER 0
+#define GQM_OFFCENTER 1
+/* refinement mode (GPU_Refine/refine.cu:131: run_mode != 0 is Ruppert) */
+#define GQM_CHEW 0
+#define GQM_RUPPERT 1
+/* predicate arithmetic */
+#define GQM_PRED_REFERENCE 0 /* the reference's effective FP64 arithmetic (bit-exact parity) */
+#define GQM_PRED_EXACT 1     /* exact orient2d/incircle (adaptive filter + expansions) */
+
+/* Input CDT in Triangle's triangulateio layout (GPU_Refine/triangle.h:253-284):
+ * zero-based indices, counterclockwise triangles, neighbour j opposite vertex
+ * j (-1 on the boundary), convex hull enclosed by segments. */
+typedef struct {
+  int numberofpoints;
+  const double *pointlist;   /* 2 * numberofpoints, x y interleaved */
+  int numberoftriangles;
+  const int *trianglelist;   /* 3 * numberoftriangles */
+  const int *neighborlist;   /* 3 * numberoftriangles */
+  int numberofsegments;
+  const int *segmentlist;    /* 2 * numberofsegments */
+} gqm_cdt_in;
+
+/* Output CDT.  Arrays are allocated by the library with malloc() and released
+ * with gqm_free_result().  pstatus / tstatus hold the reference's PStatus /
+ * TStatus bytes of the compacted points / triangles (refine.h:36-205). */
+typedef struct {
+  int numberofpoints;
+  double *pointlist;
+  int numberoftriangles;
+  int *trianglelist;
+  int *neighborlist;
+  int numberofsegments;
+  int *segmentlist;
+  unsigned char *pstatus;
+  unsigned char *tstatus;
+} gqm_cdt_out;
+
+typedef struct {
+  double theta;         /* minimum angle in degrees */
+  int insert_policy;    /* GQM_CIRCUMCENTER / GQM_OFFCENTER */
+  int mode;             /* GQM_RUPPERT / GQM_CHEW */
+  int predicates;       /* GQM_PRED_REFERENCE / GQM_PRED_EXACT */
+  int device;           /* CUDA device ordinal */
+  long long max_rounds; /* bound on every refinement loop; 0 = default (1e6) */
+} gqm_options;
+
+typedef struct {
+  int rounds;                   /* quality iterations */
+  long long flip_steps;         /* flip-flop steps */
+  long long steiner_inserted;   /* interior/edge Steiner points inserted */
+  long long midpoints_inserted; /* subsegment split points inserted */
+  long long bad_total;          /* bad triangles summed over rounds */
+  long long host_syncs;         /* device-to-host count reads */
+  long long kernel_launches;    /* kernels launched by the refinement */
+  long long exact_fallbacks;    /* predicate evaluations that needed the expansion path */
+  double goodcos2;              /* cos^2(theta) as evaluated on the device */
+  double device_ms;             /* device time of the refinement (CUDA events) */
+} gqm_stats;
+
+/* Default options: theta 20, Offcenter, Ruppert, reference predicates, device 0. */
+void gqm_default_options(gqm_options *opt);
+
+/* One call: host CDT in, host CDT out (host<->device copies included).
+ * Equivalent of GPU_Refine_Quality. */
+int gqm_refine(const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt, gqm_stats *stats);
+void gqm_free_result(gqm_cdt_out *out);
+
+/* Reusable context: device buffers are kept between runs. */
+typedef struct gqm_context gqm_context;
+int gqm_context_create(int device, gqm_context **ctx);
+void gqm_context_destroy(gqm_context *ctx);
+/* Refine a CDT whose arrays already reside in device memory (in_on_device != 0)
+ * or in host memory; the result stays on the device until gqm_context_result. */
+int gqm_context_run(gqm_context *ctx, const gqm_cdt_in *in, int in_on_device, const gqm_options *opt,
+                    gqm_stats *stats);
+int gqm_context_result(gqm_context *ctx, gqm_cdt_out *out);
+/* Sizes of the last result without copying it. */
+int gqm_context_result_sizes(gqm_context *ctx, int *npoints, int *ntriangles, int *nsegments);
+/* The CUDA stream the context launches on (a cudaStream_t). */
+void *gqm_context_stream(gqm_context *ctx);
+
+const char *gqm_status_string(int status);
+int gqm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

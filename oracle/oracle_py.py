@@ -1,0 +1,85 @@
+"""ctypes bindings of the test oracle (oracle/_build/libgqm_oracle.so).
+
+Test infrastructure: imported only by tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libgqm_oracle.so")
+
+
+class OracleOut(ctypes.Structure):
+    _fields_ = [("numberofpoints", ctypes.c_int), ("numberoftriangles", ctypes.c_int),
+                ("numberofsegments", ctypes.c_int),
+                ("pointlist", ctypes.POINTER(ctypes.c_double)),
+                ("trianglelist", ctypes.POINTER(ctypes.c_int)),
+                ("neighborlist", ctypes.POINTER(ctypes.c_int)),
+                ("segmentlist", ctypes.POINTER(ctypes.c_int)),
+                ("pstatus", ctypes.POINTER(ctypes.c_ubyte)),
+                ("tstatus", ctypes.POINTER(ctypes.c_ubyte)),
+                ("rounds", ctypes.c_int), ("status", ctypes.c_int),
+                ("flip_steps", ctypes.c_longlong), ("steiner_inserted", ctypes.c_longlong),
+                ("midpoints_inserted", ctypes.c_longlong), ("bad_total", ctypes.c_longlong)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            raise RuntimeError(f"{LIB} missing: run `make -C oracle oracle`")
+        L = ctypes.CDLL(LIB)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.gqm_oracle_refine.argtypes = [ctypes.c_int, dp, ctypes.c_int, ip, ip, ctypes.c_int, ip, ctypes.c_double,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_longlong, ctypes.POINTER(OracleOut)]
+        L.gqm_oracle_refine.restype = ctypes.c_int
+        L.gqm_oracle_free.argtypes = [ctypes.POINTER(OracleOut)]
+        for f in ("gqm_oracle_orient",):
+            getattr(L, f).argtypes = [dp, dp, dp]
+            getattr(L, f).restype = ctypes.c_double
+        for f in ("gqm_oracle_incircle", "gqm_oracle_incircle_exact"):
+            getattr(L, f).argtypes = [dp, dp, dp, dp]
+            getattr(L, f).restype = ctypes.c_double
+        L.gqm_oracle_circumcenter.argtypes = [dp, dp, dp, ctypes.c_double, ctypes.c_int, dp]
+        _lib = L
+    return _lib
+
+
+def refine(cdt, theta=20.0, policy=1, mode=1, max_rounds=100000):
+    """Run the oracle on a CDT; returns (CDT, info dict)."""
+    from gpu_cdt_refine_b200.cdtio import CDT
+    L = lib()
+    out = OracleOut()
+    p = np.ascontiguousarray(cdt.pointlist, np.float64)
+    t = np.ascontiguousarray(cdt.trianglelist, np.int32)
+    n = np.ascontiguousarray(cdt.neighborlist, np.int32)
+    s = np.ascontiguousarray(cdt.segmentlist, np.int32)
+    ip = ctypes.POINTER(ctypes.c_int)
+    rc = L.gqm_oracle_refine(p.shape[0], p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), t.shape[0],
+                             t.ctypes.data_as(ip), n.ctypes.data_as(ip), s.shape[0], s.ctypes.data_as(ip),
+                             float(theta), int(policy), int(mode), int(max_rounds), ctypes.byref(out))
+    info = dict(status=rc, rounds=out.rounds, flip_steps=out.flip_steps, steiner=out.steiner_inserted,
+                midpoints=out.midpoints_inserted, bad_total=out.bad_total)
+    if rc != 0:
+        L.gqm_oracle_free(ctypes.byref(out))
+        raise RuntimeError(f"oracle failed: {info}")
+    try:
+        np_, nt_, ns_ = out.numberofpoints, out.numberoftriangles, out.numberofsegments
+        res = CDT(np.ctypeslib.as_array(out.pointlist, shape=(2 * np_,)).copy(),
+                  np.ctypeslib.as_array(out.trianglelist, shape=(3 * nt_,)).copy(),
+                  np.ctypeslib.as_array(out.neighborlist, shape=(3 * nt_,)).copy(),
+                  np.ctypeslib.as_array(out.segmentlist, shape=(2 * ns_,)).copy())
+        info["pstatus"] = np.ctypeslib.as_array(out.pstatus, shape=(np_,)).copy()
+        info["tstatus"] = np.ctypeslib.as_array(out.tstatus, shape=(nt_,)).copy()
+    finally:
+        L.gqm_oracle_free(ctypes.byref(out))
+    return res, info
