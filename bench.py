@@ -1,0 +1,291 @@
+"""Benchmark: output triangles/s of constrained-Delaunay quality refinement.
+
+Workload (default): the large clustered configuration - 2,000,000 FP64 points
+from 64 isotropic Gaussians (centres uniform in [0,1e4]^2, sigma log-uniform in
+[5,200]) plus 10% uniform background, 100,000 non-crossing endpoint-disjoint
+segments, CDT with the convex hull enclosed; theta = 20 deg, Ruppert mode,
+Offcenter policy.  Inputs are synthetic and seeded (no dataset exists for it).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  `value` is output triangles per second of the
+refinement with the input CDT already resident in HBM; `e2e` is the same
+metric through the reference-facing C ABI call (host arrays in, host arrays
+out, copies included).  The working set (input CDT ~130 MB plus the mesh
+arrays) exceeds the 126 MB L2, so no explicit flush is done between steps.
+
+--impl reference times the reference's own CPU quality refinement (Triangle
+1.6 as vendored by the reference, triangulate("pzDQnrq20"),
+GPU_Refine/main.cpp:389-407) compiled from the reference sources into
+oracle/_ref, on the host cores.
+
+Multi-GPU: the single-domain refinement does not shard (its rounds resolve
+conflicts globally), so --gpus N runs N independent replicas, one per GPU,
+each refining the full workload; value is the sum over ranks of output
+triangles divided by the slowest rank's time ("scaling": "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "output triangles/s at theta=20 deg, 1 B200 (learned vs plain); output vertex count"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--points", type=int, default=2_000_000)
+    p.add_argument("--segments", type=int, default=100_000)
+    p.add_argument("--seed", type=int, default=20261205)
+    p.add_argument("--cpu-baseline", type=int, default=1, help="time the CPU baseline (rank 0, N=1)")
+    p.add_argument("--e2e-steps", type=int, default=3)
+    return p.parse_args()
+
+
+def workload(args):
+    from gpu_cdt_refine_b200 import inputs
+    t0 = time.time()
+    cdt = inputs.clustered(seed=args.seed, n=args.points, nseg=args.segments)
+    return cdt, time.time() - t0
+
+
+def config(args, cdt):
+    return {"workload": "clustered Gaussian mixture, theta=20 Ruppert Offcenter",
+            "points_in": cdt.numberofpoints, "triangles_in": cdt.numberoftriangles,
+            "segments_in": cdt.numberofsegments, "theta": 20.0, "mode": "ruppert", "policy": "offcenter",
+            "predicates": "reference", "l2": "working set larger than L2 (126 MB); no flush",
+            "seed": args.seed}
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.idx), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[1]))
+                mx = float(s[2])
+                for k, n in enumerate(names):
+                    if s[5 + k].lower().startswith("active"):
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                pass
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def cpu_sample(args):
+    """Bounded sample of the workload for the CPU legs: the same generator at
+    1/8 of the points and segments (Triangle needs ~40 s for the full 2M-point
+    input on one core)."""
+    from gpu_cdt_refine_b200 import inputs
+    return inputs.clustered(seed=args.seed + 7, n=max(args.points // 8, 1000), nseg=max(args.segments // 8, 50))
+
+
+def time_triangle(cdt, reps, theta=20.0, mode=1):
+    """Triangle -q (reference CPU quality refinement) on the CDT; returns (tri/s, ms list, out tris)."""
+    from oracle import tri_ref
+    times, nt = [], 0
+    for _ in range(reps):
+        ms, nt = tri_ref.quality(cdt, theta, mode)
+        times.append(ms)
+    return nt / (np.mean(times) / 1e3), times, nt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    full, _ = workload(args)
+    cdt = cpu_sample(args)
+    from oracle import tri_ref
+    for _ in range(min(args.warmup, 1)):
+        tri_ref.quality(cdt, 20.0, 1)
+    tps, times, nt = time_triangle(cdt, args.steps)
+    ms = float(np.mean(times))
+    line = {"metric": METRIC, "value": tps, "unit": "triangles/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)", "impl": "reference",
+            "config": config(args, full),
+            "cpu_baseline": {"value": tps, "unit": "triangles/s", "cores": 1, "kind": "reference",
+                             "sample": f"Triangle 1.6 pzDQnrq20 (single-threaded, as vendored by the reference) on "
+                                       f"a 1/8 sample of the workload ({cdt.numberofpoints} points, "
+                                       f"{cdt.numberofsegments} segments) per step"},
+            "e2e": {"value": tps, "unit": "triangles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "output_triangles": nt}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from gpu_cdt_refine_b200 import refine
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    cdt, gen_s = workload(args)
+    # inputs resident in HBM
+    d_pts = torch.from_numpy(cdt.pointlist).to(dev)
+    d_tri = torch.from_numpy(cdt.trianglelist).to(dev)
+    d_nbr = torch.from_numpy(cdt.neighborlist).to(dev)
+    d_seg = torch.from_numpy(cdt.segmentlist).to(dev)
+    torch.cuda.synchronize()
+    ctx = refine.Context(local_rank)
+    opt = refine.make_options(20.0, refine.Offcenter, 1, device=local_rank)
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+
+    def step():
+        return ctx.run_device(cdt.numberofpoints, cdt.numberoftriangles, cdt.numberofsegments, d_pts.data_ptr(),
+                              d_tri.data_ptr(), d_nbr.data_ptr(), d_seg.data_ptr(), opt)
+
+    for _ in range(args.warmup):
+        st = step()
+    np_out, nt_out, ns_out = ctx.sizes()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    with Clocks(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            stats.append(step())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms_total = ev0.elapsed_time(ev1)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = ms_total / args.steps
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    tris = torch.tensor([float(nt_out)], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tris, op=dist.ReduceOp.SUM)
+    ms_max = float(t.item())
+    value = float(tris.item()) / (ms_max / 1e3)
+
+    # end to end through the reference-facing call: host arrays in, host arrays out
+    e2e_ms, h2d, d2h = [], cdt.nbytes(), 0
+    for _ in range(args.e2e_steps):
+        t0 = time.perf_counter()
+        out, _ = refine.refine(cdt, 20.0, refine.Offcenter, 1, device=local_rank)
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+        d2h = out.nbytes() + out.numberofpoints + out.numberoftriangles
+    e2e_t = torch.tensor([float(np.median(e2e_ms))], device=dev, dtype=torch.float64)
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = float(tris.item()) / (float(e2e_t.item()) / 1e3)
+
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        s = stats[-1]
+        # path-level algorithmic bytes (input + output mesh + one quality check of
+        # every output triangle): 16 B/point, 24 B/triangle, 8 B/segment, 60 B/tri
+        alg = (16 * cdt.numberofpoints + 24 * cdt.numberoftriangles + 8 * cdt.numberofsegments + 16 * np_out +
+               24 * nt_out + 8 * ns_out + 60 * nt_out)
+        achieved = alg / (ms / 1e3) / 1e9
+        line = {"metric": METRIC, "value": value, "unit": "triangles/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+                "config": config(args, cdt),
+                "output_vertices": np_out, "output_triangles": nt_out, "output_segments": ns_out,
+                "e2e": {"value": e2e_value, "unit": "triangles/s", "h2d_bytes_per_step": int(h2d),
+                        "d2h_bytes_per_step": int(d2h), "ms_per_step": float(e2e_t.item())},
+                "gpu_launches": int(s["kernel_launches"]),
+                "host_syncs": int(s["host_syncs"]), "rounds": int(s["rounds"]),
+                "flip_steps": int(s["flip_steps"]),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                             "kernel": "whole refinement path (algorithmic bytes per output triangle)"},
+                "clocks": clk.summary(), "input_generation_s": gen_s}
+        if args.cpu_baseline and world == 1:
+            try:
+                smp = cpu_sample(args)
+                tps, times, ntc = time_triangle(smp, 2)
+                line["cpu_baseline"] = {"value": tps, "unit": "triangles/s", "cores": 1, "kind": "reference",
+                                        "sample": f"Triangle 1.6 pzDQnrq20 on a 1/8 sample of the workload "
+                                                  f"({smp.numberofpoints} points), 2 runs",
+                                        "output_triangles": ntc}
+            except Exception as e:  # the reference build is test infrastructure; report, do not fail
+                line["cpu_baseline"] = {"value": None, "unit": "triangles/s", "cores": 1, "kind": "reference",
+                                        "sample": f"unavailable: {e}"}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -265,27 +265,40 @@ struct Refiner {
     if (g > 148L * 64) g = 148L * 64;
     return (int)g;
   }
-#define LAUNCH(kernel, n, ...)                                              \
-  do {                                                                      \
-    kernel<<<grid_for(n), 256, 0, st>>>(__VA_ARGS__);                       \
-    stats.kernel_launches++;                                                \
+#ifdef GQM_HOST_EMU
+#define KL(kernel, g, b) kernel
+#else
+#define KL(kernel, g, b) kernel<<<(g), (b), 0, st>>>
+#endif
+#define LAUNCH(kernel, n, ...)                   \
+  do {                                           \
+    KL(kernel, grid_for(n), 256)(__VA_ARGS__);   \
+    stats.kernel_launches++;                     \
   } while (0)
 
   // Ordered compaction over [lo, hi) into out; the count lands in dcount[slot].
   template <class F, class Mp>
   void compact(F f, Mp m, int lo, int hi, int *out, int slot) {
     int n = hi - lo;
+#ifdef GQM_HOST_EMU
+    int c = 0;
+    for (int i = lo; i < hi; ++i)
+      if (f(i)) out[c++] = m(i);
+    dcount[slot] = c;
+    stats.kernel_launches += 3;
+    return;
+#endif
     if (n <= 0) {
-      k_set_count<<<1, 32, 0, st>>>(dcount + slot, 0);
+      KL(k_set_count, 1, 32)(dcount + slot, 0);
       stats.kernel_launches++;
       return;
     }
     int chunk = std::max(4 * kCompactThreads, (n + kMaxCompactBlocks - 1) / kMaxCompactBlocks);
     chunk = (chunk + kCompactThreads - 1) / kCompactThreads * kCompactThreads;
     int nb = (n + chunk - 1) / chunk;
-    k_cnt<<<nb, kCompactThreads, 0, st>>>(f, lo, hi, chunk, bc);
-    k_scan<<<1, 1024, 0, st>>>(bc, nb, dcount + slot);
-    k_emit<<<nb, kCompactThreads, 0, st>>>(f, m, lo, hi, chunk, bc, out);
+    KL(k_cnt, nb, kCompactThreads)(f, lo, hi, chunk, bc);
+    KL(k_scan, 1, 1024)(bc, nb, dcount + slot);
+    KL(k_emit, nb, kCompactThreads)(f, m, lo, hi, chunk, bc, out);
     stats.kernel_launches += 3;
   }
   int fetch(int slot) {
@@ -308,7 +321,7 @@ struct Refiner {
     long old = pphys;
     if (n <= old) return GQM_OK;
     if (regrow(&M.pts, old, n) || regrow(&M.ps, old, n) || regrow(&M.pred, old, n) || regrow(&emptyp, 0, n) ||
-        regrow(&pnew, old, n))
+        regrow(&pnew, old, n) || regrow(&tail, 0, std::max<long>(n, tphys)))
       return GQM_ERR_MEMORY;
     // new slots are deleted points
     if (n > old) {
@@ -327,7 +340,8 @@ struct Refiner {
         regrow(&M.tmark, old, n) || regrow(&M.tpos, old, n) || regrow(&emptyt, 0, n) || regrow(&bad, old, n) ||
         regrow(&imark, old, n) || regrow(&ilist, old, n) || regrow(&sinks, old, n) || regrow(&wl, old, n) ||
         regrow(&act, old, n) || regrow(&win, old, n) || regrow(&neg, old, n) || regrow(&ll, 2 * old, 2 * n) ||
-        regrow(&sl, 6 * old, 6 * n) || regrow(&newidx, 0, n) || regrow(&tail, 0, n) || regrow(&center, old, n))
+        regrow(&sl, 6 * old, 6 * n) || regrow(&newidx, 0, n) || regrow(&tail, 0, std::max<long>(n, pphys)) ||
+        regrow(&center, old, n))
       return GQM_ERR_MEMORY;
     if (n > old) {
       cudaMemsetAsync(M.tst + old, 0, n - old, st);
@@ -371,7 +385,11 @@ struct Refiner {
       if (num) {
         long ncap = pcap + num * pointblock;
         if (ncap > pphys) {
+#ifdef GQM_TEST_TIGHT_BUFFERS
+          int rc = alloc_points(ncap);
+#else
           int rc = alloc_points(std::max(ncap, pphys + pphys / 2));
+#endif
           if (rc) return rc;
         }
         pcap = ncap;
@@ -385,7 +403,11 @@ struct Refiner {
       if (num) {
         long ncap = tcap + num * triblock;
         if (ncap > tphys) {
+#ifdef GQM_TEST_TIGHT_BUFFERS
+          int rc = alloc_tris(ncap);
+#else
           int rc = alloc_tris(std::max(ncap, tphys + tphys / 2));
+#endif
           if (rc) return rc;
         }
         tcap = ncap;
@@ -581,10 +603,19 @@ struct Refiner {
     triblock = 2 * pointblock;
     pcap = np + pointblock;
     tcap = nt + triblock;
+#ifdef GQM_TEST_TIGHT_BUFFERS
+    // test builds: physical buffers exactly the logical capacity, so every
+    // growth step goes through the reallocation path
+    rc = alloc_points(std::max<long>(pcap, pphys));
+    if (rc) return rc;
+    rc = alloc_tris(std::max<long>(tcap, tphys));
+    if (rc) return rc;
+#else
     rc = alloc_points(std::max<long>(pcap + 3L * pointblock, pphys));
     if (rc) return rc;
     rc = alloc_tris(std::max<long>(tcap + 4L * triblock, tphys));
     if (rc) return rc;
+#endif
     rc = alloc_subsegs(std::max<long>(4L * ns + 1024, sphys));
     if (rc) return rc;
     // inputs
@@ -627,7 +658,7 @@ struct Refiner {
     cudaMemsetAsync(M.err, 0, sizeof(int), st);
     cudaMemsetAsync(dctr, 0, sizeof(unsigned long long) * 4, st);
     // cos^2(theta) on the device, as the reference evaluates it
-    k_goodcos<<<1, 32, 0, st>>>(theta, dgc);
+    KL(k_goodcos, 1, 32)(theta, dgc);
     double hgc[2];
     cudaMemcpyAsync(hgc, dgc, sizeof(double) * 2, cudaMemcpyDeviceToHost, st);
     cudaStreamSynchronize(st);

@@ -1,0 +1,132 @@
+// Test-only stand-in for the CUDA runtime, used to compile the refiner's own
+// sources (gpu_cdt_refine_b200/csrc/refine.cu) as host C++ so that their index
+// arithmetic and results can be checked on a machine without a GPU.  Kernels
+// run as ordinary functions with one thread covering every element of its
+// grid-stride loop.  Never linked into the product library.
+#pragma once
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+
+#define GQM_HOST_EMU 1
+#define __global__
+#define __device__
+#define __host__
+#define __forceinline__ inline
+#define __noinline__
+#define __shared__ static
+#define __launch_bounds__(...)
+
+struct dim3_emu {
+  unsigned x, y, z;
+};
+static dim3_emu threadIdx = {0, 0, 0}, blockIdx = {0, 0, 0}, blockDim = {1, 1, 1}, gridDim = {1, 1, 1};
+
+struct int2 {
+  int x, y;
+};
+struct int4 {
+  int x, y, z, w;
+};
+struct double2 {
+  double x, y;
+};
+inline int4 make_int4(int a, int b, int c, int d) { return int4{a, b, c, d}; }
+inline int2 make_int2(int a, int b) { return int2{a, b}; }
+inline double2 make_double2(double a, double b) { return double2{a, b}; }
+using std::max;
+using std::min;
+
+inline int atomicMin(int *a, int v) {
+  int o = *a;
+  if (v < o) *a = v;
+  return o;
+}
+inline int atomicMax(int *a, int v) {
+  int o = *a;
+  if (v > o) *a = v;
+  return o;
+}
+inline unsigned long long atomicMax(unsigned long long *a, unsigned long long v) {
+  unsigned long long o = *a;
+  if (v > o) *a = v;
+  return o;
+}
+inline unsigned long long atomicCAS(unsigned long long *a, unsigned long long c, unsigned long long v) {
+  unsigned long long o = *a;
+  if (o == c) *a = v;
+  return o;
+}
+inline int atomicCAS(int *a, int c, int v) {
+  int o = *a;
+  if (o == c) *a = v;
+  return o;
+}
+inline unsigned long long atomicAdd(unsigned long long *a, unsigned long long v) {
+  unsigned long long o = *a;
+  *a += v;
+  return o;
+}
+inline void __syncthreads() {}
+inline int __shfl_down_sync(unsigned, int v, int) { return v; }
+inline unsigned __ballot_sync(unsigned, bool p) { return p ? 1u : 0u; }
+inline int __popc(unsigned v) { return __builtin_popcount(v); }
+
+typedef int cudaError_t;
+typedef void *cudaStream_t;
+typedef std::chrono::steady_clock::time_point *cudaEvent_t;
+enum { cudaSuccess = 0, cudaErrorMemoryAllocation = 2 };
+enum cudaMemcpyKind { cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, cudaMemcpyDeviceToDevice };
+#define cudaStreamNonBlocking 1
+
+inline cudaError_t cudaMalloc(void **p, size_t n) {
+  *p = calloc(1, n ? n : 1);
+  return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+inline cudaError_t cudaMallocHost(void **p, size_t n) { return cudaMalloc(p, n); }
+inline cudaError_t cudaFree(void *p) {
+  free(p);
+  return cudaSuccess;
+}
+inline cudaError_t cudaFreeHost(void *p) { return cudaFree(p); }
+inline cudaError_t cudaMemcpyAsync(void *d, const void *s, size_t n, cudaMemcpyKind, cudaStream_t = nullptr) {
+  memmove(d, s, n);
+  return cudaSuccess;
+}
+inline cudaError_t cudaMemcpy(void *d, const void *s, size_t n, cudaMemcpyKind k) { return cudaMemcpyAsync(d, s, n, k); }
+inline cudaError_t cudaMemsetAsync(void *d, int v, size_t n, cudaStream_t = nullptr) {
+  memset(d, v, n);
+  return cudaSuccess;
+}
+inline cudaError_t cudaStreamCreateWithFlags(cudaStream_t *s, int) {
+  *s = (void *)1;
+  return cudaSuccess;
+}
+inline cudaError_t cudaStreamDestroy(cudaStream_t) { return cudaSuccess; }
+inline cudaError_t cudaStreamSynchronize(cudaStream_t) { return cudaSuccess; }
+inline cudaError_t cudaSetDevice(int) { return cudaSuccess; }
+inline cudaError_t cudaGetDeviceCount(int *n) {
+  *n = 1;
+  return cudaSuccess;
+}
+inline cudaError_t cudaEventCreate(cudaEvent_t *e) {
+  *e = new std::chrono::steady_clock::time_point();
+  return cudaSuccess;
+}
+inline cudaError_t cudaEventDestroy(cudaEvent_t e) {
+  delete e;
+  return cudaSuccess;
+}
+inline cudaError_t cudaEventRecord(cudaEvent_t e, cudaStream_t = nullptr) {
+  *e = std::chrono::steady_clock::now();
+  return cudaSuccess;
+}
+inline cudaError_t cudaEventElapsedTime(float *ms, cudaEvent_t a, cudaEvent_t b) {
+  *ms = std::chrono::duration<float, std::milli>(*b - *a).count();
+  return cudaSuccess;
+}
+inline cudaError_t cudaGetLastError() { return cudaSuccess; }
+inline const char *cudaGetErrorString(cudaError_t) { return "emulated"; }
