@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "../../include/gqm_refine.h"
@@ -876,9 +877,125 @@ const char *gqm_status_string(int s) {
     case GQM_ERR_CUDA: return "CUDA runtime error";
     case GQM_ERR_NO_DEVICE: return "no CUDA device";
     case GQM_ERR_MEMORY: return "device allocation failed";
+    case GQM_ERR_TOO_LARGE: return "result larger than the no-allocation staging array";
     default: return "unknown status";
   }
 }
 int gqm_version(void) { return 100; }
 
 }  // extern "C"
+
+// ============================================================================
+// Result copy without allocation (gqm_context_result_noalloc).
+//
+// For callers that cannot allocate at the time they read a result: a service
+// with a device memory budget fixed at start-up that reads many small results
+// in a loop, or code sharing the GPU with work that must not be stalled by the
+// device-wide synchronization cudaFree implies.  The kernel below is the
+// result-emission kernel of gqm_context_result() staging into a statically
+// allocated device array instead of per-call cudaMalloc buffers; the caller
+// provides the host arrays.
+// ============================================================================
+namespace gqm {
+
+constexpr int kNoAllocRows = GQM_NOALLOC_MAX_ELEMENTS;
+// Staging layout (bytes): triangles 3 ints, neighbours 3 ints, segments
+// 2 ints, triangle status 1 byte, point status 1 byte per row.
+constexpr size_t kNoAllocTri = 0;
+constexpr size_t kNoAllocNbr = kNoAllocTri + sizeof(int) * 3 * kNoAllocRows;
+constexpr size_t kNoAllocSeg = kNoAllocNbr + sizeof(int) * 3 * kNoAllocRows;
+constexpr size_t kNoAllocTs = kNoAllocSeg + sizeof(int) * 2 * kNoAllocRows;
+constexpr size_t kNoAllocPs = kNoAllocTs + (size_t)kNoAllocRows;
+constexpr size_t kNoAllocBytes = kNoAllocPs + (size_t)kNoAllocRows;
+
+// One array per device, held until the process exits; shared by every call.
+static __device__ __align__(256) unsigned char g_noalloc_staging[kNoAllocBytes];
+
+// Device address of g_noalloc_staging per device ordinal.  In host code the
+// array's name is only a host-side handle, so the address is looked up once
+// per device, with that device current, and then passed to the kernel.
+static unsigned char *g_noalloc_addr[64];
+static bool g_noalloc_ready[64];
+static std::mutex g_noalloc_mutex;
+
+static int noalloc_staging(int device, unsigned char **p) {
+  if (device < 0 || device >= 64) return GQM_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_ready[device]) {
+    void *addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_staging);
+    if (e != cudaSuccess || addr == nullptr) return GQM_ERR_CUDA;
+    g_noalloc_addr[device] = (unsigned char *)addr;
+    g_noalloc_ready[device] = true;
+  }
+  *p = g_noalloc_addr[device];
+  return GQM_OK;
+}
+
+// k_emit_output / k_emit_pstatus writing into the staging array.  Every row
+// that is copied out is written first, so nothing has to start at zero.
+__global__ void k_emit_output_staged(Mesh M, int np, int nt, int ns, unsigned char *stage) {
+  int *tri = reinterpret_cast<int *>(stage + kNoAllocTri);
+  int *nbr = reinterpret_cast<int *>(stage + kNoAllocNbr);
+  int *seg = reinterpret_cast<int *>(stage + kNoAllocSeg);
+  uint8_t *ts = stage + kNoAllocTs;
+  uint8_t *ps = stage + kNoAllocPs;
+  GS_LOOP(i, max(max(nt, ns), np)) {
+    if (i < nt) {
+      int4 v = M.tv[i], nb = M.tn[i];
+      tri[3 * i] = v.x;
+      tri[3 * i + 1] = v.y;
+      tri[3 * i + 2] = v.z;
+      nbr[3 * i] = dtri(nb.x);
+      nbr[3 * i + 1] = dtri(nb.y);
+      nbr[3 * i + 2] = dtri(nb.z);
+      ts[i] = (uint8_t)((M.tst[i] & 7) | (M.tflip[i] ? 8 : 0) | (M.tfo[i] << 4));
+    }
+    if (i < ns) {
+      int o = s2t_get(M, i);
+      if (o < 0) {
+        seg[2 * i] = seg[2 * i + 1] = -1;
+      } else {
+        int4 v = M.tv[dtri(o)];
+        int r = dori(o);
+        seg[2 * i] = comp(v, m3(r + 1));
+        seg[2 * i + 1] = comp(v, m3(r + 2));
+      }
+    }
+    if (i < np) ps[i] = (uint8_t)((M.ps[i] & 15) | (M.pred[i] ? 16 : 0));
+  }
+}
+
+}  // namespace gqm
+
+extern "C" int gqm_context_result_noalloc(gqm_context *ctx, gqm_cdt_out *out) {
+  if (!ctx || !out || !ctx->r.have_result) return GQM_ERR_ARGUMENT;
+  gqm::Refiner &R = ctx->r;
+  int np = R.out_np, nt = R.out_nt, ns = R.out_ns;
+  if (np > gqm::kNoAllocRows || nt > gqm::kNoAllocRows || ns > gqm::kNoAllocRows) return GQM_ERR_TOO_LARGE;
+  if (!out->pointlist || !out->trianglelist || !out->neighborlist || !out->segmentlist || !out->pstatus ||
+      !out->tstatus)
+    return GQM_ERR_ARGUMENT;
+  if (cudaSetDevice(R.device) != cudaSuccess) return GQM_ERR_CUDA;
+  unsigned char *stage = nullptr;
+  int rc = gqm::noalloc_staging(R.device, &stage);
+  if (rc) return rc;
+  cudaStream_t st = R.st;
+  int work = std::max(std::max(nt, ns), np);
+  KL(gqm::k_emit_output_staged, gqm::Refiner::grid_for(work), 256)(R.M, np, nt, ns, stage);
+  if (cudaGetLastError() != cudaSuccess) return GQM_ERR_CUDA;
+  cudaMemcpyAsync(out->pointlist, R.M.pts, sizeof(double) * 2 * (size_t)np, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(out->trianglelist, stage + gqm::kNoAllocTri, sizeof(int) * 3 * (size_t)nt,
+                  cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(out->neighborlist, stage + gqm::kNoAllocNbr, sizeof(int) * 3 * (size_t)nt,
+                  cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(out->segmentlist, stage + gqm::kNoAllocSeg, sizeof(int) * 2 * (size_t)ns,
+                  cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(out->tstatus, stage + gqm::kNoAllocTs, (size_t)nt, cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(out->pstatus, stage + gqm::kNoAllocPs, (size_t)np, cudaMemcpyDeviceToHost, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_ERR_CUDA;
+  out->numberofpoints = np;
+  out->numberoftriangles = nt;
+  out->numberofsegments = ns;
+  return GQM_OK;
+}

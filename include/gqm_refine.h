@@ -115,6 +115,32 @@ int gqm_context_result_sizes(gqm_context *ctx, int *npoints, int *ntriangles, in
 /* The CUDA stream the context launches on (a cudaStream_t). */
 void *gqm_context_stream(gqm_context *ctx);
 
+/* Copy the last result of `ctx` into arrays the caller already owns, without
+ * allocating any memory, host or device.
+ *
+ * No counterpart in the reference: its result path always allocates (new[] on
+ * the host, device_vector on the GPU).  gqm_context_result() above also
+ * allocates: it mallocs the host arrays and cudaMallocs device staging buffers
+ * for every call, and cudaFree synchronizes the whole device.  Callers that
+ * cannot do that - a service that fixes its device memory budget at start-up
+ * and reads many small results in a steady-state loop, or code sharing the GPU
+ * with work that must not be stalled by an implicit device-wide sync - use
+ * this entry point instead.
+ *
+ * The caller fills out->pointlist, trianglelist, neighborlist, segmentlist,
+ * pstatus and tstatus with buffers sized from gqm_context_result_sizes(); the
+ * counts are written back.  Staging goes through one statically allocated
+ * device array of GQM_NOALLOC_MAX_ELEMENTS rows (about 4.4 MB), which every GPU
+ * that loads the library holds until the process exits.  A result with more
+ * points, triangles or segments than GQM_NOALLOC_MAX_ELEMENTS is rejected with
+ * GQM_ERR_TOO_LARGE.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  All calls on one device share the array, so calls that overlap on
+ * the GPU (from different host threads or contexts) race; serialize them. */
+#define GQM_NOALLOC_MAX_ELEMENTS 131072
+#define GQM_ERR_TOO_LARGE (-13)
+int gqm_context_result_noalloc(gqm_context *ctx, gqm_cdt_out *out);
+
 const char *gqm_status_string(int status);
 int gqm_version(void);
 

@@ -19,6 +19,7 @@
 #define __noinline__
 #define __shared__ static
 #define __launch_bounds__(...)
+#define __align__(n) __attribute__((aligned(n)))
 
 struct dim3_emu {
   unsigned x, y, z;
@@ -130,3 +131,8 @@ inline cudaError_t cudaEventElapsedTime(float *ms, cudaEvent_t a, cudaEvent_t b)
 }
 inline cudaError_t cudaGetLastError() { return cudaSuccess; }
 inline const char *cudaGetErrorString(cudaError_t) { return "emulated"; }
+template <class T>
+inline cudaError_t cudaGetSymbolAddress(void **p, T &sym) {
+  *p = (void *)&sym;
+  return cudaSuccess;
+}
