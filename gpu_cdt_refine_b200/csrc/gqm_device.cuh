@@ -38,6 +38,7 @@ struct Mesh {
   uint8_t *tst, *tflip, *tfo, *flip0;
   int *tmark;
   int *tpos;  // winner-slot of each triangle during a flip step
+  int *fstamp, *tstamp;  // per-triangle generation stamps deduplicating the flip-step queues
   unsigned long long *s2t;
   int *s2seg, *enc;
   const int2 *segs;

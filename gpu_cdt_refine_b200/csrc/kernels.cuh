@@ -266,187 +266,7 @@ __device__ void mark_fan(const Mesh &M, int triIndex, int triOri) {
   } while (cur > -1 && cur != triIndex);
 }
 
-__global__ void k_flip_init(Mesh M, int ntri) {
-  GS_LOOP(t, ntri) {
-    M.tmark[t] = kMaxInt;
-    M.tfo[t] = 15;
-    M.flip0[t] = M.tflip[t];
-  }
-}
-
 __device__ __forceinline__ bool is_red(const Mesh &M, int p) { return M.pred[p] != 0; }
-
-// kernelCheckFlipping, refine.cu:778-1070.  Neighbour flip flags are read from
-// flip0, the state at kernel start.
-template <int PRED>
-__global__ void k_check_flip(Mesh M, const int *act, const int *dn) {
-  int n = *dn;
-  GS_LOOP(k, n) {
-    int index = act[k];
-    int4 p = M.tv[index];
-    int4 nb = M.tn[index];
-    int4 sg = M.tsg[index];
-    int pp[3] = {p.x, p.y, p.z};
-    int mn = kMaxInt;
-    for (int i = 0; i < 3; ++i)
-      if (is_red(M, pp[i]) && pp[i] < mn) mn = pp[i];
-    double2 v[3] = {M.pts[p.x], M.pts[p.y], M.pts[p.z]};
-    bool done = false;
-    for (int i = 0; i < 3 && !done; i++) {
-      if (mn == pp[i]) continue;
-      if (comp(sg, i) != -1) continue;
-      int tri = comp(nb, i);
-      int pTri = dtri(tri), pOri = dori(tri);
-      if (!(index < pTri || (pTri >= 0 && !M.flip0[pTri]))) continue;
-      int pOpp = ld1(M.tv, pTri, pOri);
-      if (is_red(M, pOpp) && pOpp < mn) continue;
-      double2 vOpp = M.pts[pOpp];
-      int org = m3(i + 1), dest = m3(i + 2), apex = i;
-      if (mn != kMaxInt) {
-        int deleteOri, n1, n2;
-        if (mn == pp[org]) {
-          deleteOri = m3(i + 2);
-          n1 = comp(nb, dest);
-          n2 = ld1(M.tn, pTri, m3(pOri + 1));
-        } else {
-          deleteOri = i;
-          n1 = comp(nb, org);
-          n2 = ld1(M.tn, pTri, m3(pOri + 2));
-        }
-        if (dtri(n1) == dtri(n2)) {  // 3-1 flip
-          M.tfo[index] = (uint8_t)(3 + deleteOri);
-          atomicMin(M.tmark + index, index);
-          atomicMin(M.tmark + pTri, index);
-          if (dtri(n1) >= 0) atomicMin(M.tmark + dtri(n1), index);
-          done = true;
-          break;
-        } else {
-          int n1_tri = dtri(n1), n1_ori = dori(n1), n2_tri = dtri(n2), n2_ori = dori(n2);
-          int n1_pOpp = ld1(M.tv, n1_tri, n1_ori), n2_pOpp = ld1(M.tv, n2_tri, n2_ori);
-          double2 n1_vOpp = M.pts[n1_pOpp], n2_vOpp = M.pts[n2_pOpp];
-          int n3 = (mn == pp[org]) ? ld1(M.tn, n1_tri, m3(n1_ori + 2)) : ld1(M.tn, n1_tri, m3(n1_ori + 1));
-          if (dtri(n3) == dtri(n2)) {
-            bool four = false;
-            if (mn == pp[org]) {
-              double d = orient<PRED>(v[apex], v[org], vOpp);
-              if (d == 0) {
-                double t0 = orient<PRED>(v[dest], v[apex], n1_vOpp);
-                double t1 = orient<PRED>(v[dest], v[org], n1_vOpp);
-                bool f0 = (t0 > 0 && t1 < 0);
-                t0 = orient<PRED>(v[dest], v[org], n2_vOpp);
-                t1 = orient<PRED>(v[dest], vOpp, n2_vOpp);
-                bool f1 = (t0 > 0 && t1 < 0);
-                four = (!f0 && !f1);
-              }
-            } else {
-              double d = orient<PRED>(v[apex], v[dest], vOpp);
-              if (d == 0) {
-                double t0 = orient<PRED>(v[org], v[dest], n1_vOpp);
-                double t1 = orient<PRED>(v[org], v[apex], n1_vOpp);
-                bool f0 = (t0 > 0 && t1 < 0);
-                t0 = orient<PRED>(v[org], vOpp, n2_vOpp);
-                t1 = orient<PRED>(v[org], v[dest], n2_vOpp);
-                bool f1 = (t0 > 0 && t1 < 0);
-                four = (!f0 && !f1);
-              }
-            }
-            if (four) {
-              if (is_red(M, n1_pOpp) && n1_pOpp < mn) continue;
-              M.tfo[index] = (uint8_t)(6 + i);
-              atomicMin(M.tmark + index, index);
-              atomicMin(M.tmark + pTri, index);
-              atomicMin(M.tmark + n1_tri, index);
-              atomicMin(M.tmark + n2_tri, index);
-              done = true;
-              break;
-            }
-          }
-        }
-        double t1 = orient<PRED>(v[apex], v[org], vOpp);
-        if (t1 <= 0) continue;
-        double t2 = orient<PRED>(v[apex], v[dest], vOpp);
-        if (t2 >= 0) continue;
-        M.tfo[index] = (uint8_t)m3(i + 2);
-        atomicMin(M.tmark + index, index);
-        atomicMin(M.tmark + pTri, index);
-        done = true;
-        break;
-      }
-      double ret = incircle<PRED>(v[apex], v[org], v[dest], vOpp);
-      double ret_opp = incircle<PRED>(v[org], vOpp, v[dest], v[apex]);
-      double ret_after = incircle<PRED>(v[apex], v[org], vOpp, v[dest]);
-      double ret_after_opp = incircle<PRED>(vOpp, v[dest], v[apex], v[org]);
-      if (ret > 0 && ret_opp > 0 && ret_after < 0 && ret_after_opp < 0) {
-        // deleteOneFromTwo, refine.cu:733-757
-        int pa = pp[apex];
-        uint8_t sa = M.ps[pa], so = M.ps[pOpp];
-        int td = -1;
-        if ((sa & PS_SEGSPLIT) && (so & PS_SEGSPLIT))
-          td = -1;
-        else if ((sa & PS_NEW) && (so & PS_NEW)) {
-          if (sa & PS_SEGSPLIT)
-            td = 1;
-          else if (so & PS_SEGSPLIT)
-            td = 0;
-          else
-            td = pa < pOpp ? 1 : 0;
-        }
-        if (td == -1) {
-          M.tfo[index] = (uint8_t)m3(i + 2);
-          atomicMin(M.tmark + index, index);
-          atomicMin(M.tmark + pTri, index);
-        } else if (td == 0) {
-          atomicMin(M.tmark + index, negate_idx(etri(index, m3(i + 2))));
-        } else {
-          int tv2 = negate_idx(etri(pTri, m3(pOri + 2)));
-          atomicMin(M.tmark + index, tv2);
-          atomicMin(M.tmark + pTri, tv2);
-        }
-        done = true;
-        break;
-      }
-    }
-    if (!done) M.tflip[index] = 0;
-  }
-}
-
-// kernelMarkFlipWinner, refine.cu:1072-1170
-__global__ void k_flip_winner(Mesh M, const int *act, const int *dn) {
-  int n = *dn;
-  GS_LOOP(k, n) {
-    int index = act[k];
-    int ori = M.tfo[index];
-    if (ori == 15) continue;
-    bool win = false;
-    if (M.tmark[index] == index) {
-      if (ori < 3) {
-        int pOppTri = dtri(ld1(M.tn, index, m3(ori + 1)));
-        win = (M.tmark[pOppTri] == index);
-      } else if (ori < 6) {
-        ori = m3(ori - 3 + 1);
-        int t1 = dtri(ld1(M.tn, index, ori)), t2 = dtri(ld1(M.tn, index, m3(ori + 2)));
-        win = (t1 < 0 || M.tmark[t1] == index) && (t2 < 0 || M.tmark[t2] == index);
-      } else {
-        ori -= 6;
-        int pOpp = ld1(M.tn, index, ori);
-        int pOppTri = dtri(pOpp), pOppOri = dori(pOpp);
-        int pOrg = ld1(M.tv, index, m3(ori + 1)), pDest = ld1(M.tv, index, m3(ori + 2));
-        int t1, t2;
-        if (is_red(M, pOrg) && (!is_red(M, pDest) || pOrg < pDest)) {
-          t1 = ld1(M.tn, index, m3(ori + 2));
-          t2 = ld1(M.tn, pOppTri, m3(pOppOri + 1));
-        } else {
-          t1 = ld1(M.tn, index, m3(ori + 1));
-          t2 = ld1(M.tn, pOppTri, m3(pOppOri + 2));
-        }
-        t1 = dtri(t1);
-        t2 = dtri(t2);
-        win = (M.tmark[pOppTri] == index && M.tmark[t1] == index && M.tmark[t2] == index);
-      }
-    }
-    if (!win) M.tfo[index] = 15;
-  }
-}
 
 // Direction of a 4-2 flip, recomputed from the partner's current vertices
 // (refine.cu:1232-1250, 1740-1758, 2120-2138).
@@ -462,10 +282,8 @@ __device__ __forceinline__ bool flip42_outward(const Mesh &M, int pOppTri, int p
 // kernelInitLinklist, refine.cu:1172-1278.  Besides the winner's triangle
 // list, each listed triangle records its list slot in tpos so that phase 2
 // finds it directly instead of by binary search over the winners.
-__global__ void k_init_link(Mesh M, const int *win, const int *dn, int *ll) {
-  int n = *dn;
-  GS_LOOP(pos, n) {
-    int index = win[pos];
+__device__ void init_link_body(const Mesh &M, int pos, int index, int *ll) {
+  {
     int ori = M.tfo[index];
     int l[4] = {index, -1, -1, -1};
     if (ori < 3) {
@@ -510,10 +328,8 @@ __device__ __forceinline__ void set_link(int *sl, int nOrg, int nDest, int nApex
 }
 
 // kernelUpdatePhase1, refine.cu:1295-1552
-__global__ void k_phase1(Mesh M, const int *win, const int *dn, int *sl, uint32_t epoch) {
-  int n = *dn;
-  GS_LOOP(pos, n) {
-    int index = win[pos];
+__device__ void phase1_body(const Mesh &M, int pos, int index, int *sl, uint32_t epoch) {
+  {
     int ori = M.tfo[index];
     if (ori < 3) {
       int pOpp = ld1(M.tn, index, m3(ori + 1));
@@ -746,10 +562,9 @@ __device__ __forceinline__ int unlink_slot(const Mesh &M, int v, int newlink) {
 }
 
 // kernelUpdatePhase3, refine.cu:1924-2296
-__global__ void k_phase3(Mesh M, const int *win, const int *dn, const int *sl) {
-  int n = *dn;
-  GS_LOOP(pos, n) {
-    int index = win[pos];
+template <class SetFlag>
+__device__ void phase3_body(const Mesh &M, int pos, int index, const int *sl, const SetFlag &set_flag) {
+  {
     int ori = M.tfo[index];
     M.tfo[index] = 15;
     if (ori < 3) {
@@ -778,7 +593,7 @@ __global__ void k_phase3(Mesh M, const int *win, const int *dn, const int *sl) {
       if (sDest != -1) reset_encseg(M, sDest, (index << 2) | m3(ori + 1), -npDest);
       if (spOrg != -1) reset_encseg(M, spOrg, (pOppTri << 2) | pOppOri, -nApex);
       if (spApex != -1) reset_encseg(M, spApex, (pOppTri << 2) | m3(pOppOri + 2), -npApex);
-      M.tflip[pOppTri] = 1;
+      set_flag(pOppTri);
     } else if (ori < 6) {
       ori = m3(ori - 3 + 1);
       int t1 = ld1(M.tn, index, ori), t2 = ld1(M.tn, index, m3(ori + 2));
@@ -856,26 +671,13 @@ __global__ void k_phase3(Mesh M, const int *win, const int *dn, const int *sl) {
         if (spDest != -1) reset_encseg(M, spDest, (t1 << 2) | m3(t1_ori + 1), -npDest);
         if (spApex != -1) reset_encseg(M, spApex, (t1 << 2) | m3(t1_ori + 2), -npApex);
       }
-      M.tflip[t1] = 1;
+      set_flag(t1);
       M.tflip[pOppTri] = 0;
       M.tflip[t2] = 0;
     }
   }
 }
 
-// kernelMarkReduntantSteiner, refine.cu:2298-2326
-__global__ void k_mark_red_steiner(Mesh M, const int *neg, const int *dn) {
-  int n = *dn;
-  GS_LOOP(k, n) {
-    int index = neg[k];
-    int otri = negate_idx(M.tmark[index]);
-    int triIndex = dtri(otri), triOri = dori(otri);
-    if (triIndex != index) M.tflip[index] = 1;
-    int p = ld1(M.tv, triIndex, m3(triOri + 1));
-    M.pred[p] = 1;
-    mark_fan(M, triIndex, triOri);
-  }
-}
 
 // kernelMarkReduantPoints, refine.cu:604-677
 __global__ void k_mark_redundant(Mesh M, int *delmarker, const int *dellist, const int *dn) {
@@ -910,6 +712,377 @@ __global__ void k_mark_redundant(Mesh M, int *delmarker, const int *dellist, con
       }
     }
     delmarker[pos] = out;
+  }
+}
+
+// ============================================================================
+// Flip-flop driven by active sets.  The reference rescans every triangle slot
+// several times per flip step (refine.cu:2356-2489).  Here a step works on
+//   A : the triangles whose flip flag is set (built from queue Q),
+//   T : the triangles claimed in the step (tmark reset at the next step),
+//   W : the winners,
+// and every flag set during a step pushes its triangle onto the next queue,
+// deduplicated by a generation stamp.  The per-triangle results are the
+// reference's: no kernel below depends on the order of its list.
+// ============================================================================
+// Control block of a flip-flop loop, resident on the device so that the loop
+// can run as a CUDA graph with a device-side condition.
+struct FlipCtl {
+  int gen;          // generation of the stamps of the current step
+  unsigned epoch;   // launch epoch of the subseg2tri stores (all kernels share it)
+  int nact;         // |A|
+  int winn;         // |W|
+  int qn;           // length of the next queue
+  int tn;           // number of claimed triangles
+  int steps;        // flip steps executed (all loops)
+  int entry_steps;  // steps at entry of the current loop
+  int cap_hit;      // the step bound stopped a loop
+  int cond;         // loop condition of the last step
+  long long cap;    // bound on the steps of one loop
+  int *errp;        // device error word (GQM_ERR_ROUND_LIMIT on cap_hit)
+};
+struct FlipQ {
+  int *q;           // next queue
+  int *qn;          // its length
+  const int *genp;  // generation of the next queue
+};
+__device__ __forceinline__ void push_flag(const Mesh &M, const FlipQ &Q, int t) {
+  M.tflip[t] = 1;
+  int g = *Q.genp;
+  if (atomicExch(M.fstamp + t, g) != g) Q.q[atomicAdd(Q.qn, 1)] = t;
+}
+struct TouchL {
+  int *l;
+  int *n;
+  const int *genp;
+};
+__device__ __forceinline__ void touch(const Mesh &M, const TouchL &T, int t) {
+  int g = *T.genp;
+  if (atomicExch(M.tstamp + t, g) != g) T.l[atomicAdd(T.n, 1)] = t;
+}
+__device__ __forceinline__ void claim(const Mesh &M, const TouchL &T, int t, int v) {
+  atomicMin(M.tmark + t, v);
+  touch(M, T, t);
+}
+
+// Loop condition of a flip-flop step (refine.cu:2489: continue while any
+// triangle is flagged), with a bound on the steps of one loop.  On continue,
+// the counters of the next step are prepared here.
+__device__ __forceinline__ int flip_next(FlipCtl *c) {
+  int cond = c->nact > 0;
+  if (cond && (long long)(c->steps - c->entry_steps) >= c->cap) {
+    cond = 0;
+    c->cap_hit = 1;
+    atomicCAS(c->errp, 0, -2);
+  }
+  if (cond) {
+    c->gen++;
+    c->epoch++;
+    c->winn = 0;
+    c->qn = 0;
+    c->tn = 0;
+    c->steps++;
+  }
+  c->cond = cond;
+  return cond;
+}
+#ifdef GQM_HOST_EMU
+typedef int cudaGraphConditionalHandle;
+#endif
+__global__ void k_flip_prep(FlipCtl *c, cudaGraphConditionalHandle h, int use_graph) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    c->entry_steps = c->steps;
+    int cond = flip_next(c);
+#ifndef GQM_HOST_EMU
+    if (use_graph) cudaGraphSetConditional(h, cond);
+#endif
+    (void)cond;
+    (void)use_graph;
+    (void)h;
+  }
+}
+__global__ void k_flip_cond(FlipCtl *c, cudaGraphConditionalHandle h, int use_graph) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    int cond = flip_next(c);
+#ifndef GQM_HOST_EMU
+    if (use_graph) cudaGraphSetConditional(h, cond);
+#endif
+    (void)cond;
+    (void)use_graph;
+    (void)h;
+  }
+}
+__global__ void k_bump_epoch(FlipCtl *c) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) c->epoch++;
+}
+// per-run reset of the control block; gen and epoch keep growing across runs
+// so that stamps and subseg2tri tags left by earlier runs never collide
+__global__ void k_ctl_reset(FlipCtl *c, long long cap, int *errp) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    c->steps = 0;
+    c->entry_steps = 0;
+    c->cap_hit = 0;
+    c->cond = 0;
+    c->cap = cap;
+    c->errp = errp;
+  }
+}
+
+
+// reset tmark / tfo before the first step of a flip-flop
+__global__ void k_flip_entry_reset(Mesh M, int ntri) {
+  GS_LOOP(t, ntri) {
+    M.tmark[t] = kMaxInt;
+    M.tfo[t] = 15;
+  }
+}
+// A = queue entries whose flag is still set on a live triangle
+__global__ void k_flip_filter(Mesh M, const int *q, const int *qn, int *act, int *actn) {
+  int n = *qn;
+  GS_LOOP(k, n) {
+    int t = q[k];
+    if (M.tflip[t] && (M.tst[t] & TS_NOTNULL)) act[atomicAdd(actn, 1)] = t;
+  }
+}
+// tmark of the triangles claimed in this step back to "unclaimed"; also
+// empties A for the filter that follows (A is not read after the winners).
+__global__ void k_flip_reset_touched(Mesh M, const int *tl, const int *tn, int *nact) {
+  int n = *tn;
+  GS_LOOP(k, n) M.tmark[tl[k]] = kMaxInt;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *nact = 0;
+}
+
+// kernelCheckFlipping (refine.cu:778-1070) on A.  No flag is cleared here
+// (the decision is kept in clr[k] and applied by k_flip_winner2), so the
+// neighbour flags read below are the ones the step started with.
+template <int PRED>
+__global__ void k_check_flip2(Mesh M, const int *act, const int *dn, uint8_t *clr, TouchL T) {
+  int n = *dn;
+  GS_LOOP(k, n) {
+    int index = act[k];
+    int4 p = M.tv[index];
+    int4 nb = M.tn[index];
+    int4 sg = M.tsg[index];
+    int pp[3] = {p.x, p.y, p.z};
+    int mn = kMaxInt;
+    for (int i = 0; i < 3; ++i)
+      if (is_red(M, pp[i]) && pp[i] < mn) mn = pp[i];
+    double2 v[3] = {M.pts[p.x], M.pts[p.y], M.pts[p.z]};
+    bool done = false;
+    for (int i = 0; i < 3 && !done; i++) {
+      if (mn == pp[i]) continue;
+      if (comp(sg, i) != -1) continue;
+      int tri = comp(nb, i);
+      int pTri = dtri(tri), pOri = dori(tri);
+      if (!(index < pTri || (pTri >= 0 && !M.tflip[pTri]))) continue;
+      int pOpp = ld1(M.tv, pTri, pOri);
+      if (is_red(M, pOpp) && pOpp < mn) continue;
+      double2 vOpp = M.pts[pOpp];
+      int org = m3(i + 1), dest = m3(i + 2), apex = i;
+      if (mn != kMaxInt) {
+        int deleteOri, n1, n2;
+        if (mn == pp[org]) {
+          deleteOri = m3(i + 2);
+          n1 = comp(nb, dest);
+          n2 = ld1(M.tn, pTri, m3(pOri + 1));
+        } else {
+          deleteOri = i;
+          n1 = comp(nb, org);
+          n2 = ld1(M.tn, pTri, m3(pOri + 2));
+        }
+        if (dtri(n1) == dtri(n2)) {  // 3-1 flip
+          M.tfo[index] = (uint8_t)(3 + deleteOri);
+          claim(M, T, index, index);
+          claim(M, T, pTri, index);
+          if (dtri(n1) >= 0) claim(M, T, dtri(n1), index);
+          done = true;
+          break;
+        } else {
+          int n1_tri = dtri(n1), n1_ori = dori(n1), n2_tri = dtri(n2), n2_ori = dori(n2);
+          int n1_pOpp = ld1(M.tv, n1_tri, n1_ori), n2_pOpp = ld1(M.tv, n2_tri, n2_ori);
+          double2 n1_vOpp = M.pts[n1_pOpp], n2_vOpp = M.pts[n2_pOpp];
+          int n3 = (mn == pp[org]) ? ld1(M.tn, n1_tri, m3(n1_ori + 2)) : ld1(M.tn, n1_tri, m3(n1_ori + 1));
+          if (dtri(n3) == dtri(n2)) {
+            bool four = false;
+            if (mn == pp[org]) {
+              double d = orient<PRED>(v[apex], v[org], vOpp);
+              if (d == 0) {
+                double t0 = orient<PRED>(v[dest], v[apex], n1_vOpp);
+                double t1 = orient<PRED>(v[dest], v[org], n1_vOpp);
+                bool f0 = (t0 > 0 && t1 < 0);
+                t0 = orient<PRED>(v[dest], v[org], n2_vOpp);
+                t1 = orient<PRED>(v[dest], vOpp, n2_vOpp);
+                bool f1 = (t0 > 0 && t1 < 0);
+                four = (!f0 && !f1);
+              }
+            } else {
+              double d = orient<PRED>(v[apex], v[dest], vOpp);
+              if (d == 0) {
+                double t0 = orient<PRED>(v[org], v[dest], n1_vOpp);
+                double t1 = orient<PRED>(v[org], v[apex], n1_vOpp);
+                bool f0 = (t0 > 0 && t1 < 0);
+                t0 = orient<PRED>(v[org], vOpp, n2_vOpp);
+                t1 = orient<PRED>(v[org], v[dest], n2_vOpp);
+                bool f1 = (t0 > 0 && t1 < 0);
+                four = (!f0 && !f1);
+              }
+            }
+            if (four) {
+              if (is_red(M, n1_pOpp) && n1_pOpp < mn) continue;
+              M.tfo[index] = (uint8_t)(6 + i);
+              claim(M, T, index, index);
+              claim(M, T, pTri, index);
+              claim(M, T, n1_tri, index);
+              claim(M, T, n2_tri, index);
+              done = true;
+              break;
+            }
+          }
+        }
+        double t1 = orient<PRED>(v[apex], v[org], vOpp);
+        if (t1 <= 0) continue;
+        double t2 = orient<PRED>(v[apex], v[dest], vOpp);
+        if (t2 >= 0) continue;
+        M.tfo[index] = (uint8_t)m3(i + 2);
+        claim(M, T, index, index);
+        claim(M, T, pTri, index);
+        done = true;
+        break;
+      }
+      double ret = incircle<PRED>(v[apex], v[org], v[dest], vOpp);
+      double ret_opp = incircle<PRED>(v[org], vOpp, v[dest], v[apex]);
+      double ret_after = incircle<PRED>(v[apex], v[org], vOpp, v[dest]);
+      double ret_after_opp = incircle<PRED>(vOpp, v[dest], v[apex], v[org]);
+      if (ret > 0 && ret_opp > 0 && ret_after < 0 && ret_after_opp < 0) {
+        int pa = pp[apex];
+        uint8_t sa = M.ps[pa], so = M.ps[pOpp];
+        int td = -1;
+        if ((sa & PS_SEGSPLIT) && (so & PS_SEGSPLIT))
+          td = -1;
+        else if ((sa & PS_NEW) && (so & PS_NEW)) {
+          if (sa & PS_SEGSPLIT)
+            td = 1;
+          else if (so & PS_SEGSPLIT)
+            td = 0;
+          else
+            td = pa < pOpp ? 1 : 0;
+        }
+        if (td == -1) {
+          M.tfo[index] = (uint8_t)m3(i + 2);
+          claim(M, T, index, index);
+          claim(M, T, pTri, index);
+        } else if (td == 0) {
+          claim(M, T, index, negate_idx(etri(index, m3(i + 2))));
+        } else {
+          int tv2 = negate_idx(etri(pTri, m3(pOri + 2)));
+          claim(M, T, index, tv2);
+          claim(M, T, pTri, tv2);
+        }
+        done = true;
+        break;
+      }
+    }
+    clr[k] = done ? 0 : 1;
+  }
+}
+
+// kernelMarkFlipWinner (refine.cu:1072-1170) on A; applies the deferred flag
+// clears, re-queues the triangles that keep their flag, collects winners.
+__global__ void k_flip_winner2(Mesh M, const int *act, const int *dn, const uint8_t *clr, FlipQ Q, int *win,
+                               int *winn) {
+  int n = *dn;
+  GS_LOOP(k, n) {
+    int index = act[k];
+    if (clr[k]) {
+      M.tflip[index] = 0;
+      continue;
+    }
+    push_flag(M, Q, index);
+    int ori = M.tfo[index];
+    if (ori == 15) continue;
+    bool w = false;
+    if (M.tmark[index] == index) {
+      if (ori < 3) {
+        int pOppTri = dtri(ld1(M.tn, index, m3(ori + 1)));
+        w = (M.tmark[pOppTri] == index);
+      } else if (ori < 6) {
+        int o = m3(ori - 3 + 1);
+        int t1 = dtri(ld1(M.tn, index, o)), t2 = dtri(ld1(M.tn, index, m3(o + 2)));
+        w = (t1 < 0 || M.tmark[t1] == index) && (t2 < 0 || M.tmark[t2] == index);
+      } else {
+        int o = ori - 6;
+        int pOpp = ld1(M.tn, index, o);
+        int pOppTri = dtri(pOpp), pOppOri = dori(pOpp);
+        int pOrg = ld1(M.tv, index, m3(o + 1)), pDest = ld1(M.tv, index, m3(o + 2));
+        int t1, t2;
+        if (is_red(M, pOrg) && (!is_red(M, pDest) || pOrg < pDest)) {
+          t1 = ld1(M.tn, index, m3(o + 2));
+          t2 = ld1(M.tn, pOppTri, m3(pOppOri + 1));
+        } else {
+          t1 = ld1(M.tn, index, m3(o + 1));
+          t2 = ld1(M.tn, pOppTri, m3(pOppOri + 2));
+        }
+        t1 = dtri(t1);
+        t2 = dtri(t2);
+        w = (M.tmark[pOppTri] == index && M.tmark[t1] == index && M.tmark[t2] == index);
+      }
+    }
+    if (w)
+      win[atomicAdd(winn, 1)] = index;
+    else
+      M.tfo[index] = 15;
+  }
+}
+
+// kernelInitLinklist + kernelUpdatePhase1 in one launch: each winner's list
+// setup reads only triangles the winner owns, before its own phase-1 writes.
+__global__ void k_link_phase1(Mesh M, const int *win, const int *dn, int *ll, int *sl, const unsigned *ep) {
+  int n = *dn;
+  uint32_t epoch = *ep;
+  GS_LOOP(pos, n) {
+    int index = win[pos];
+    init_link_body(M, pos, index, ll);
+    phase1_body(M, pos, index, sl, epoch);
+  }
+}
+
+// kernelUpdatePhase3 (refine.cu:1924-2296) with flags pushed onto the queue
+struct QueueFlag {
+  const Mesh *M;
+  const FlipQ *Q;
+  __device__ void operator()(int t) const { push_flag(*M, *Q, t); }
+};
+__global__ void k_phase3q(Mesh M, const int *win, const int *dn, const int *sl, FlipQ Q) {
+  int n = *dn;
+  QueueFlag f{&M, &Q};
+  GS_LOOP(pos, n) phase3_body(M, pos, win[pos], sl, f);
+}
+
+// kernelMarkReduntantSteiner (refine.cu:2298-2326) over the claimed triangles
+__device__ void mark_fan_q(const Mesh &M, const FlipQ &Q, int triIndex, int triOri) {
+  int cur = triIndex, ori = triOri, guard = 0;
+  do {
+    push_flag(M, Q, cur);
+    int nx = ld1(M.tn, cur, m3(ori + 2));
+    cur = dtri(nx);
+    ori = dori(nx);
+    if (++guard > (1 << 20)) {
+      raise_err(M, -4);
+      return;
+    }
+  } while (cur > -1 && cur != triIndex);
+}
+__global__ void k_mark_red_steiner_q(Mesh M, const int *tl, const int *dn, FlipQ Q) {
+  int n = *dn;
+  GS_LOOP(k, n) {
+    int index = tl[k];
+    if (M.tmark[index] >= 0) continue;
+    int otri = negate_idx(M.tmark[index]);
+    int triIndex = dtri(otri), triOri = dori(otri);
+    if (triIndex != index) push_flag(M, Q, index);
+    int p = ld1(M.tv, triIndex, m3(triOri + 1));
+    M.pred[p] = 1;
+    mark_fan_q(M, Q, triIndex, triOri);
   }
 }
 
@@ -958,8 +1131,9 @@ __global__ void k_mid_snapshot(Mesh M, const int *mids, const int *dn, const int
 
 // kernelInsertMidPoints, refine.cu:2594-2927 (debug printing left out)
 __global__ void k_insert_mid(Mesh M, const int *mids, const int *dn, int *imark, const int *snap, const int *pslots,
-                             const int *tslots, int nsub, uint32_t epoch, unsigned long long *counter) {
+                             const int *tslots, int nsub, const unsigned *ep, unsigned long long *counter) {
   int n = *dn;
+  uint32_t epoch = *ep;
   GS_LOOP(pos, n) {
     int tindex = mids[pos];
     int sindex = imark[tindex];
@@ -1417,8 +1591,10 @@ __global__ void k_reset_steiner(Mesh M, const int *wl, const int *dn, const int 
 
 // kernelInsertSteinerPoints, refine.cu:4651-4900
 __global__ void k_insert_steiner(Mesh M, const int *wl, const int *dn, const int *sinks, const double2 *center,
-                                 const int *pslots, const int *tslots, uint32_t epoch, unsigned long long *counter) {
+                                 const int *pslots, const int *tslots, const unsigned *ep,
+                                 unsigned long long *counter) {
   int n = *dn;
+  uint32_t epoch = *ep;
   GS_LOOP(pos, n) {
     int tindex = wl[pos];
     int index = sinks[tindex] >> 2, direction = sinks[tindex] & 3;

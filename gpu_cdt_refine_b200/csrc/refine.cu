@@ -165,12 +165,20 @@ struct Refiner {
   long pcap = 0, tcap = 0;
   int last_point = 0, last_triangle = 0, last_subseg = 0, nseg_in = 0;
   int pointblock = 0, triblock = 0, nempty_p = 0, nempty_t = 0, lenp = 0, lent = 0;
-  uint32_t epoch = 1;
   // per-triangle scratch (capacity tphys)
   int *emptyt = nullptr, *bad = nullptr, *imark = nullptr, *ilist = nullptr, *sinks = nullptr, *wl = nullptr;
   int *act = nullptr, *win = nullptr, *neg = nullptr, *ll = nullptr, *sl = nullptr, *newidx = nullptr;
   int *tail = nullptr;
   double2 *center = nullptr;
+  int *fq = nullptr, *tl = nullptr;  // flip-step queue and claimed-triangle list
+  uint8_t *clr = nullptr;            // deferred flag clears of a flip step
+  FlipCtl *fc = nullptr;             // flip-loop control block (device)
+  // the flip-flop loop as a CUDA graph with a device-side while condition
+  bool use_graph = true;
+  cudaGraph_t flip_graph = nullptr;
+  cudaGraphExec_t flip_exec = nullptr;
+  Mesh flip_graph_mesh{};
+  int flip_graph_pred = -1;
   // per-point scratch (capacity pphys)
   int *emptyp = nullptr, *pnew = nullptr;
   // per-subsegment scratch (capacity sphys)
@@ -194,7 +202,7 @@ struct Refiner {
   int out_np = 0, out_nt = 0, out_ns = 0;
   bool have_result = false;
 
-  enum { C_LIST0 = 0, C_LIST1, C_LIST2, C_LIST3, C_LIST4, C_LIST5, C_MISC };
+  enum { C_LIST0 = 0, C_LIST1, C_LIST2, C_LIST3, C_LIST4, C_LIST5, C_MISC, C_QN, C_TN };
 
   ~Refiner() { release(); }
 
@@ -218,17 +226,30 @@ struct Refiner {
     return cudaSuccess;
   }
 
+  void drop_flip_graph() {
+#ifndef GQM_HOST_EMU
+    if (flip_exec) cudaGraphExecDestroy(flip_exec);
+    if (flip_graph) cudaGraphDestroy(flip_graph);
+#endif
+    flip_exec = nullptr;
+    flip_graph = nullptr;
+  }
+
   void release() {
+    drop_flip_graph();
     void *ptrs[] = {M.pts, M.ps, M.pred, M.tv, M.tn, M.tsg, M.tst, M.tflip, M.tfo, M.flip0, M.tmark, M.tpos,
                     M.s2t, M.s2seg, M.enc, M.err, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
                     newidx, tail, center, emptyp, pnew, enclist, encl2, smark, mids, snap, segs, dcount, bc,
-                    dctr, dgc, dinput};
+                    dctr, dgc, dinput, M.fstamp, M.tstamp, fq, tl, clr, fc};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     if (hcount) cudaFreeHost(hcount);
     hcount = nullptr;
     M = Mesh{};
     emptyt = bad = imark = ilist = sinks = wl = act = win = neg = ll = sl = newidx = tail = nullptr;
+    fq = tl = nullptr;
+    clr = nullptr;
+    fc = nullptr;
     center = nullptr;
     emptyp = pnew = enclist = encl2 = smark = mids = snap = nullptr;
     segs = nullptr;
@@ -253,8 +274,15 @@ struct Refiner {
     if (!ev1) cudaEventCreate(&ev1);
     if (!dcount) {
       if (dalloc(&dcount, 16) || dalloc(&bc, kMaxCompactBlocks + 1) || dalloc(&dctr, 4) || dalloc(&dgc, 2) ||
-          dalloc(&M.err, 1))
+          dalloc(&M.err, 1) || dalloc(&fc, 1))
         return GQM_ERR_MEMORY;
+      cudaMemsetAsync(fc, 0, sizeof(FlipCtl), st);
+#ifdef GQM_HOST_EMU
+      use_graph = false;
+#else
+      const char *ng = getenv("GQM_NO_GRAPH");
+      use_graph = !(ng && ng[0] == '1');
+#endif
       if (cudaMallocHost((void **)&hcount, sizeof(int) * 16) != cudaSuccess) return GQM_ERR_MEMORY;
     }
     return GQM_OK;
@@ -280,17 +308,21 @@ struct Refiner {
   // Ordered compaction over [lo, hi) into out; the count lands in dcount[slot].
   template <class F, class Mp>
   void compact(F f, Mp m, int lo, int hi, int *out, int slot) {
+    compact_to(f, m, lo, hi, out, dcount + slot);
+  }
+  template <class F, class Mp>
+  void compact_to(F f, Mp m, int lo, int hi, int *out, int *dcnt) {
     int n = hi - lo;
 #ifdef GQM_HOST_EMU
     int c = 0;
     for (int i = lo; i < hi; ++i)
       if (f(i)) out[c++] = m(i);
-    dcount[slot] = c;
+    *dcnt = c;
     stats.kernel_launches += 3;
     return;
 #endif
     if (n <= 0) {
-      KL(k_set_count, 1, 32)(dcount + slot, 0);
+      KL(k_set_count, 1, 32)(dcnt, 0);
       stats.kernel_launches++;
       return;
     }
@@ -298,7 +330,7 @@ struct Refiner {
     chunk = (chunk + kCompactThreads - 1) / kCompactThreads * kCompactThreads;
     int nb = (n + chunk - 1) / chunk;
     KL(k_cnt, nb, kCompactThreads)(f, lo, hi, chunk, bc);
-    KL(k_scan, 1, 1024)(bc, nb, dcount + slot);
+    KL(k_scan, 1, 1024)(bc, nb, dcnt);
     KL(k_emit, nb, kCompactThreads)(f, m, lo, hi, chunk, bc, out);
     stats.kernel_launches += 3;
   }
@@ -342,7 +374,8 @@ struct Refiner {
         regrow(&imark, old, n) || regrow(&ilist, old, n) || regrow(&sinks, old, n) || regrow(&wl, old, n) ||
         regrow(&act, old, n) || regrow(&win, old, n) || regrow(&neg, old, n) || regrow(&ll, 2 * old, 2 * n) ||
         regrow(&sl, 6 * old, 6 * n) || regrow(&newidx, 0, n) || regrow(&tail, 0, std::max<long>(n, pphys)) ||
-        regrow(&center, old, n))
+        regrow(&center, old, n) || regrow(&M.fstamp, old, n) || regrow(&M.tstamp, old, n) || regrow(&fq, 0, n) ||
+        regrow(&tl, 0, n) || regrow(&clr, 0, n))
       return GQM_ERR_MEMORY;
     if (n > old) {
       cudaMemsetAsync(M.tst + old, 0, n - old, st);
@@ -350,6 +383,8 @@ struct Refiner {
       cudaMemsetAsync(M.tfo + old, 0, n - old, st);
       cudaMemsetAsync(M.tsg + old, 0xff, sizeof(int4) * (n - old), st);
       cudaMemsetAsync(M.tpos + old, 0xff, sizeof(int) * (n - old), st);
+      cudaMemsetAsync(M.fstamp + old, 0, sizeof(int) * (n - old), st);
+      cudaMemsetAsync(M.tstamp + old, 0, sizeof(int) * (n - old), st);
     }
     tphys = n;
     return GQM_OK;
@@ -431,30 +466,116 @@ struct Refiner {
   const int *pslots() const { return emptyp + (lenp - nempty_p); }
   const int *tslots() const { return emptyt + (lent - nempty_t); }
 
-  // ---- flip-flop (refine.cu:2328-2490) ----
+  // ---- flip-flop (refine.cu:2328-2490), driven by active sets ----
+  // One step: check (A) -> winners (W) -> link+phase 1 -> phase 2 -> phase 3
+  // -> redundant points -> reset claims -> next A -> loop condition.  Every
+  // count lives in the control block, so the whole loop runs on the device.
+  static constexpr int kStepGrid = 148 * 4;
+  void flip_body(cudaGraphConditionalHandle h, int graph) {
+    FlipQ Q{fq, &fc->qn, &fc->gen};
+    TouchL T{tl, &fc->tn, &fc->gen};
+    if (pred_mode)
+      KL(k_check_flip2<1>, kStepGrid, 256)(M, act, &fc->nact, clr, T);
+    else
+      KL(k_check_flip2<0>, kStepGrid, 256)(M, act, &fc->nact, clr, T);
+    KL(k_flip_winner2, kStepGrid, 256)(M, act, &fc->nact, clr, Q, win, &fc->winn);
+    KL(k_link_phase1, kStepGrid, 256)(M, win, &fc->winn, ll, sl, &fc->epoch);
+    KL(k_phase2, kStepGrid, 256)(M, win, &fc->winn, ll, sl);
+    KL(k_phase3q, kStepGrid, 256)(M, win, &fc->winn, sl, Q);
+    KL(k_mark_red_steiner_q, kStepGrid, 256)(M, tl, &fc->tn, Q);
+    KL(k_flip_reset_touched, kStepGrid, 256)(M, tl, &fc->tn, &fc->nact);
+    KL(k_flip_filter, kStepGrid, 256)(M, fq, &fc->qn, act, &fc->nact);
+    KL(k_flip_cond, 1, 32)(fc, h, graph);
+  }
+  int build_flip_graph() {
+#ifdef GQM_HOST_EMU
+    return GQM_ERR_CUDA;
+#else
+    drop_flip_graph();
+    cudaGraph_t g = nullptr;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) return GQM_ERR_CUDA;
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return GQM_ERR_CUDA;
+    }
+    // node 1: k_flip_prep sets the condition for the first step
+    if (cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return GQM_ERR_CUDA;
+    }
+    k_flip_prep<<<1, 32, 0, st>>>(fc, h, 1);
+    cudaGraph_t gc = nullptr;
+    if (cudaStreamEndCapture(st, &gc) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return GQM_ERR_CUDA;
+    }
+    cudaGraphNode_t prep = nullptr;
+    size_t nn = 1;
+    if (cudaGraphGetNodes(g, &prep, &nn) != cudaSuccess || nn != 1) {
+      cudaGraphDestroy(g);
+      return GQM_ERR_CUDA;
+    }
+    // node 2: while (condition) { step }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn = nullptr;
+    if (cudaGraphAddNode(&cn, g, &prep, 1, &cp) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return GQM_ERR_CUDA;
+    }
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess) {
+      cudaGraphDestroy(g);
+      return GQM_ERR_CUDA;
+    }
+    flip_body(h, 1);
+    cudaGraph_t bc2 = nullptr;
+    if (cudaStreamEndCapture(st, &bc2) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return GQM_ERR_CUDA;
+    }
+    if (cudaGraphInstantiate(&flip_exec, g, 0) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      flip_exec = nullptr;
+      return GQM_ERR_CUDA;
+    }
+    flip_graph = g;
+    flip_graph_mesh = M;
+    flip_graph_pred = pred_mode;
+    return GQM_OK;
+#endif
+  }
   int flip_flop(int ntri) {
-    long long steps = 0;
+    LAUNCH(k_flip_entry_reset, ntri, M, ntri);
+    compact_to(PNotNullFlag{M.tst, M.tflip}, Ident{}, 0, ntri, act, &fc->nact);
+    if (use_graph) {
+      if (!flip_exec || memcmp(&flip_graph_mesh, &M, sizeof(Mesh)) != 0 || flip_graph_pred != pred_mode) {
+        if (build_flip_graph() != GQM_OK) {
+          use_graph = false;
+          cudaGetLastError();
+        }
+      }
+    }
+    if (use_graph) {
+      if (cudaGraphLaunch(flip_exec, st) != cudaSuccess) return GQM_ERR_CUDA;
+      stats.kernel_launches++;
+      return GQM_OK;
+    }
+    cudaGraphConditionalHandle h{};
+    KL(k_flip_prep, 1, 32)(fc, h, 0);
+    stats.kernel_launches++;
     for (;;) {
-      compact(PNotNullFlag{M.tst, M.tflip}, Ident{}, 0, ntri, act, C_LIST3);
-      int nact = fetch(C_LIST3);
-      if (nact == 0) break;
-      if (++steps > 64 * max_rounds) return GQM_ERR_ROUND_LIMIT;
-      stats.flip_steps++;
-      LAUNCH(k_flip_init, ntri, M, ntri);
-      if (pred_mode)
-        LAUNCH(k_check_flip<1>, nact, M, act, dcount + C_LIST3);
-      else
-        LAUNCH(k_check_flip<0>, nact, M, act, dcount + C_LIST3);
-      LAUNCH(k_flip_winner, nact, M, act, dcount + C_LIST3);
-      compact(PWinner{M.tst, M.tfo}, Ident{}, 0, ntri, win, C_LIST4);
-      int bound = nact;  // winners are active triangles
-      LAUNCH(k_init_link, bound, M, win, dcount + C_LIST4, ll);
-      uint32_t ep = ++epoch;
-      LAUNCH(k_phase1, bound, M, win, dcount + C_LIST4, sl, ep);
-      LAUNCH(k_phase2, bound, M, win, dcount + C_LIST4, ll, sl);
-      LAUNCH(k_phase3, bound, M, win, dcount + C_LIST4, sl);
-      compact(PNeg{M.tmark}, Ident{}, 0, ntri, neg, C_LIST5);
-      LAUNCH(k_mark_red_steiner, 2 * nact, M, neg, dcount + C_LIST5);
+      cudaMemcpyAsync(hcount + C_MISC, &fc->cond, sizeof(int), cudaMemcpyDeviceToHost, st);
+      cudaStreamSynchronize(st);
+      stats.host_syncs++;
+      if (!hcount[C_MISC]) break;
+      flip_body(h, 0);
+      stats.kernel_launches += 9;
     }
     return GQM_OK;
   }
@@ -498,9 +619,9 @@ struct Refiner {
         LAUNCH(k_reset_mid, nmid, M, mids, dcount + C_LIST1, smark);
         LAUNCH(k_mark_mid, nmid, M, mids, dcount + C_LIST1, smark);
         LAUNCH(k_mid_snapshot, nmid, M, mids, dcount + C_LIST1, smark, snap);
-        uint32_t ep = ++epoch;
-        LAUNCH(k_insert_mid, nmid, M, mids, dcount + C_LIST1, smark, snap, pslots(), tslots(), last_subseg, ep,
-               dctr + 1);
+        KL(k_bump_epoch, 1, 32)(fc);
+        LAUNCH(k_insert_mid, nmid, M, mids, dcount + C_LIST1, smark, snap, pslots(), tslots(), last_subseg,
+               &fc->epoch, dctr + 1);
         LAUNCH(k_update_mid_nbrs, nmid, M, mids, dcount + C_LIST1, smark, enclist);
       }
       consume_slots(nenc, 2 * nenc);
@@ -539,8 +660,8 @@ struct Refiner {
     int rc = ensure_slots(nst, 2 * nst);
     if (rc) return rc;
     LAUNCH(k_reset_steiner, nst, M, wl, dw, sinks);
-    uint32_t ep = ++epoch;
-    LAUNCH(k_insert_steiner, nst, M, wl, dw, sinks, center, pslots(), tslots(), ep, dctr + 0);
+    KL(k_bump_epoch, 1, 32)(fc);
+    LAUNCH(k_insert_steiner, nst, M, wl, dw, sinks, center, pslots(), tslots(), &fc->epoch, dctr + 0);
     LAUNCH(k_update_steiner_nbrs, nst, M, wl, dw, sinks);
     consume_slots(nst, 2 * nst);
     rc = flip_flop(last_triangle);
@@ -658,6 +779,7 @@ struct Refiner {
     cudaMemsetAsync(M.s2t, 0, sizeof(unsigned long long) * sphys, st);
     cudaMemsetAsync(M.err, 0, sizeof(int), st);
     cudaMemsetAsync(dctr, 0, sizeof(unsigned long long) * 4, st);
+    KL(k_ctl_reset, 1, 32)(fc, 64 * max_rounds, M.err);
     // cos^2(theta) on the device, as the reference evaluates it
     KL(k_goodcos, 1, 32)(theta, dgc);
     double hgc[2];
@@ -730,6 +852,9 @@ struct Refiner {
     stats.device_ms = ms;
     unsigned long long hc[4];
     cudaMemcpy(hc, dctr, sizeof(hc), cudaMemcpyDeviceToHost);
+    FlipCtl hf;
+    cudaMemcpy(&hf, fc, sizeof(hf), cudaMemcpyDeviceToHost);
+    stats.flip_steps = hf.steps;
     stats.steiner_inserted = (long long)hc[0];
     stats.midpoints_inserted = (long long)hc[1];
     stats.exact_fallbacks = (long long)hc[2];
