@@ -217,13 +217,9 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     ms = ms_total / args.steps
-    t = torch.tensor([ms], device=dev, dtype=torch.float64)
-    tris = torch.tensor([float(nt_out)], device=dev, dtype=torch.float64)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tris, op=dist.ReduceOp.SUM)
-    ms_max = float(t.item())
-    value = float(tris.item()) / (ms_max / 1e3)
+    from gpu_cdt_refine_b200 import replicas
+    ms_max, tris_all = replicas.reduce_step(ms, nt_out, device=dev)
+    value = tris_all / (ms_max / 1e3)
 
     # end to end through the reference-facing call: host arrays in, host arrays out
     e2e_ms, h2d, d2h = [], cdt.nbytes(), 0
@@ -232,10 +228,8 @@ def run_ours(args, rank, world, local_rank):
         out, _ = refine.refine(cdt, 20.0, refine.Offcenter, 1, device=local_rank)
         e2e_ms.append((time.perf_counter() - t0) * 1e3)
         d2h = out.nbytes() + out.numberofpoints + out.numberoftriangles
-    e2e_t = torch.tensor([float(np.median(e2e_ms))], device=dev, dtype=torch.float64)
-    if dist:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = float(tris.item()) / (float(e2e_t.item()) / 1e3)
+    e2e_max, _ = replicas.reduce_step(float(np.median(e2e_ms)), nt_out, device=dev)
+    e2e_value = tris_all / (e2e_max / 1e3)
 
     if rank == 0:
         peak, peak_kind = measured_peak()
@@ -251,7 +245,7 @@ def run_ours(args, rank, world, local_rank):
                 "config": config(args, cdt),
                 "output_vertices": np_out, "output_triangles": nt_out, "output_segments": ns_out,
                 "e2e": {"value": e2e_value, "unit": "triangles/s", "h2d_bytes_per_step": int(h2d),
-                        "d2h_bytes_per_step": int(d2h), "ms_per_step": float(e2e_t.item())},
+                        "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_max},
                 "gpu_launches": int(s["kernel_launches"]),
                 "host_syncs": int(s["host_syncs"]), "rounds": int(s["rounds"]),
                 "flip_steps": int(s["flip_steps"]),

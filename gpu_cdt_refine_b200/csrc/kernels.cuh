@@ -6,6 +6,14 @@
 #pragma once
 #include "gqm_device.cuh"
 
+// Register budget of the latency-bound walk kernels (flip checks, cavity
+// walks, link updates): ask for at least this many resident 256-thread blocks
+// per SM, so enough warps are in flight to cover their dependent loads.
+#ifndef GQM_WALK_MIN_BLOCKS
+#define GQM_WALK_MIN_BLOCKS 3
+#endif
+#define GQM_WALK_BOUNDS __launch_bounds__(256, GQM_WALK_MIN_BLOCKS)
+
 namespace gqm {
 
 #define GS_LOOP(i, n) for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
@@ -36,6 +44,31 @@ __device__ __forceinline__ int incident_ori(const int *tri, int t, int n) {
   int d = inc0 - inc1;
   int idx = (d == -1 || d == 2) ? inc0 : inc1;
   return idx == 0 ? 2 : (idx == 1 ? 0 : 1);
+}
+
+// Input index check, run before anything dereferences the input: vertices in
+// [0, np), neighbours in [-1, nt), segment endpoints in [0, np) and distinct,
+// coordinates finite.  The reference trusts its input; a bad index here would
+// make the initialisation read outside the input arrays.
+__global__ void k_check_input(const double2 *pts, int np, const int *tri, const int *nbr, int nt,
+                              const int *seg, int ns, int *err) {
+  int bad = 0;
+  GS_LOOP(i, np) {
+    double2 p = pts[i];
+    if (!isfinite(p.x) || !isfinite(p.y)) bad = 1;
+  }
+  GS_LOOP(t, nt) {
+    for (int k = 0; k < 3; k++) {
+      unsigned v = (unsigned)tri[3 * t + k];
+      int n = nbr[3 * t + k];
+      if (v >= (unsigned)np || n < -1 || n >= nt) bad = 1;
+    }
+  }
+  GS_LOOP(s, ns) {
+    unsigned a = (unsigned)seg[2 * s], b = (unsigned)seg[2 * s + 1];
+    if (a >= (unsigned)np || b >= (unsigned)np || a == b) bad = 1;
+  }
+  if (bad) atomicCAS(err, 0, GQM_ERR_ARGUMENT);
 }
 
 __global__ void k_init_tris(Mesh M, const int *tri, const int *nbr, int nt, int tcap) {
@@ -856,7 +889,7 @@ __global__ void k_flip_reset_touched(Mesh M, const int *tl, const int *tn, int *
 // (the decision is kept in clr[k] and applied by k_flip_winner2), so the
 // neighbour flags read below are the ones the step started with.
 template <int PRED>
-__global__ void k_check_flip2(Mesh M, const int *act, const int *dn, uint8_t *clr, TouchL T) {
+__global__ void GQM_WALK_BOUNDS k_check_flip2(Mesh M, const int *act, const int *dn, uint8_t *clr, TouchL T) {
   int n = *dn;
   GS_LOOP(k, n) {
     int index = act[k];
@@ -1036,7 +1069,7 @@ __global__ void k_flip_winner2(Mesh M, const int *act, const int *dn, const uint
 
 // kernelInitLinklist + kernelUpdatePhase1 in one launch: each winner's list
 // setup reads only triangles the winner owns, before its own phase-1 writes.
-__global__ void k_link_phase1(Mesh M, const int *win, const int *dn, int *ll, int *sl, const unsigned *ep) {
+__global__ void GQM_WALK_BOUNDS k_link_phase1(Mesh M, const int *win, const int *dn, int *ll, int *sl, const unsigned *ep) {
   int n = *dn;
   uint32_t epoch = *ep;
   GS_LOOP(pos, n) {
@@ -1130,7 +1163,7 @@ __global__ void k_mid_snapshot(Mesh M, const int *mids, const int *dn, const int
 }
 
 // kernelInsertMidPoints, refine.cu:2594-2927 (debug printing left out)
-__global__ void k_insert_mid(Mesh M, const int *mids, const int *dn, int *imark, const int *snap, const int *pslots,
+__global__ void GQM_WALK_BOUNDS k_insert_mid(Mesh M, const int *mids, const int *dn, int *imark, const int *snap, const int *pslots,
                              const int *tslots, int nsub, const unsigned *ep, unsigned long long *counter) {
   int n = *dn;
   uint32_t epoch = *ep;
@@ -1474,12 +1507,20 @@ __global__ void k_remove_losers(Mesh M, const int *bad, const int *dn, const int
   }
 }
 
-// Cavity walk of kernelMarkCavities (4237-4368) / kernelCheckCavities
-// (4422-4547): depth-first over neighbours whose circumcircle contains the
-// centre, not crossing subsegments except the sink's split edge, at most 50
-// triangles.
-template <int PRED, bool CHECK>
-__device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, int badIndex) {
+// Cavity walk of kernelMarkCavities (4237-4368): depth-first over neighbours
+// whose circumcircle contains the centre, not crossing subsegments except the
+// sink's split edge, at most 50 triangles.  Returns the number of triangles in
+// the cavity (stored, in visiting order, at out[j * stride]) or -1 when the
+// cavity exceeds the cap.
+//
+// kernelCheckCavities (4422-4547) repeats the same walk and fails at the first
+// triangle whose marker is not the candidate's.  Between the two launches only
+// the markers change, never the mesh or the centres, so its walk visits exactly
+// the triangles stored here (up to the first failure): checking the stored
+// list gives the same verdict without a second walk or any predicate.
+template <int PRED>
+__device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, int badIndex, int *out,
+                           int stride) {
   int region[kCavityCap], loop[kCavityCap];
   int rsize = 0, lsize = 0;
   int cur = sink;
@@ -1491,14 +1532,10 @@ __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, i
         break;
       }
     if (!found) {
-      if (rsize == kCavityCap || lsize == kCavityCap) return CHECK ? 0 : -1;
+      if (rsize == kCavityCap || lsize == kCavityCap) return -1;
       region[rsize++] = cur;
       loop[lsize++] = cur;
-      if (CHECK) {
-        if (M.tmark[cur] != badIndex) return -1;
-      } else {
-        atomicMin(M.tmark + cur, badIndex);
-      }
+      atomicMin(M.tmark + cur, badIndex);
     }
     bool recursive = false;
     int nIdx = -1;
@@ -1532,7 +1569,10 @@ __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, i
       cur = nIdx;
     else {
       if (lsize > 0) lsize--;
-      if (lsize == 0) return 0;
+      if (lsize == 0) {
+        for (int j = 0; j < rsize; ++j) out[(long)j * stride] = region[j];
+        return rsize;
+      }
       cur = loop[lsize - 1];
     }
   }
@@ -1540,26 +1580,36 @@ __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, i
   return 0;
 }
 
+// kernelMarkCavities: claim every cavity triangle (atomicMin of the bad index);
+// an oversized cavity makes its candidate an unconditional winner (negated
+// index).  cavn[k] = stored cavity size (0 for an oversized one).
 template <int PRED>
-__global__ void k_cavity_mark(Mesh M, const int *dn, const int *sinks, const double2 *center, const int *imark,
-                              int *ilist) {
+__global__ void GQM_WALK_BOUNDS k_cavity_mark(Mesh M, const int *dn, const int *sinks, const double2 *center, const int *imark,
+                              int *ilist, int *cav, int *cavn, int stride) {
   int n = *dn;
   GS_LOOP(k, n) {
     if (imark[k] < 0) continue;
     int badIndex = ilist[k];
-    if (cavity_walk<PRED, false>(M, sinks[k] >> 2, sinks[k] & 3, center[k], badIndex) < 0)
-      ilist[k] = negate_idx(badIndex);
+    int c = cavity_walk<PRED>(M, sinks[k] >> 2, sinks[k] & 3, center[k], badIndex, cav + k, stride);
+    if (c < 0) ilist[k] = negate_idx(badIndex);
+    cavn[k] = c < 0 ? 0 : c;
   }
 }
-template <int PRED>
-__global__ void k_cavity_check(Mesh M, const int *dn, const int *sinks, const double2 *center, int *imark,
+// kernelCheckCavities: a candidate loses if any triangle of its cavity was
+// claimed by a smaller bad index.
+__global__ void k_cavity_check(Mesh M, const int *dn, const int *cav, const int *cavn, int stride, int *imark,
                                const int *ilist) {
   int n = *dn;
   GS_LOOP(k, n) {
     if (imark[k] < 0) continue;
     int badIndex = ilist[k];
     if (badIndex < 0) continue;
-    if (cavity_walk<PRED, true>(M, sinks[k] >> 2, sinks[k] & 3, center[k], badIndex) < 0) imark[k] = -1;
+    int c = cavn[k];
+    for (int j = 0; j < c; ++j)
+      if (M.tmark[cav[(long)j * stride + k]] != badIndex) {
+        imark[k] = -1;
+        break;
+      }
   }
 }
 

@@ -15,7 +15,9 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../../include/gqm_refine.h"
@@ -29,13 +31,20 @@ namespace gqm {
 // per-block ordered emit (warp ballots).  No spin waits.
 // ============================================================================
 constexpr int kCompactThreads = 256;
+constexpr int kCompactItems = 16;  // consecutive elements per thread
+constexpr int kCompactTile = kCompactThreads * kCompactItems;
 constexpr int kMaxCompactBlocks = 2048;
 
+// per-block counts: block b covers [lo + b*chunk, lo + (b+1)*chunk)
 template <class F>
-__global__ void k_cnt(F f, int lo, int hi, int chunk, int *bc) {
+__global__ void __launch_bounds__(kCompactThreads) k_cnt(F f, int lo, int hi, int chunk, int *bc) {
   int b0 = lo + blockIdx.x * chunk, b1 = min(hi, b0 + chunk);
   int c = 0;
-  for (int i = b0 + threadIdx.x; i < b1; i += blockDim.x) c += f(i) ? 1 : 0;
+  for (int s = b0 + threadIdx.x * kCompactItems; s < b1; s += kCompactTile) {
+#pragma unroll
+    for (int j = 0; j < kCompactItems; ++j)
+      if (s + j < b1 && f(s + j)) ++c;
+  }
   __shared__ int red[32];
   for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
@@ -70,29 +79,44 @@ __global__ void k_scan(int *bc, int nb, int *total) {
   }
   if (threadIdx.x == 0) *total = carry;
 }
+// ordered emit: each thread takes 16 consecutive elements of a 4096-element
+// tile, a block-wide exclusive scan of the per-thread counts gives the slots
 template <class F, class Mp>
-__global__ void k_emit(F f, Mp m, int lo, int hi, int chunk, const int *bc, int *out) {
-  __shared__ int wsum[32];
-  __shared__ int base;
+__global__ void __launch_bounds__(kCompactThreads) k_emit(F f, Mp m, int lo, int hi, int chunk, const int *bc,
+                                                          int *out) {
+  __shared__ int wsum[kCompactThreads / 32];
   int b0 = lo + blockIdx.x * chunk, b1 = min(hi, b0 + chunk);
-  if (threadIdx.x == 0) base = bc[blockIdx.x];
-  __syncthreads();
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  for (int s = b0; s < b1; s += blockDim.x) {
-    int i = s + threadIdx.x;
-    bool p = (i < b1) && f(i);
-    unsigned bal = __ballot_sync(0xffffffffu, p);
-    if (lane == 0) wsum[warp] = __popc(bal);
-    __syncthreads();
-    int off = 0, tot = 0;
-    for (int w = 0; w < nw; ++w) {
-      int c = wsum[w];
-      if (w < warp) off += c;
-      tot += c;
+  int base = bc[blockIdx.x];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int tile = b0; tile < b1; tile += kCompactTile) {
+    int s = tile + threadIdx.x * kCompactItems;
+    unsigned bits = 0;
+#pragma unroll
+    for (int j = 0; j < kCompactItems; ++j)
+      if (s + j < b1 && f(s + j)) bits |= 1u << j;
+    int c = __popc(bits);
+    // inclusive warp scan of c
+    int x = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
     }
-    if (p) out[base + off + __popc(bal & ((1u << lane) - 1))] = m(i);
+    if (lane == 31) wsum[warp] = x;
     __syncthreads();
-    if (threadIdx.x == 0) base += tot;
+    int woff = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < kCompactThreads / 32; ++w) {
+      int v = wsum[w];
+      woff += (w < warp) ? v : 0;
+      tot += v;
+    }
+    int pos = base + woff + x - c;
+    while (bits) {
+      int j = __ffs(bits) - 1;
+      bits &= bits - 1;
+      out[pos++] = m(s + j);
+    }
+    base += tot;
     __syncthreads();
   }
 }
@@ -170,6 +194,8 @@ struct Refiner {
   int *act = nullptr, *win = nullptr, *neg = nullptr, *ll = nullptr, *sl = nullptr, *newidx = nullptr;
   int *tail = nullptr;
   double2 *center = nullptr;
+  int *cav = nullptr, *cavn = nullptr;  // stored cavities of the Steiner candidates
+  long cav_cap = 0;
   int *fq = nullptr, *tl = nullptr;  // flip-step queue and claimed-triangle list
   uint8_t *clr = nullptr;            // deferred flag clears of a flip step
   FlipCtl *fc = nullptr;             // flip-loop control block (device)
@@ -240,7 +266,7 @@ struct Refiner {
     void *ptrs[] = {M.pts, M.ps, M.pred, M.tv, M.tn, M.tsg, M.tst, M.tflip, M.tfo, M.flip0, M.tmark, M.tpos,
                     M.s2t, M.s2seg, M.enc, M.err, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
                     newidx, tail, center, emptyp, pnew, enclist, encl2, smark, mids, snap, segs, dcount, bc,
-                    dctr, dgc, dinput, M.fstamp, M.tstamp, fq, tl, clr, fc};
+                    dctr, dgc, dinput, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     if (hcount) cudaFreeHost(hcount);
@@ -251,6 +277,8 @@ struct Refiner {
     clr = nullptr;
     fc = nullptr;
     center = nullptr;
+    cav = cavn = nullptr;
+    cav_cap = 0;
     emptyp = pnew = enclist = encl2 = smark = mids = snap = nullptr;
     segs = nullptr;
     dcount = bc = nullptr;
@@ -326,8 +354,8 @@ struct Refiner {
       stats.kernel_launches++;
       return;
     }
-    int chunk = std::max(4 * kCompactThreads, (n + kMaxCompactBlocks - 1) / kMaxCompactBlocks);
-    chunk = (chunk + kCompactThreads - 1) / kCompactThreads * kCompactThreads;
+    int chunk = std::max(kCompactTile, (n + kMaxCompactBlocks - 1) / kMaxCompactBlocks);
+    chunk = (chunk + kCompactTile - 1) / kCompactTile * kCompactTile;
     int nb = (n + chunk - 1) / chunk;
     KL(k_cnt, nb, kCompactThreads)(f, lo, hi, chunk, bc);
     KL(k_scan, 1, 1024)(bc, nb, dcnt);
@@ -470,7 +498,11 @@ struct Refiner {
   // One step: check (A) -> winners (W) -> link+phase 1 -> phase 2 -> phase 3
   // -> redundant points -> reset claims -> next A -> loop condition.  Every
   // count lives in the control block, so the whole loop runs on the device.
-  static constexpr int kStepGrid = 148 * 4;
+#ifndef GQM_STEP_GRID
+#define GQM_STEP_GRID (148 * 4)
+#endif
+  // grid of the flip-step kernels, whose item counts live on the device
+  static constexpr int kStepGrid = GQM_STEP_GRID;
   void flip_body(cudaGraphConditionalHandle h, int graph) {
     FlipQ Q{fq, &fc->qn, &fc->gen};
     TouchL T{tl, &fc->tn, &fc->gen};
@@ -645,13 +677,21 @@ struct Refiner {
       LAUNCH(k_locate<0>, nbad, M, bad, dn, center, sinks);
     LAUNCH(k_remove_losers, nbad, M, bad, dn, sinks, imark);
     LAUNCH(k_fill, last_triangle, M.tmark, last_triangle, kMaxInt);
-    if (pred_mode) {
-      LAUNCH(k_cavity_mark<1>, nbad, M, dn, sinks, center, imark, ilist);
-      LAUNCH(k_cavity_check<1>, nbad, M, dn, sinks, center, imark, ilist);
-    } else {
-      LAUNCH(k_cavity_mark<0>, nbad, M, dn, sinks, center, imark, ilist);
-      LAUNCH(k_cavity_check<0>, nbad, M, dn, sinks, center, imark, ilist);
+    if (nbad > cav_cap) {  // stored cavities: kCavityCap rows of nbad entries
+      long cap = std::max<long>(nbad, 2 * cav_cap);
+      cudaStreamSynchronize(st);
+      if (cav) cudaFree(cav);
+      if (cavn) cudaFree(cavn);
+      cav = cavn = nullptr;
+      cav_cap = 0;
+      if (dalloc(&cav, (size_t)kCavityCap * cap) || dalloc(&cavn, cap)) return GQM_ERR_MEMORY;
+      cav_cap = cap;
     }
+    if (pred_mode)
+      LAUNCH(k_cavity_mark<1>, nbad, M, dn, sinks, center, imark, ilist, cav, cavn, nbad);
+    else
+      LAUNCH(k_cavity_mark<0>, nbad, M, dn, sinks, center, imark, ilist, cav, cavn, nbad);
+    LAUNCH(k_cavity_check, nbad, M, dn, cav, cavn, nbad, imark, ilist);
     compact(PNonNeg{imark}, Ident{}, 0, nbad, wl, C_LIST1);
     int nst = fetch(C_LIST1);
     int *dw = dcount + C_LIST1;
@@ -780,6 +820,9 @@ struct Refiner {
     cudaMemsetAsync(M.err, 0, sizeof(int), st);
     cudaMemsetAsync(dctr, 0, sizeof(unsigned long long) * 4, st);
     KL(k_ctl_reset, 1, 32)(fc, 64 * max_rounds, M.err);
+    LAUNCH(k_check_input, std::max(np, nt), (const double2 *)dpts, np, dtri_in, dnbr_in, nt, dseg_in, ns, M.err);
+    rc = check_device_error();
+    if (rc) return rc;
     // cos^2(theta) on the device, as the reference evaluates it
     KL(k_goodcos, 1, 32)(theta, dgc);
     double hgc[2];
@@ -970,13 +1013,67 @@ int gqm_refine(const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt, g
   }
   int rc = validate(in, opt);
   if (rc) return rc;
-  gqm_context *ctx = nullptr;
-  rc = gqm_context_create(opt->device, &ctx);
-  if (rc) return rc;
+  // One cached context per device: device buffers and the captured flip-loop
+  // graph are reused by later calls instead of being allocated every time.
+  static std::mutex cache_mutex;
+  static gqm_context *cache[64] = {};
+  if (opt->device < 0 || opt->device >= 64) return GQM_ERR_NO_DEVICE;
+  std::lock_guard<std::mutex> lock(cache_mutex);
+  gqm_context *&ctx = cache[opt->device];
+  if (!ctx) {
+    rc = gqm_context_create(opt->device, &ctx);
+    if (rc) return rc;
+  }
   rc = gqm_context_run(ctx, in, 0, opt, stats);
   if (rc == GQM_OK) rc = gqm_context_result(ctx, out);
-  gqm_context_destroy(ctx);
   return rc;
+}
+
+int gqm_refine_batch(int ndomains, const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt,
+                     gqm_stats *stats, int workers, int *failed_domain) {
+  if (failed_domain) *failed_domain = -1;
+  if (ndomains < 0 || (ndomains > 0 && (!in || !out || !opt))) return GQM_ERR_ARGUMENT;
+  for (int i = 0; i < ndomains; ++i) memset(&out[i], 0, sizeof(gqm_cdt_out));
+  if (ndomains == 0) return GQM_OK;
+  for (int i = 0; i < ndomains; ++i) {
+    int rc = validate(&in[i], &opt[i]);
+    if (rc) {
+      if (failed_domain) *failed_domain = i;
+      return rc;
+    }
+  }
+  if (workers < 1) workers = 1;
+  if (workers > ndomains) workers = ndomains;
+  // largest domains first (longest-processing-time order)
+  std::vector<int> order(ndomains);
+  for (int i = 0; i < ndomains; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return in[a].numberofpoints > in[b].numberofpoints; });
+  std::atomic<int> next(0), first_err(0), err_dom(-1);
+  auto work = [&](int) {
+    gqm_context *ctx = nullptr;
+    for (;;) {
+      int k = next.fetch_add(1);
+      if (k >= ndomains || first_err.load() != 0) break;
+      int d = order[k];
+      int rc = GQM_OK;
+      if (!ctx) rc = gqm_context_create(opt[d].device, &ctx);
+      gqm_stats st;
+      if (rc == GQM_OK) rc = gqm_context_run(ctx, &in[d], 0, &opt[d], &st);
+      if (rc == GQM_OK) rc = gqm_context_result(ctx, &out[d]);
+      if (rc == GQM_OK && stats) stats[d] = st;
+      if (rc != GQM_OK) {
+        int zero = 0;
+        if (first_err.compare_exchange_strong(zero, rc)) err_dom.store(d);
+      }
+    }
+    if (ctx) gqm_context_destroy(ctx);
+  };
+  std::vector<std::thread> pool;
+  for (int w = 0; w < workers; ++w) pool.emplace_back(work, w);
+  for (auto &t : pool) t.join();
+  if (failed_domain) *failed_domain = err_dom.load();
+  return first_err.load();
 }
 
 void gqm_free_result(gqm_cdt_out *out) {

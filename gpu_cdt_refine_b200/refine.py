@@ -89,6 +89,10 @@ def lib() -> ctypes.CDLL:
         L.gqm_context_stream.argtypes = [ctypes.c_void_p]
         L.gqm_context_stream.restype = ctypes.c_void_p
         L.gqm_version.restype = ctypes.c_int
+        L.gqm_refine_batch.argtypes = [ctypes.c_int, ctypes.POINTER(CdtIn), ctypes.POINTER(CdtOut),
+                                       ctypes.POINTER(Options), ctypes.POINTER(Stats), ctypes.c_int,
+                                       ctypes.POINTER(ctypes.c_int)]
+        L.gqm_refine_batch.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -146,6 +150,31 @@ def refine(cdt: CDT, theta=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED
     if with_status:
         return (*got, st.as_dict())
     return got, st.as_dict()
+
+
+def refine_batch(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0,
+                 workers=8, max_rounds=0):
+    """Refine independent CDTs concurrently (gqm_refine_batch); returns
+    (list of CDT, list of stats dicts)."""
+    L = lib()
+    n = len(cdts)
+    if np.isscalar(thetas):
+        thetas = [float(thetas)] * n
+    keep = []
+    ins = (CdtIn * n)(*[_cdt_in(c, keep) for c in cdts])
+    outs = (CdtOut * n)()
+    opts = (Options * n)(*[make_options(t, insertpolicy, mode, predicates, device, max_rounds) for t in thetas])
+    sts = (Stats * n)()
+    bad = ctypes.c_int(-1)
+    rc = L.gqm_refine_batch(n, ins, outs, opts, sts, int(workers), ctypes.byref(bad))
+    try:
+        if rc != 0:
+            raise RefineError(rc, f"domain {bad.value}: " + L.gqm_status_string(rc).decode())
+        res = [_take(outs[i]) for i in range(n)]
+    finally:
+        for i in range(n):
+            L.gqm_free_result(ctypes.byref(outs[i]))
+    return res, [sts[i].as_dict() for i in range(n)]
 
 
 def GPU_Refine_Quality(input: CDT, theta: float, insertpolicy=Offcenter, deletepolicy=Connected, mode=1,

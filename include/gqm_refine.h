@@ -97,7 +97,8 @@ typedef struct {
 void gqm_default_options(gqm_options *opt);
 
 /* One call: host CDT in, host CDT out (host<->device copies included).
- * Equivalent of GPU_Refine_Quality. */
+ * Equivalent of GPU_Refine_Quality.  Device buffers are kept in one cached
+ * context per device between calls; calls are serialized by a mutex. */
 int gqm_refine(const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt, gqm_stats *stats);
 void gqm_free_result(gqm_cdt_out *out);
 
@@ -140,6 +141,16 @@ void *gqm_context_stream(gqm_context *ctx);
 #define GQM_NOALLOC_MAX_ELEMENTS 131072
 #define GQM_ERR_TOO_LARGE (-13)
 int gqm_context_result_noalloc(gqm_context *ctx, gqm_cdt_out *out);
+
+/* Batched refinement of independent domains (no counterpart in the
+ * reference, which refines one CDT per call).  Domains are taken largest first
+ * by `workers` host threads; each worker owns a context with its own CUDA
+ * stream, so the GPU work of different domains overlaps.  opt[i] and stats[i]
+ * belong to domain i (stats may be NULL); out[i] is released with
+ * gqm_free_result.  Each domain's result is the one gqm_refine would return.
+ * Returns GQM_OK or the first failing domain's status (*failed_domain set). */
+int gqm_refine_batch(int ndomains, const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt,
+                     gqm_stats *stats, int workers, int *failed_domain);
 
 const char *gqm_status_string(int status);
 int gqm_version(void);

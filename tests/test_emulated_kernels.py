@@ -63,3 +63,30 @@ def test_emulated_round_limit(emulated):
     with pytest.raises(refine.RefineError) as e:
         refine.refine(cdt, 20.0, max_rounds=1)
     assert e.value.status == -2
+
+
+@pytest.mark.parametrize("field,row,col,value", [
+    ("segmentlist", 0, 0, 10**6),   # segment endpoint out of range
+    ("segmentlist", 1, 1, -4),      # negative endpoint
+    ("trianglelist", 5, 2, 10**6),  # triangle vertex out of range
+    ("neighborlist", 7, 0, 10**7),  # neighbour index out of range
+])
+def test_emulated_rejects_bad_indices(emulated, field, row, col, value):
+    """Out-of-range indices are caught on the device before any kernel reads
+    through them (GQM_ERR_ARGUMENT)."""
+    cdt = inputs.plain_small(seed=304, n=500, nseg=20)
+    arr = getattr(cdt, field).copy()
+    arr.reshape(-1, arr.shape[-1])[row, col] = value
+    setattr(cdt, field, arr)
+    with pytest.raises(refine.RefineError) as e:
+        refine.refine(cdt, 20.0)
+    assert e.value.status == -1
+
+
+def test_emulated_batch(emulated):
+    doms = [inputs.plain_small(seed=310 + i, n=n, nseg=n // 20) for i, n in enumerate([300, 1500, 700])]
+    got, stats = refine.refine_batch(doms, [15.0, 20.0, 18.0], workers=2)
+    for d, th, g, st in zip(doms, [15.0, 20.0, 18.0], got, stats):
+        want, info = oracle_py.refine(d, th, 1, 1)
+        _same(g, want)
+        assert st["rounds"] == info["rounds"]
