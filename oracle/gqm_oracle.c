@@ -2036,6 +2036,12 @@ static int find_incident_ori(const int *tri, int t1, int t2) { /* findIncidentOr
 
 int gqm_oracle_refine(int np, const double *pts, int nt, const int *tri, const int *nbr, int ns, const int *segs,
                       double theta, int policy, int mode, long long max_rounds, gqm_oracle_out *out) {
+  return gqm_oracle_refine_gc(np, pts, nt, tri, nbr, ns, segs, theta, 0.0, policy, mode, max_rounds, out);
+}
+
+int gqm_oracle_refine_gc(int np, const double *pts, int nt, const int *tri, const int *nbr, int ns,
+                         const int *segs, double theta, double goodcos2, int policy, int mode, long long max_rounds,
+                         gqm_oracle_out *out) {
   memset(out, 0, sizeof(*out));
   St Sv;
   St *S = &Sv;
@@ -2043,7 +2049,9 @@ int gqm_oracle_refine(int np, const double *pts, int nt, const int *tri, const i
   S->theta = theta;
   S->mode = mode;
   S->max_rounds = max_rounds;
-  {
+  if (goodcos2 > 0.0) {
+    S->gc2 = goodcos2;
+  } else {  /* refine.cu:418-419 */
     double c = cos(theta * PI_REF / 180.0);
     S->gc2 = c * c;
   }

@@ -34,6 +34,13 @@ typedef struct {
  * nbr uses Triangle's plain format (neighbour triangle index, -1 boundary). */
 int gqm_oracle_refine(int np, const double *pts, int nt, const int *tri, const int *nbr, int ns, const int *segs,
                       double theta, int policy, int mode, long long max_rounds, gqm_oracle_out *out);
+/* Same, with cos^2(theta) given.  The reference evaluates cos(theta*PI/180)
+ * on the device (refine.cu:418-419), whose cos() can differ from the host's
+ * by one ulp for some angles (it does at 20.7 degrees); goodcos2 > 0 replaces
+ * the host evaluation by that device value.  goodcos2 <= 0: host cos(). */
+int gqm_oracle_refine_gc(int np, const double *pts, int nt, const int *tri, const int *nbr, int ns,
+                         const int *segs, double theta, double goodcos2, int policy, int mode, long long max_rounds,
+                         gqm_oracle_out *out);
 void gqm_oracle_free(gqm_oracle_out *out);
 
 /* Reference predicate arithmetic, exported for the predicate tests. */
