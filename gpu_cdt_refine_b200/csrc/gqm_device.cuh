@@ -11,9 +11,11 @@
 //   tflip uint8[Tcap]     flip-flop marker (set concurrently)
 //   tfo   uint8[Tcap]     flip orientation code, 15 = none
 //   tmark int[Tcap]       ownership marker (atomicMin) / flipBy
-//   s2t   uint64[Scap]    subsegment -> oriented triangle, tagged with the
-//                         launch epoch in the high word (see s2t_store)
+//   s2t   u128[Scap]      subsegment -> oriented triangle in the low word,
+//                         tagged with the launch epoch and the storing
+//                         thread's key (see s2t_store)
 //   s2seg int[Scap], enc int[Scap], segs int2[S_in]
+//   wbits uint32[Tcap/32], wcnt/wpre int[Tcap/1024]   flip winners of a step
 // Edge i of a triangle joins vertices i+1 and i+2 and faces vertex i; an
 // oriented triangle (t << 2 | i) names edge i of t (GPU_Refine/refine.cu:95-113).
 // Flags the reference keeps in one byte (GPU_Refine/refine.h:36-205) are split
@@ -26,6 +28,8 @@
 namespace gqm {
 
 constexpr int kMaxInt = 2147483647;
+// subseg2tri entry: bits 127..64 launch epoch, 63..32 writer key, 31..0 oriented triangle
+typedef unsigned __int128 s2t_t;
 constexpr int kCavityCap = 50;  // MyList capacity, GPU_Refine/refine.h:30
 
 enum : uint8_t { PS_DELETED = 1, PS_STEINER = 2, PS_SEGSPLIT = 4, PS_NEW = 8 };
@@ -39,7 +43,11 @@ struct Mesh {
   int *tmark;
   int *tpos;  // winner-slot of each triangle during a flip step
   int *fstamp, *tstamp;  // per-triangle generation stamps deduplicating the flip-step queues
-  unsigned long long *s2t;
+  s2t_t *s2t;
+  // flip winners of the current step: one bit per triangle slot, winner counts
+  // per chunk of 1024 slots and their exclusive prefix (see win_rank)
+  unsigned *wbits;
+  int *wcnt, *wpre;
   int *s2seg, *enc;
   const int2 *segs;
   int *err;  // first error code raised on the device
@@ -67,10 +75,41 @@ __device__ __forceinline__ void st1(int4 *a, int t, int i, int x) { reinterpret_
 __device__ __forceinline__ int ld1(const int4 *a, int t, int i) { return reinterpret_cast<const int *>(a + t)[i]; }
 
 __device__ __forceinline__ int s2t_get(const Mesh &M, int s) { return (int)(uint32_t)M.s2t[s]; }
-// Rule for concurrent writers of one subsegment's entry within a launch: the
-// largest oriented triangle wins; a value from an earlier launch always loses.
-__device__ __forceinline__ void s2t_store(const Mesh &M, int s, int v, uint32_t epoch) {
-  atomicMax(M.s2t + s, ((unsigned long long)epoch << 32) | (uint32_t)v);
+__device__ __forceinline__ s2t_t s2t_plain(int v) { return (s2t_t)(uint32_t)v; }  // epoch 0: older than any launch
+// Key of a store into subseg2tri by the thread at position `pos` of a launch,
+// `slot` being the store's place in the kernel's program order.  When threads
+// of one launch store into the same entry, the largest key is kept: within a
+// warp the later store instruction (a warp issues its stores in order) and,
+// for one instruction, the lower lane; across warps the lower warp.  That is
+// the order in which the reference's racing stores (GPU_Refine/refine.cu:
+// 1362-1372, 1419-1424, 1533-1544, 2844-2850, 2900-2903, 4744-4876) were seen
+// to land on a B200, and the oracle applies the same key.
+__device__ __forceinline__ uint32_t wkey(int pos, int slot) {
+  return ((0x7FFFFFu - ((uint32_t)pos >> 5)) << 9) | ((uint32_t)slot << 5) | (31u - ((uint32_t)pos & 31u));
+}
+// A value stored in an earlier launch always loses to one of this launch; in
+// one launch the larger (epoch, key) wins.  The loop reads the entry with the
+// compare-and-swap itself, so a torn read is never acted on.
+__device__ __forceinline__ void s2t_store(const Mesh &M, int s, int v, uint32_t epoch, uint32_t key) {
+  const s2t_t nw = ((s2t_t)epoch << 64) | ((s2t_t)key << 32) | (uint32_t)v;
+  s2t_t cur = 0;
+  for (;;) {
+    const s2t_t o = atomicCAS(M.s2t + s, cur, nw);
+    if (o == cur || (o >> 32) >= (nw >> 32)) return;
+    cur = o;
+  }
+}
+
+// Position of flip winner `index` in the reference's winner list, which is
+// compacted in triangle order (kernelUpdatePhase1's pos, refine.cu:1312): the
+// number of this step's winners with a smaller slot.  The winners' own list
+// here is filled by atomics in any order, so the position comes from the
+// winner bitmap: the prefix of its 1024-slot chunk plus the bits before it.
+__device__ __forceinline__ int win_rank(const Mesh &M, int index) {
+  const int w = index >> 5;
+  int r = M.wpre[index >> 10];
+  for (int i = w & ~31; i < w; ++i) r += __popc(M.wbits[i]);
+  return r + __popc(M.wbits[w] & ((1u << (index & 31)) - 1u));
 }
 
 __device__ __forceinline__ void raise_err(const Mesh &M, int code) { atomicCAS(M.err, 0, code); }

@@ -168,7 +168,7 @@ __global__ void k_init_subsegs(Mesh M, int nt, const unsigned long long *keys, c
 }
 __global__ void k_pack_s2t(Mesh M, const int *s2t_int, int ns) {
   GS_LOOP(s, ns) {
-    M.s2t[s] = (unsigned long long)(uint32_t)s2t_int[s];
+    M.s2t[s] = s2t_plain(s2t_int[s]);
     M.s2seg[s] = s;
   }
 }
@@ -391,10 +391,10 @@ __device__ void phase1_body(const Mesh &M, int pos, int index, int *sl, uint32_t
       b.w = 0;
       M.tsg[index] = a;
       M.tsg[pOppTri] = b;
-      if (sOrg != -1) s2t_store(M, sOrg, (index << 2) | ori, epoch);
-      if (spDest != -1) s2t_store(M, spDest, (index << 2) | m3(ori + 1), epoch);
-      if (sApex != -1) s2t_store(M, sApex, (pOppTri << 2) | pOppOri, epoch);
-      if (spApex != -1) s2t_store(M, spApex, (pOppTri << 2) | m3(pOppOri + 2), epoch);
+      if (sOrg != -1) s2t_store(M, sOrg, (index << 2) | ori, epoch, wkey(win_rank(M, index), 0));
+      if (spDest != -1) s2t_store(M, spDest, (index << 2) | m3(ori + 1), epoch, wkey(win_rank(M, index), 1));
+      if (sApex != -1) s2t_store(M, sApex, (pOppTri << 2) | pOppOri, epoch, wkey(win_rank(M, index), 2));
+      if (spApex != -1) s2t_store(M, spApex, (pOppTri << 2) | m3(pOppOri + 2), epoch, wkey(win_rank(M, index), 3));
       M.tst[index] |= TS_CHECK;
       M.tst[pOppTri] |= TS_CHECK;
     } else if (ori < 6) {
@@ -421,9 +421,9 @@ __device__ void phase1_body(const Mesh &M, int pos, int index, int *sl, uint32_t
       setc(a, m3(ori + 2), sDest);
       a.w = 0;
       M.tsg[index] = a;
-      if (sOrg != -1) s2t_store(M, sOrg, (index << 2) | m3(ori + 1), epoch);
-      if (sApex != -1) s2t_store(M, sApex, (index << 2) | ori, epoch);
-      if (sDest != -1) s2t_store(M, sDest, (index << 2) | m3(ori + 2), epoch);
+      if (sOrg != -1) s2t_store(M, sOrg, (index << 2) | m3(ori + 1), epoch, wkey(win_rank(M, index), 4));
+      if (sApex != -1) s2t_store(M, sApex, (index << 2) | ori, epoch, wkey(win_rank(M, index), 5));
+      if (sDest != -1) s2t_store(M, sDest, (index << 2) | m3(ori + 2), epoch, wkey(win_rank(M, index), 6));
       M.tst[index] |= TS_CHECK;
       M.tst[t1] &= (uint8_t)~TS_NOTNULL;
       M.tst[t2] &= (uint8_t)~TS_NOTNULL;
@@ -492,12 +492,12 @@ __device__ void phase1_body(const Mesh &M, int pos, int index, int *sl, uint32_t
       b.w = 0;
       M.tsg[index] = a;
       M.tsg[t1] = b;
-      if (sOrg != -1) s2t_store(M, sOrg, (index << 2) | ori, epoch);
-      if (sDest != -1) s2t_store(M, sDest, (index << 2) | m3(ori + 1), epoch);
-      if (sApex != -1) s2t_store(M, sApex, (index << 2) | m3(ori + 2), epoch);
-      if (snOrg != -1) s2t_store(M, snOrg, (t1 << 2) | t1_ori, epoch);
-      if (snDest != -1) s2t_store(M, snDest, (t1 << 2) | m3(t1_ori + 1), epoch);
-      if (snApex != -1) s2t_store(M, snApex, (t1 << 2) | m3(t1_ori + 2), epoch);
+      if (sOrg != -1) s2t_store(M, sOrg, (index << 2) | ori, epoch, wkey(win_rank(M, index), 7));
+      if (sDest != -1) s2t_store(M, sDest, (index << 2) | m3(ori + 1), epoch, wkey(win_rank(M, index), 8));
+      if (sApex != -1) s2t_store(M, sApex, (index << 2) | m3(ori + 2), epoch, wkey(win_rank(M, index), 9));
+      if (snOrg != -1) s2t_store(M, snOrg, (t1 << 2) | t1_ori, epoch, wkey(win_rank(M, index), 10));
+      if (snDest != -1) s2t_store(M, snDest, (t1 << 2) | m3(t1_ori + 1), epoch, wkey(win_rank(M, index), 11));
+      if (snApex != -1) s2t_store(M, snApex, (t1 << 2) | m3(t1_ori + 2), epoch, wkey(win_rank(M, index), 12));
       M.tst[index] |= TS_CHECK;
       M.tst[t1] |= TS_CHECK;
       M.tst[pOppTri] &= (uint8_t)~TS_NOTNULL;
@@ -760,6 +760,59 @@ __global__ void k_mark_redundant(Mesh M, int *delmarker, const int *dellist, con
 // ============================================================================
 // Control block of a flip-flop loop, resident on the device so that the loop
 // can run as a CUDA graph with a device-side condition.
+// Launch timer of one kernel inside the device-side flip loop, where CUDA
+// events cannot bracket single launches.  Each block stamps %globaltimer when
+// it starts and when it ends; the last block to finish adds (latest end -
+// earliest start) to the total, i.e. the launch's execution time from its
+// first block to its last, and counts the launch and its items.
+struct KTimer {
+  unsigned long long t0, t1;  // earliest block start / latest block end of the current launch
+  unsigned long long total_ns, launches, items;
+  unsigned blocks_done;
+  int on;
+};
+__device__ __forceinline__ unsigned long long global_ns() {
+#ifdef GQM_HOST_EMU
+  return (unsigned long long)std::chrono::duration_cast<std::chrono::nanoseconds>(
+             std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+#else
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+#endif
+}
+// called by every thread of the block after its work, with the block's start stamp
+__device__ __forceinline__ void ktimer_end(KTimer *tm, unsigned long long start, int items) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    atomicMin(&tm->t0, start);
+    atomicMax(&tm->t1, global_ns());
+    __threadfence();
+    unsigned done = atomicAdd(&tm->blocks_done, 1u);
+    if (done == gridDim.x - 1) {
+      __threadfence();
+      volatile KTimer *v = tm;
+      v->total_ns += v->t1 - v->t0;
+      v->launches += 1;
+      v->items += (unsigned long long)items;
+      v->t0 = ~0ull;
+      v->t1 = 0;
+      v->blocks_done = 0;
+    }
+  }
+}
+__global__ void k_ktimer_reset(KTimer *tm, int on) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    tm->t0 = ~0ull;
+    tm->t1 = 0;
+    tm->total_ns = tm->launches = tm->items = 0;
+    tm->blocks_done = 0;
+    tm->on = on;
+  }
+}
+
+constexpr int kFlipProfileBins = 32;
 struct FlipCtl {
   int gen;          // generation of the stamps of the current step
   unsigned epoch;   // launch epoch of the subseg2tri stores (all kernels share it)
@@ -773,6 +826,8 @@ struct FlipCtl {
   int cond;         // loop condition of the last step
   long long cap;    // bound on the steps of one loop
   int *errp;        // device error word (GQM_ERR_ROUND_LIMIT on cap_hit)
+  // step profile of the run: steps and active triangles by floor(log2 |A|)
+  unsigned long long prof_steps[kFlipProfileBins], prof_items[kFlipProfileBins];
 };
 struct FlipQ {
   int *q;           // next queue
@@ -803,6 +858,11 @@ __device__ __forceinline__ void claim(const Mesh &M, const TouchL &T, int t, int
 // the counters of the next step are prepared here.
 __device__ __forceinline__ int flip_next(FlipCtl *c) {
   int cond = c->nact > 0;
+  if (cond) {
+    int b = 31 - __clz(c->nact);
+    c->prof_steps[b]++;
+    c->prof_items[b] += (unsigned long long)c->nact;
+  }
   if (cond && (long long)(c->steps - c->entry_steps) >= c->cap) {
     cond = 0;
     c->cap_hit = 1;
@@ -851,6 +911,10 @@ __global__ void k_bump_epoch(FlipCtl *c) {
 // per-run reset of the control block; gen and epoch keep growing across runs
 // so that stamps and subseg2tri tags left by earlier runs never collide
 __global__ void k_ctl_reset(FlipCtl *c, long long cap, int *errp) {
+  if (blockIdx.x == 0 && threadIdx.x < kFlipProfileBins) {
+    c->prof_steps[threadIdx.x] = 0;
+    c->prof_items[threadIdx.x] = 0;
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     c->steps = 0;
     c->entry_steps = 0;
@@ -889,7 +953,10 @@ __global__ void k_flip_reset_touched(Mesh M, const int *tl, const int *tn, int *
 // (the decision is kept in clr[k] and applied by k_flip_winner2), so the
 // neighbour flags read below are the ones the step started with.
 template <int PRED>
-__global__ void GQM_WALK_BOUNDS k_check_flip2(Mesh M, const int *act, const int *dn, uint8_t *clr, TouchL T) {
+__global__ void GQM_WALK_BOUNDS k_check_flip2(Mesh M, const int *act, const int *dn, uint8_t *clr, TouchL T,
+                                              KTimer *tm) {
+  const int timed = tm->on;
+  const unsigned long long start = timed ? global_ns() : 0;
   int n = *dn;
   GS_LOOP(k, n) {
     int index = act[k];
@@ -1017,6 +1084,7 @@ __global__ void GQM_WALK_BOUNDS k_check_flip2(Mesh M, const int *act, const int 
     }
     clr[k] = done ? 0 : 1;
   }
+  if (timed) ktimer_end(tm, start, n);
 }
 
 // kernelMarkFlipWinner (refine.cu:1072-1170) on A; applies the deferred flag
@@ -1060,10 +1128,42 @@ __global__ void k_flip_winner2(Mesh M, const int *act, const int *dn, const uint
         w = (M.tmark[pOppTri] == index && M.tmark[t1] == index && M.tmark[t2] == index);
       }
     }
-    if (w)
+    if (w) {
       win[atomicAdd(winn, 1)] = index;
-    else
+      atomicOr(M.wbits + (index >> 5), 1u << (index & 31));
+      atomicAdd(M.wcnt + (index >> 10), 1);
+    } else {
       M.tfo[index] = 15;
+    }
+  }
+}
+
+// Exclusive prefix of the per-chunk winner counts (one block), which clears
+// the counts for the next step.
+__global__ void k_win_prefix(Mesh M, int nchunks) {
+  __shared__ int part[1024];
+  __shared__ int carry;
+  const int nt = (int)blockDim.x, t = (int)threadIdx.x;  // nt <= 1024
+  if (t == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < nchunks; base += nt) {
+    const int i = base + t;
+    const int c = i < nchunks ? M.wcnt[i] : 0;
+    part[t] = c;
+    __syncthreads();
+    for (int off = 1; off < nt; off <<= 1) {
+      const int v = t >= off ? part[t - off] : 0;
+      __syncthreads();
+      part[t] += v;
+      __syncthreads();
+    }
+    if (i < nchunks) {
+      M.wpre[i] = carry + part[t] - c;
+      M.wcnt[i] = 0;
+    }
+    __syncthreads();
+    if (t == nt - 1) carry += part[nt - 1];
+    __syncthreads();
   }
 }
 
@@ -1088,7 +1188,11 @@ struct QueueFlag {
 __global__ void k_phase3q(Mesh M, const int *win, const int *dn, const int *sl, FlipQ Q) {
   int n = *dn;
   QueueFlag f{&M, &Q};
-  GS_LOOP(pos, n) phase3_body(M, pos, win[pos], sl, f);
+  GS_LOOP(pos, n) {
+    const int index = win[pos];
+    phase3_body(M, pos, index, sl, f);
+    atomicAnd(M.wbits + (index >> 5), ~(1u << (index & 31)));  // phase 1 has read the bitmap
+  }
 }
 
 // kernelMarkReduntantSteiner (refine.cu:2298-2326) over the claimed triangles
@@ -1222,11 +1326,11 @@ __global__ void GQM_WALK_BOUNDS k_insert_mid(Mesh M, const int *mids, const int 
     int seg[3] = {comp(s0, triOri[0]), comp(s0, m3(triOri[0] + 1)), comp(s0, m3(triOri[0] + 2))};
     M.tsg[tri[0]] = make_int4(seg[2], seg[0], -1, 0);
     M.tsg[tri[1]] = make_int4(seg[1], -1, nsub + tindex, 0);
-    s2t_store(M, seg[0], (tri[0] << 2) | 1, epoch);
-    s2t_store(M, nsub + tindex, (tri[1] << 2) | 2, epoch);
+    s2t_store(M, seg[0], (tri[0] << 2) | 1, epoch, wkey(pos, 0));
+    s2t_store(M, nsub + tindex, (tri[1] << 2) | 2, epoch, wkey(pos, 1));
     M.s2seg[nsub + tindex] = M.s2seg[seg[0]];
-    if (seg[1] != -1) s2t_store(M, seg[1], (tri[1] << 2) | 0, epoch);
-    if (seg[2] != -1) s2t_store(M, seg[2], (tri[0] << 2) | 0, epoch);
+    if (seg[1] != -1) s2t_store(M, seg[1], (tri[1] << 2) | 0, epoch, wkey(pos, 2));
+    if (seg[2] != -1) s2t_store(M, seg[2], (tri[0] << 2) | 0, epoch, wkey(pos, 3));
     int e_s = -1, e_n = -1;
     if (encroached(a, m, c, M.gc2, M.mode)) e_s = 0;
     if (encroached(m, b, c, M.gc2, M.mode)) e_n = 0;
@@ -1250,8 +1354,8 @@ __global__ void GQM_WALK_BOUNDS k_insert_mid(Mesh M, const int *mids, const int 
       int sg2[3] = {comp(s2, triOri[1]), comp(s2, m3(triOri[1] + 1)), comp(s2, m3(triOri[1] + 2))};
       M.tsg[tri[2]] = make_int4(sg2[1], -1, sg2[0], 0);
       M.tsg[tri[3]] = make_int4(sg2[2], nsub + tindex, -1, 0);
-      if (sg2[1] != -1) s2t_store(M, sg2[1], (tri[2] << 2) | 0, epoch);
-      if (sg2[2] != -1) s2t_store(M, sg2[2], (tri[3] << 2) | 0, epoch);
+      if (sg2[1] != -1) s2t_store(M, sg2[1], (tri[2] << 2) | 0, epoch, wkey(pos, 4));
+      if (sg2[2] != -1) s2t_store(M, sg2[2], (tri[3] << 2) | 0, epoch, wkey(pos, 5));
       int4 v2 = M.tv[tri[2]];
       int q[3] = {comp(v2, m3(triOri[1] + 1)), comp(v2, m3(triOri[1] + 2)), comp(v2, triOri[1])};
       double2 qa = M.pts[q[0]], qb = M.pts[q[1]], qc = M.pts[q[2]];
@@ -1662,9 +1766,9 @@ __global__ void k_insert_steiner(Mesh M, const int *wl, const int *dn, const int
       M.tsg[t0] = make_int4(s0.x, -1, -1, 0);
       M.tsg[t1] = make_int4(s0.y, -1, -1, 0);
       M.tsg[t2] = make_int4(s0.z, -1, -1, 0);
-      if (s0.x != -1) s2t_store(M, s0.x, (t0 << 2) | 0, epoch);
-      if (s0.y != -1) s2t_store(M, s0.y, (t1 << 2) | 0, epoch);
-      if (s0.z != -1) s2t_store(M, s0.z, (t2 << 2) | 0, epoch);
+      if (s0.x != -1) s2t_store(M, s0.x, (t0 << 2) | 0, epoch, wkey(pos, 0));
+      if (s0.y != -1) s2t_store(M, s0.y, (t1 << 2) | 0, epoch, wkey(pos, 1));
+      if (s0.z != -1) s2t_store(M, s0.z, (t2 << 2) | 0, epoch, wkey(pos, 2));
       // p[i] = vertex (i+1)%3 of the old triangle; neighbour[i] = old edge i
       M.tv[t0] = make_int4(newp, v0.y, v0.z, 0);
       M.tn[t0] = make_int4(n0.x, (t1 << 2) | 2, (t2 << 2) | 1, 0);
@@ -1690,8 +1794,8 @@ __global__ void k_insert_steiner(Mesh M, const int *wl, const int *dn, const int
       int seg[3] = {comp(s0, o0), comp(s0, m3(o0 + 1)), comp(s0, m3(o0 + 2))};
       M.tsg[tri0] = make_int4(seg[2], seg[0], -1, 0);
       M.tsg[tri1] = make_int4(seg[1], -1, seg[0], 0);
-      if (seg[1] != -1) s2t_store(M, seg[1], (tri1 << 2) | 0, epoch);
-      if (seg[2] != -1) s2t_store(M, seg[2], (tri0 << 2) | 0, epoch);
+      if (seg[1] != -1) s2t_store(M, seg[1], (tri1 << 2) | 0, epoch, wkey(pos, 3));
+      if (seg[2] != -1) s2t_store(M, seg[2], (tri0 << 2) | 0, epoch, wkey(pos, 4));
       int nb1 = comp(n0, m3(o0 + 1)), nb2 = comp(n0, m3(o0 + 2));
       M.tv[tri0] = make_int4(newp, p2, p0, 0);
       M.tv[tri1] = make_int4(newp, p1, p2, 0);
@@ -1714,8 +1818,8 @@ __global__ void k_insert_steiner(Mesh M, const int *wl, const int *dn, const int
         int sg2[3] = {comp(s2, o1), comp(s2, m3(o1 + 1)), comp(s2, m3(o1 + 2))};
         M.tsg[tri2] = make_int4(sg2[1], -1, sg2[0], 0);
         M.tsg[tri3] = make_int4(sg2[2], sg2[0], -1, 0);
-        if (sg2[1] != -1) s2t_store(M, sg2[1], (tri2 << 2) | 0, epoch);
-        if (sg2[2] != -1) s2t_store(M, sg2[2], (tri3 << 2) | 0, epoch);
+        if (sg2[1] != -1) s2t_store(M, sg2[1], (tri2 << 2) | 0, epoch, wkey(pos, 5));
+        if (sg2[2] != -1) s2t_store(M, sg2[2], (tri3 << 2) | 0, epoch, wkey(pos, 6));
         int m1 = comp(n2, m3(o1 + 1)), m2 = comp(n2, m3(o1 + 2));
         M.tv[tri2] = make_int4(newp, q1, q2, 0);
         M.tn[tri2] = make_int4(m1, (tri3 << 2) | 2, (tri0 << 2) | 1, 0);
@@ -1800,7 +1904,7 @@ __global__ void k_fix_nbrs(Mesh M, const int *newidx, int newn) {
 __global__ void k_fix_s2t(Mesh M, const int *newidx, int ns) {
   GS_LOOP(s, ns) {
     int o = s2t_get(M, s);
-    if (o >= 0) M.s2t[s] = (unsigned long long)(uint32_t)etri(newidx[dtri(o)], dori(o));
+    if (o >= 0) M.s2t[s] = s2t_plain(etri(newidx[dtri(o)], dori(o)));
   }
 }
 __global__ void k_compact_pts_move(Mesh M, const int *tail, const int *empty, const int *dn, int *newidx) {

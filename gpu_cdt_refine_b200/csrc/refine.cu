@@ -199,6 +199,12 @@ struct Refiner {
   int *fq = nullptr, *tl = nullptr;  // flip-step queue and claimed-triangle list
   uint8_t *clr = nullptr;            // deferred flag clears of a flip step
   FlipCtl *fc = nullptr;             // flip-loop control block (device)
+  KTimer *ktm = nullptr;             // launch timer of the flip-step check kernel
+  bool probing = false;              // events around every flip-loop launch
+  std::vector<cudaEvent_t> loop_ev;  // pairs, reused every run
+  size_t loop_ev_used = 0;
+  double probe_loop_ms = 0.0;
+  long long probe_loops = 0;
   // the flip-flop loop as a CUDA graph with a device-side while condition
   bool use_graph = true;
   cudaGraph_t flip_graph = nullptr;
@@ -227,6 +233,7 @@ struct Refiner {
   // result sizes
   int out_np = 0, out_nt = 0, out_ns = 0;
   bool have_result = false;
+  long long flip_prof_steps[kFlipProfileBins] = {}, flip_prof_items[kFlipProfileBins] = {};
 
   enum { C_LIST0 = 0, C_LIST1, C_LIST2, C_LIST3, C_LIST4, C_LIST5, C_MISC, C_QN, C_TN };
 
@@ -266,7 +273,7 @@ struct Refiner {
     void *ptrs[] = {M.pts, M.ps, M.pred, M.tv, M.tn, M.tsg, M.tst, M.tflip, M.tfo, M.flip0, M.tmark, M.tpos,
                     M.s2t, M.s2seg, M.enc, M.err, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
                     newidx, tail, center, emptyp, pnew, enclist, encl2, smark, mids, snap, segs, dcount, bc,
-                    dctr, dgc, dinput, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn};
+                    dctr, dgc, dinput, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wpre};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     if (hcount) cudaFreeHost(hcount);
@@ -276,6 +283,10 @@ struct Refiner {
     fq = tl = nullptr;
     clr = nullptr;
     fc = nullptr;
+    ktm = nullptr;
+    for (cudaEvent_t e : loop_ev) cudaEventDestroy(e);
+    loop_ev.clear();
+    loop_ev_used = 0;
     center = nullptr;
     cav = cavn = nullptr;
     cav_cap = 0;
@@ -302,9 +313,10 @@ struct Refiner {
     if (!ev1) cudaEventCreate(&ev1);
     if (!dcount) {
       if (dalloc(&dcount, 16) || dalloc(&bc, kMaxCompactBlocks + 1) || dalloc(&dctr, 4) || dalloc(&dgc, 2) ||
-          dalloc(&M.err, 1) || dalloc(&fc, 1))
+          dalloc(&M.err, 1) || dalloc(&fc, 1) || dalloc(&ktm, 1))
         return GQM_ERR_MEMORY;
       cudaMemsetAsync(fc, 0, sizeof(FlipCtl), st);
+      cudaMemsetAsync(ktm, 0, sizeof(KTimer), st);  // off until gqm_context_probe
 #ifdef GQM_HOST_EMU
       use_graph = false;
 #else
@@ -403,8 +415,12 @@ struct Refiner {
         regrow(&act, old, n) || regrow(&win, old, n) || regrow(&neg, old, n) || regrow(&ll, 2 * old, 2 * n) ||
         regrow(&sl, 6 * old, 6 * n) || regrow(&newidx, 0, n) || regrow(&tail, 0, std::max<long>(n, pphys)) ||
         regrow(&center, old, n) || regrow(&M.fstamp, old, n) || regrow(&M.tstamp, old, n) || regrow(&fq, 0, n) ||
-        regrow(&tl, 0, n) || regrow(&clr, 0, n))
+        regrow(&tl, 0, n) || regrow(&clr, 0, n) || regrow(&M.wbits, 0, n / 32 + 1) ||
+        regrow(&M.wcnt, 0, n / 1024 + 1) || regrow(&M.wpre, 0, n / 1024 + 1))
       return GQM_ERR_MEMORY;
+    // winner bitmap and chunk counts are all zero between flip steps
+    cudaMemsetAsync(M.wbits, 0, sizeof(unsigned) * (n / 32 + 1), st);
+    cudaMemsetAsync(M.wcnt, 0, sizeof(int) * (n / 1024 + 1), st);
     if (n > old) {
       cudaMemsetAsync(M.tst + old, 0, n - old, st);
       cudaMemsetAsync(M.tflip + old, 0, n - old, st);
@@ -424,7 +440,7 @@ struct Refiner {
         regrow(&encl2, old, n) || regrow(&smark, old, n) || regrow(&mids, old, n) || regrow(&snap, old, n))
       return GQM_ERR_MEMORY;
     // new subsegment entries start at epoch 0 so that the first tagged store wins
-    cudaMemsetAsync(M.s2t + old, 0, sizeof(unsigned long long) * (n - old), st);
+    cudaMemsetAsync(M.s2t + old, 0, sizeof(s2t_t) * (n - old), st);
     sphys = n;
     return GQM_OK;
   }
@@ -507,10 +523,11 @@ struct Refiner {
     FlipQ Q{fq, &fc->qn, &fc->gen};
     TouchL T{tl, &fc->tn, &fc->gen};
     if (pred_mode)
-      KL(k_check_flip2<1>, kStepGrid, 256)(M, act, &fc->nact, clr, T);
+      KL(k_check_flip2<1>, kStepGrid, 256)(M, act, &fc->nact, clr, T, ktm);
     else
-      KL(k_check_flip2<0>, kStepGrid, 256)(M, act, &fc->nact, clr, T);
+      KL(k_check_flip2<0>, kStepGrid, 256)(M, act, &fc->nact, clr, T, ktm);
     KL(k_flip_winner2, kStepGrid, 256)(M, act, &fc->nact, clr, Q, win, &fc->winn);
+    KL(k_win_prefix, 1, 1024)(M, (int)(tphys / 1024 + 1));
     KL(k_link_phase1, kStepGrid, 256)(M, win, &fc->winn, ll, sl, &fc->epoch);
     KL(k_phase2, kStepGrid, 256)(M, win, &fc->winn, ll, sl);
     KL(k_phase3q, kStepGrid, 256)(M, win, &fc->winn, sl, Q);
@@ -582,6 +599,24 @@ struct Refiner {
     return GQM_OK;
 #endif
   }
+  // next pair of probe events (nullptr when none can be created)
+  cudaEvent_t *loop_events() {
+    while (loop_ev.size() < 2 * (loop_ev_used + 1)) {
+      cudaEvent_t e;
+      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+      loop_ev.push_back(e);
+    }
+    return &loop_ev[2 * loop_ev_used++];
+  }
+  // after the run's final sync: add the probe events' intervals to the totals
+  void collect_loop_events() {
+    for (size_t i = 0; i < loop_ev_used; ++i) {
+      float ms = 0.0f;
+      if (cudaEventElapsedTime(&ms, loop_ev[2 * i], loop_ev[2 * i + 1]) == cudaSuccess) probe_loop_ms += ms;
+      probe_loops++;
+    }
+    loop_ev_used = 0;
+  }
   int flip_flop(int ntri) {
     LAUNCH(k_flip_entry_reset, ntri, M, ntri);
     compact_to(PNotNullFlag{M.tst, M.tflip}, Ident{}, 0, ntri, act, &fc->nact);
@@ -594,7 +629,10 @@ struct Refiner {
       }
     }
     if (use_graph) {
+      cudaEvent_t *ev = probing ? loop_events() : nullptr;
+      if (ev) cudaEventRecord(ev[0], st);
       if (cudaGraphLaunch(flip_exec, st) != cudaSuccess) return GQM_ERR_CUDA;
+      if (ev) cudaEventRecord(ev[1], st);
       stats.kernel_launches++;
       return GQM_OK;
     }
@@ -816,7 +854,11 @@ struct Refiner {
     if (dalloc(&segs, ns + 1)) return GQM_ERR_MEMORY;
     if (ns) cudaMemcpyAsync(segs, dseg_in, sizeof(int2) * ns, cudaMemcpyDeviceToDevice, st);
     M.segs = segs;
-    cudaMemsetAsync(M.s2t, 0, sizeof(unsigned long long) * sphys, st);
+    cudaMemsetAsync(M.s2t, 0, sizeof(s2t_t) * sphys, st);
+    if (M.wbits) {  // left set only by a run that stopped inside a flip step
+      cudaMemsetAsync(M.wbits, 0, sizeof(unsigned) * (tphys / 32 + 1), st);
+      cudaMemsetAsync(M.wcnt, 0, sizeof(int) * (tphys / 1024 + 1), st);
+    }
     cudaMemsetAsync(M.err, 0, sizeof(int), st);
     cudaMemsetAsync(dctr, 0, sizeof(unsigned long long) * 4, st);
     KL(k_ctl_reset, 1, 32)(fc, 64 * max_rounds, M.err);
@@ -893,11 +935,16 @@ struct Refiner {
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
     stats.device_ms = ms;
+    collect_loop_events();
     unsigned long long hc[4];
     cudaMemcpy(hc, dctr, sizeof(hc), cudaMemcpyDeviceToHost);
     FlipCtl hf;
     cudaMemcpy(&hf, fc, sizeof(hf), cudaMemcpyDeviceToHost);
     stats.flip_steps = hf.steps;
+    for (int b = 0; b < kFlipProfileBins; ++b) {
+      flip_prof_steps[b] = (long long)hf.prof_steps[b];
+      flip_prof_items[b] = (long long)hf.prof_items[b];
+    }
     stats.steiner_inserted = (long long)hc[0];
     stats.midpoints_inserted = (long long)hc[1];
     stats.exact_fallbacks = (long long)hc[2];
@@ -993,6 +1040,43 @@ int gqm_context_run(gqm_context *ctx, const gqm_cdt_in *in, int in_on_device, co
 int gqm_context_result(gqm_context *ctx, gqm_cdt_out *out) {
   if (!ctx || !out) return GQM_ERR_ARGUMENT;
   return ctx->r.result(out);
+}
+int gqm_context_probe(gqm_context *ctx, int enable) {
+  if (!ctx || !ctx->r.ktm) return GQM_ERR_ARGUMENT;
+  gqm::Refiner &r = ctx->r;
+  if (cudaSetDevice(r.device) != cudaSuccess) return GQM_ERR_CUDA;
+#ifdef GQM_HOST_EMU
+  gqm::k_ktimer_reset(r.ktm, enable ? 1 : 0);
+#else
+  gqm::k_ktimer_reset<<<1, 32, 0, r.st>>>(r.ktm, enable ? 1 : 0);
+#endif
+  r.probing = enable != 0;
+  r.probe_loop_ms = 0.0;
+  r.probe_loops = 0;
+  return cudaStreamSynchronize(r.st) == cudaSuccess ? GQM_OK : GQM_ERR_CUDA;
+}
+int gqm_context_probe_read(gqm_context *ctx, gqm_probe *p) {
+  if (!ctx || !p || !ctx->r.ktm) return GQM_ERR_ARGUMENT;
+  gqm::Refiner &r = ctx->r;
+  if (cudaSetDevice(r.device) != cudaSuccess) return GQM_ERR_CUDA;
+  gqm::KTimer h;
+  if (cudaStreamSynchronize(r.st) != cudaSuccess ||
+      cudaMemcpy(&h, r.ktm, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return GQM_ERR_CUDA;
+  p->check_launches = (long long)h.launches;
+  p->check_items = (long long)h.items;
+  p->check_ms = (double)h.total_ns * 1e-6;
+  p->loop_launches = r.probe_loops;
+  p->loop_ms = r.probe_loop_ms;
+  return GQM_OK;
+}
+int gqm_context_flip_profile(gqm_context *ctx, long long *steps, long long *items) {
+  if (!ctx || !steps || !items) return GQM_ERR_ARGUMENT;
+  for (int b = 0; b < gqm::kFlipProfileBins; ++b) {
+    steps[b] = ctx->r.flip_prof_steps[b];
+    items[b] = ctx->r.flip_prof_items[b];
+  }
+  return GQM_OK;
 }
 int gqm_context_result_sizes(gqm_context *ctx, int *np, int *nt, int *ns) {
   if (!ctx || !ctx->r.have_result) return GQM_ERR_ARGUMENT;

@@ -93,6 +93,9 @@ def lib() -> ctypes.CDLL:
                                        ctypes.POINTER(Options), ctypes.POINTER(Stats), ctypes.c_int,
                                        ctypes.POINTER(ctypes.c_int)]
         L.gqm_refine_batch.restype = ctypes.c_int
+        L.gqm_context_flip_profile.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
+                                               ctypes.POINTER(ctypes.c_longlong)]
+        L.gqm_context_flip_profile.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -242,6 +245,14 @@ class Context:
         if rc != 0:
             raise RefineError(rc, "no result")
         return a.value, b.value, c.value
+
+    def flip_profile(self):
+        """(steps, items) per floor(log2 |active set|) bin of the last run's flip steps."""
+        st, it = (ctypes.c_longlong * 32)(), (ctypes.c_longlong * 32)()
+        rc = self._lib.gqm_context_flip_profile(self._h, st, it)
+        if rc != 0:
+            raise RefineError(rc, "flip profile")
+        return list(st), list(it)
 
     def result(self, with_status=False):
         out = CdtOut()

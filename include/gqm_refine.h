@@ -113,6 +113,26 @@ int gqm_context_run(gqm_context *ctx, const gqm_cdt_in *in, int in_on_device, co
 int gqm_context_result(gqm_context *ctx, gqm_cdt_out *out);
 /* Sizes of the last result without copying it. */
 int gqm_context_result_sizes(gqm_context *ctx, int *npoints, int *ntriangles, int *nsegments);
+/* Measurement probe (no counterpart in the reference).  While enabled, the
+ * flip-step check kernel (the refinement's most time-consuming kernel)
+ * timestamps every launch on the device: from its first block's start to its
+ * last block's end (%globaltimer), and CUDA events on the context's stream
+ * bracket every launch of the flip loop.  gqm_context_probe(ctx, 1) resets and
+ * enables, (ctx, 0) disables; gqm_context_probe_read sums since the reset. */
+typedef struct {
+  long long check_launches; /* launches of the flip-step check kernel */
+  long long check_items;    /* active triangles they checked */
+  double check_ms;          /* their summed execution time */
+  long long loop_launches;  /* flip-loop graph launches */
+  double loop_ms;           /* their summed time (CUDA events) */
+} gqm_probe;
+int gqm_context_probe(gqm_context *ctx, int enable);
+int gqm_context_probe_read(gqm_context *ctx, gqm_probe *p);
+
+/* Flip-step profile of the last run (no counterpart in the reference):
+ * steps[b] = flip steps whose active set held [2^b, 2^(b+1)) triangles,
+ * items[b] = those steps' active triangles summed; 32 bins each. */
+int gqm_context_flip_profile(gqm_context *ctx, long long *steps, long long *items);
 /* The CUDA stream the context launches on (a cudaStream_t). */
 void *gqm_context_stream(gqm_context *ctx);
 

@@ -26,7 +26,8 @@
  *     same subseg2tri entry (a subsegment whose two sides belong to two
  *     different winners: refine.cu:1362-1372, 1419-1424, 1533-1544,
  *     2844-2850, 2900-2903, 4744-4749, 4814-4817, 4873-4876).  Rule: within
- *     one kernel launch the largest stored value wins.
+ *     one kernel launch, the store that lands is decided by the storing
+ *     threads' warps and lanes and the stores' program order (wkey below).
  *  Everything else the reference does concurrently is order independent.
  *
  * Deliberate difference: initSubsegs (refine.cu:5691-5747) does not reset
@@ -40,6 +41,7 @@
 
 #include <math.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -393,7 +395,8 @@ typedef struct {
   unsigned char *ts;
   int *tmark;           /* t_trimarker, also the flipBy array, tcap */
   IV s2t, s2seg, enc;   /* per subsegment */
-  unsigned *s2t_epoch;  /* rule R2 */
+  unsigned *s2t_epoch;  /* rule R2: launch of the last store */
+  unsigned *s2t_key;    /* rule R2: writer key of the last store (wkey) */
   long s2t_epoch_cap;
   unsigned epoch;
   int *segs;
@@ -412,20 +415,36 @@ typedef struct {
 } St;
 
 static void s2t_begin(St *S) { S->epoch++; }
-static void s2t_set(St *S, int s, int v) {
+/* Key of one store to subseg2tri inside a launch (rule R2).  When several
+ * threads of one launch store into the same subseg2tri entry, the store with
+ * the largest key is the one kept, where the key orders the stores as the
+ * reference's runs on a B200 were seen to land them:
+ *   - two stores of one warp from different store instructions: the later
+ *     instruction in program order lands last (a warp issues its stores in
+ *     order);
+ *   - two lanes of one store instruction: the lower lane's value is kept;
+ *   - two different warps: the lower warp's store is kept.
+ * Across warps the order is a race in the reference; this choice is the one
+ * that the reference's own flip-step traces (tests/golden) follow on every
+ * seeded configuration recorded there.  pos is the thread's position in the
+ * launch, slot the store's place in the kernel's program order. */
+static unsigned wkey(long pos, int slot) {
+  return (unsigned)(((0x7FFFFFL - (pos >> 5)) << 9) | ((long)slot << 5) | (31 - (pos & 31)));
+}
+static void s2t_set(St *S, int s, int v, unsigned key) {
   if (s >= S->s2t_epoch_cap) {
     long c = S->s2t_epoch_cap ? S->s2t_epoch_cap : 64;
     while (c <= s) c *= 2;
     S->s2t_epoch = (unsigned *)realloc(S->s2t_epoch, sizeof(unsigned) * c);
+    S->s2t_key = (unsigned *)realloc(S->s2t_key, sizeof(unsigned) * c);
     memset(S->s2t_epoch + S->s2t_epoch_cap, 0, sizeof(unsigned) * (c - S->s2t_epoch_cap));
+    memset(S->s2t_key + S->s2t_epoch_cap, 0, sizeof(unsigned) * (c - S->s2t_epoch_cap));
     S->s2t_epoch_cap = c;
   }
-  if (S->s2t_epoch[s] == S->epoch) {
-    if (v > S->s2t.a[s]) S->s2t.a[s] = v;
-  } else {
-    S->s2t.a[s] = v;
-    S->s2t_epoch[s] = S->epoch;
-  }
+  if (S->s2t_epoch[s] == S->epoch && S->s2t_key[s] > key) return;
+  S->s2t.a[s] = v;
+  S->s2t_epoch[s] = S->epoch;
+  S->s2t_key[s] = key;
 }
 
 static void grow_points(St *S, long ncap) {
@@ -760,10 +779,10 @@ static void phase1(St *S, int pos, int index, int *sl) {
     S->t2s[3 * pOppTri + pOppOri] = sApex;
     S->t2s[3 * pOppTri + (pOppOri + 2) % 3] = spApex;
     S->t2s[3 * pOppTri + (pOppOri + 1) % 3] = -1;
-    if (sOrg != -1) s2t_set(S, sOrg, (index << 2) | ori);
-    if (spDest != -1) s2t_set(S, spDest, (index << 2) | ((ori + 1) % 3));
-    if (sApex != -1) s2t_set(S, sApex, (pOppTri << 2) | pOppOri);
-    if (spApex != -1) s2t_set(S, spApex, (pOppTri << 2) | ((pOppOri + 2) % 3));
+    if (sOrg != -1) s2t_set(S, sOrg, (index << 2) | ori, wkey(pos, 0));
+    if (spDest != -1) s2t_set(S, spDest, (index << 2) | ((ori + 1) % 3), wkey(pos, 1));
+    if (sApex != -1) s2t_set(S, sApex, (pOppTri << 2) | pOppOri, wkey(pos, 2));
+    if (spApex != -1) s2t_set(S, spApex, (pOppTri << 2) | ((pOppOri + 2) % 3), wkey(pos, 3));
     ts_set(&S->ts[index], TS_CHECK, 1);
     ts_set(&S->ts[pOppTri], TS_CHECK, 1);
   } else if (ori < 6) {
@@ -788,9 +807,9 @@ static void phase1(St *S, int pos, int index, int *sl) {
     S->t2s[3 * index + (ori + 1) % 3] = sOrg;
     S->t2s[3 * index + ori] = sApex;
     S->t2s[3 * index + (ori + 2) % 3] = sDest;
-    if (sOrg != -1) s2t_set(S, sOrg, (index << 2) | ((ori + 1) % 3));
-    if (sApex != -1) s2t_set(S, sApex, (index << 2) | ori);
-    if (sDest != -1) s2t_set(S, sDest, (index << 2) | ((ori + 2) % 3));
+    if (sOrg != -1) s2t_set(S, sOrg, (index << 2) | ((ori + 1) % 3), wkey(pos, 4));
+    if (sApex != -1) s2t_set(S, sApex, (index << 2) | ori, wkey(pos, 5));
+    if (sDest != -1) s2t_set(S, sDest, (index << 2) | ((ori + 2) % 3), wkey(pos, 6));
     ts_set(&S->ts[index], TS_CHECK, 1);
     ts_set(&S->ts[t1], TS_NOTNULL, 0);
     ts_set(&S->ts[t2], TS_NOTNULL, 0);
@@ -856,12 +875,12 @@ static void phase1(St *S, int pos, int index, int *sl) {
     S->t2s[3 * t1 + t1_ori] = snOrg;
     S->t2s[3 * t1 + (t1_ori + 1) % 3] = snDest;
     S->t2s[3 * t1 + (t1_ori + 2) % 3] = snApex;
-    if (sOrg != -1) s2t_set(S, sOrg, (index << 2) | ori);
-    if (sDest != -1) s2t_set(S, sDest, (index << 2) | ((ori + 1) % 3));
-    if (sApex != -1) s2t_set(S, sApex, (index << 2) | ((ori + 2) % 3));
-    if (snOrg != -1) s2t_set(S, snOrg, (t1 << 2) | t1_ori);
-    if (snDest != -1) s2t_set(S, snDest, (t1 << 2) | ((t1_ori + 1) % 3));
-    if (snApex != -1) s2t_set(S, snApex, (t1 << 2) | ((t1_ori + 2) % 3));
+    if (sOrg != -1) s2t_set(S, sOrg, (index << 2) | ori, wkey(pos, 7));
+    if (sDest != -1) s2t_set(S, sDest, (index << 2) | ((ori + 1) % 3), wkey(pos, 8));
+    if (sApex != -1) s2t_set(S, sApex, (index << 2) | ((ori + 2) % 3), wkey(pos, 9));
+    if (snOrg != -1) s2t_set(S, snOrg, (t1 << 2) | t1_ori, wkey(pos, 10));
+    if (snDest != -1) s2t_set(S, snDest, (t1 << 2) | ((t1_ori + 1) % 3), wkey(pos, 11));
+    if (snApex != -1) s2t_set(S, snApex, (t1 << 2) | ((t1_ori + 2) % 3), wkey(pos, 12));
     ts_set(&S->ts[index], TS_CHECK, 1);
     ts_set(&S->ts[t1], TS_CHECK, 1);
     ts_set(&S->ts[pOppTri], TS_NOTNULL, 0);
@@ -1108,6 +1127,86 @@ static void mark_redundant_steiner(St *S, int index) {
 }
 
 /* flipFlop, refine.cu:2328-2490 */
+/* ---------------- step trace (debugging aid of the test infrastructure) ----------------
+ * When enabled, one line per flip step with FNV-1a digests of the mesh arrays
+ * as kernelCheckFlipping (refine.cu:778) sees them at launch: the same line
+ * can be produced from the reference by interposing on its kernel launches,
+ * which finds the first step at which two runs part. */
+static FILE *g_trace;
+static long g_trace_seq, g_dump_step = -1;
+static char g_dump_path[512];
+void gqm_oracle_trace(const char *path) {
+  if (g_trace) fclose(g_trace);
+  g_trace = path ? fopen(path, "w") : NULL;
+  g_trace_seq = 0;
+}
+/* Also write the full arrays of flip step `step` (same layout as the trace's
+ * digests, after a 4-int header) to `path`. */
+void gqm_oracle_trace_dump(long step, const char *path) {
+  g_dump_step = path ? step : -1;
+  if (path) snprintf(g_dump_path, sizeof g_dump_path, "%s", path);
+}
+static unsigned long long fnv64(const void *p, size_t n) {
+  const unsigned char *b = (const unsigned char *)p;
+  unsigned long long h = 1469598103934665603ULL;
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ULL;
+  }
+  return h;
+}
+static int cmp_tri3(const void *a, const void *b) {
+  const int *x = (const int *)a, *y = (const int *)b;
+  for (int i = 0; i < 3; ++i)
+    if (x[i] != y[i]) return x[i] < y[i] ? -1 : 1;
+  return 0;
+}
+/* digest of the live triangles as a set: each rotated to start at its
+ * smallest vertex (orientation kept), sorted */
+static unsigned long long mesh_digest(const int *tri, const unsigned char *ts, int ntri) {
+  int *c = (int *)malloc(sizeof(int) * 3 * ((size_t)ntri + 1));
+  long m = 0;
+  for (int t = 0; t < ntri; ++t) {
+    if (!(ts[t] & TS_NOTNULL)) continue;
+    int a = tri[3 * t], b = tri[3 * t + 1], d = tri[3 * t + 2];
+    int k = (a <= b && a <= d) ? 0 : (b <= d ? 1 : 2);
+    int v[3] = {a, b, d};
+    for (int i = 0; i < 3; ++i) c[3 * m + i] = v[(k + i) % 3];
+    m++;
+  }
+  qsort(c, (size_t)m, sizeof(int) * 3, cmp_tri3);
+  unsigned long long h = fnv64(c, sizeof(int) * 3 * (size_t)m);
+  free(c);
+  return h;
+}
+static void trace_flip_step(St *S, int ntri, const IV *act) {
+  if (!g_trace) return;
+  int np = 0;
+  for (long i = 0; i < 3L * ntri; ++i)
+    if (S->tri[i] + 1 > np) np = S->tri[i] + 1;
+  fprintf(g_trace,
+          "F %ld nt=%d nact=%ld tri=%016llx nbr=%016llx t2s=%016llx ts=%016llx act=%016llx np=%d pts=%016llx "
+          "mesh=%016llx\n",
+          g_trace_seq++, ntri, act->n, fnv64(S->tri, sizeof(int) * 3L * ntri), fnv64(S->nbr, sizeof(int) * 3L * ntri),
+          fnv64(S->t2s, sizeof(int) * 3L * ntri), fnv64(S->ts, (size_t)ntri), fnv64(act->a, sizeof(int) * act->n), np,
+          fnv64(S->pts, sizeof(P2) * (size_t)np), mesh_digest(S->tri, S->ts, ntri));
+  fflush(g_trace);
+  if (g_trace_seq - 1 == g_dump_step) {
+    FILE *d = fopen(g_dump_path, "wb");
+    if (d) {
+      int hdr[4] = {(int)(g_trace_seq - 1), ntri, (int)act->n, np};
+      fwrite(hdr, 4, 4, d);
+      fwrite(S->tri, 4, 3L * ntri, d);
+      fwrite(S->nbr, 4, 3L * ntri, d);
+      fwrite(S->t2s, 4, 3L * ntri, d);
+      fwrite(S->ts, 1, (size_t)ntri, d);
+      fwrite(act->a, 4, (size_t)act->n, d);
+      fwrite(S->pts, sizeof(P2), (size_t)np, d);
+      fclose(d);
+    }
+  }
+}
+
 static void flip_flop(St *S, int ntri) {
   IV *act = &S->l3, *ll = &S->l4, *sl = &S->l5;
   unsigned char *flip0 = (unsigned char *)malloc((size_t)ntri + 1);
@@ -1125,6 +1224,7 @@ static void flip_flop(St *S, int ntri) {
     for (int t = 0; t < ntri; ++t) S->tmark[t] = MAXINT_REF;
     for (int t = 0; t < ntri; ++t) ts_setflipori(&S->ts[t], 15);
     for (int t = 0; t < ntri; ++t) flip0[t] = (S->ts[t] & TS_FLIP) ? 1 : 0;
+    trace_flip_step(S, ntri, act);
     for (long k = 0; k < act->n; ++k) check_flipping(S, act->a[k], flip0);
     for (long k = 0; k < act->n; ++k) mark_flip_winner(S, act->a[k]);
     /* winners: not null and flipOri != 15, ascending */
@@ -1194,7 +1294,7 @@ static void insert_tri(St *S, int v0, int v1, int v2, int t, int nA, int nO, int
 }
 
 /* kernelInsertMidPoints, refine.cu:2594-2927 (debug printing omitted) */
-static void insert_midpoint(St *S, int tindex, int *imarker, int nsub, int otri) {
+static void insert_midpoint(St *S, int pos, int tindex, int *imarker, int nsub, int otri) {
   int sindex = imarker[tindex];
   int tri[4], p[3], neighbor[3], seg[3], triOri[2];
   int acuteorg = 0, acutedest = 0;
@@ -1256,11 +1356,11 @@ static void insert_midpoint(St *S, int tindex, int *imarker, int nsub, int otri)
   S->t2s[3 * tri[1]] = seg[1];
   S->t2s[3 * tri[1] + 1] = -1;
   S->t2s[3 * tri[1] + 2] = nsub + tindex;
-  s2t_set(S, seg[0], (tri[0] << 2) | 1);
-  s2t_set(S, nsub + tindex, (tri[1] << 2) | 2);
+  s2t_set(S, seg[0], (tri[0] << 2) | 1, wkey(pos, 0));
+  s2t_set(S, nsub + tindex, (tri[1] << 2) | 2, wkey(pos, 1));
   S->s2seg.a[nsub + tindex] = S->s2seg.a[seg[0]];
-  if (seg[1] != -1) s2t_set(S, seg[1], tri[1] << 2 | 0);
-  if (seg[2] != -1) s2t_set(S, seg[2], tri[0] << 2 | 0);
+  if (seg[1] != -1) s2t_set(S, seg[1], tri[1] << 2 | 0, wkey(pos, 2));
+  if (seg[2] != -1) s2t_set(S, seg[2], tri[0] << 2 | 0, wkey(pos, 3));
   P2 v0 = S->pts[p[0]], v1 = S->pts[p[1]], v2 = S->pts[p[2]], v3 = S->pts[newp];
   if (encroached(v0, v3, v2, S->gc2, S->mode)) S->enc.a[sindex] = 0;
   if (encroached(v3, v1, v2, S->gc2, S->mode)) S->enc.a[nsub + tindex] = 0;
@@ -1289,8 +1389,8 @@ static void insert_midpoint(St *S, int tindex, int *imarker, int nsub, int otri)
     S->t2s[3 * tri[3]] = seg[2];
     S->t2s[3 * tri[3] + 1] = nsub + tindex;
     S->t2s[3 * tri[3] + 2] = -1;
-    if (seg[1] != -1) s2t_set(S, seg[1], tri[2] << 2 | 0);
-    if (seg[2] != -1) s2t_set(S, seg[2], tri[3] << 2 | 0);
+    if (seg[1] != -1) s2t_set(S, seg[1], tri[2] << 2 | 0, wkey(pos, 4));
+    if (seg[2] != -1) s2t_set(S, seg[2], tri[3] << 2 | 0, wkey(pos, 5));
     for (int i = 0; i < 3; i++) p[i] = S->tri[tri[2] * 3 + (triOri[1] + i + 1) % 3];
     v0 = S->pts[p[0]];
     v1 = S->pts[p[1]];
@@ -1464,7 +1564,7 @@ static void split_encsegs(St *S) {
       int *snap = (int *)malloc(sizeof(int) * (nmid + 1));
       for (int k = 0; k < nmid; ++k) snap[k] = S->s2t.a[imark->a[ilist->a[k]]];
       s2t_begin(S);
-      for (int k = 0; k < nmid; ++k) insert_midpoint(S, ilist->a[k], imark->a, S->last_subseg, snap[k]);
+      for (int k = 0; k < nmid; ++k) insert_midpoint(S, k, ilist->a[k], imark->a, S->last_subseg, snap[k]);
       free(snap);
       for (int k = 0; k < nmid; ++k) update_mid_neighbors(S, ilist->a[k], imark->a, enclist->a);
     }
@@ -1722,9 +1822,9 @@ static void insert_steiner(St *S, int pos, int tindex, const int *sinks, const P
     S->t2s[3 * tri[2]] = seg[2];
     S->t2s[3 * tri[2] + 1] = -1;
     S->t2s[3 * tri[2] + 2] = -1;
-    if (seg[0] != -1) s2t_set(S, seg[0], tri[0] << 2 | 0);
-    if (seg[1] != -1) s2t_set(S, seg[1], tri[1] << 2 | 0);
-    if (seg[2] != -1) s2t_set(S, seg[2], tri[2] << 2 | 0);
+    if (seg[0] != -1) s2t_set(S, seg[0], tri[0] << 2 | 0, wkey(pos, 0));
+    if (seg[1] != -1) s2t_set(S, seg[1], tri[1] << 2 | 0, wkey(pos, 1));
+    if (seg[2] != -1) s2t_set(S, seg[2], tri[2] << 2 | 0, wkey(pos, 2));
     for (int i = 0; i < 3; i++) neighbor[i] = S->nbr[tri[0] * 3 + i];
     insert_tri(S, newp, p[0], p[1], tri[0], neighbor[0], tri[1] << 2 | 2, tri[2] << 2 | 1);
     insert_tri(S, newp, p[1], p[2], tri[1], neighbor[1], tri[2] << 2 | 2, tri[0] << 2 | 1);
@@ -1755,8 +1855,8 @@ static void insert_steiner(St *S, int pos, int tindex, const int *sinks, const P
     S->t2s[3 * tri[1]] = seg[1];
     S->t2s[3 * tri[1] + 1] = -1;
     S->t2s[3 * tri[1] + 2] = seg[0];
-    if (seg[1] != -1) s2t_set(S, seg[1], tri[1] << 2 | 0);
-    if (seg[2] != -1) s2t_set(S, seg[2], tri[0] << 2 | 0);
+    if (seg[1] != -1) s2t_set(S, seg[1], tri[1] << 2 | 0, wkey(pos, 3));
+    if (seg[2] != -1) s2t_set(S, seg[2], tri[0] << 2 | 0, wkey(pos, 4));
     neighbor[0] = S->nbr[tri[0] * 3 + triOri[0]];
     neighbor[1] = S->nbr[tri[0] * 3 + (triOri[0] + 1) % 3];
     neighbor[2] = S->nbr[tri[0] * 3 + (triOri[0] + 2) % 3];
@@ -1783,8 +1883,8 @@ static void insert_steiner(St *S, int pos, int tindex, const int *sinks, const P
       S->t2s[3 * tri[3]] = seg[2];
       S->t2s[3 * tri[3] + 1] = seg[0];
       S->t2s[3 * tri[3] + 2] = -1;
-      if (seg[1] != -1) s2t_set(S, seg[1], tri[2] << 2 | 0);
-      if (seg[2] != -1) s2t_set(S, seg[2], tri[3] << 2 | 0);
+      if (seg[1] != -1) s2t_set(S, seg[1], tri[2] << 2 | 0, wkey(pos, 5));
+      if (seg[2] != -1) s2t_set(S, seg[2], tri[3] << 2 | 0, wkey(pos, 6));
       neighbor[0] = S->nbr[tri[2] * 3 + triOri[1]];
       neighbor[1] = S->nbr[tri[2] * 3 + (triOri[1] + 1) % 3];
       neighbor[2] = S->nbr[tri[2] * 3 + (triOri[1] + 2) % 3];
@@ -2214,6 +2314,7 @@ int gqm_oracle_refine_gc(int np, const double *pts, int nt, const int *tri, cons
   free(S->s2seg.a);
   free(S->enc.a);
   free(S->s2t_epoch);
+  free(S->s2t_key);
   free(S->segs);
   free(S->emptyp.a);
   free(S->emptyt.a);

@@ -43,6 +43,10 @@ int gqm_oracle_refine_gc(int np, const double *pts, int nt, const int *tri, cons
                          gqm_oracle_out *out);
 void gqm_oracle_free(gqm_oracle_out *out);
 
+/* Debugging aid: write one digest line per flip step to `path` (NULL: off). */
+void gqm_oracle_trace(const char *path);
+void gqm_oracle_trace_dump(long step, const char *path);
+
 /* Reference predicate arithmetic, exported for the predicate tests. */
 double gqm_oracle_orient(const double *a, const double *b, const double *c);
 double gqm_oracle_incircle(const double *a, const double *b, const double *c, const double *d);

@@ -56,8 +56,34 @@ inline unsigned long long atomicMax(unsigned long long *a, unsigned long long v)
   if (v > o) *a = v;
   return o;
 }
+inline unsigned long long atomicMin(unsigned long long *a, unsigned long long v) {
+  unsigned long long o = *a;
+  if (v < o) *a = v;
+  return o;
+}
+inline unsigned atomicAdd(unsigned *a, unsigned v) {
+  unsigned o = *a;
+  *a += v;
+  return o;
+}
+inline void __threadfence() {}
+inline unsigned atomicOr(unsigned *a, unsigned v) {
+  unsigned o = *a;
+  *a |= v;
+  return o;
+}
+inline unsigned atomicAnd(unsigned *a, unsigned v) {
+  unsigned o = *a;
+  *a &= v;
+  return o;
+}
 inline unsigned long long atomicCAS(unsigned long long *a, unsigned long long c, unsigned long long v) {
   unsigned long long o = *a;
+  if (o == c) *a = v;
+  return o;
+}
+inline unsigned __int128 atomicCAS(unsigned __int128 *a, unsigned __int128 c, unsigned __int128 v) {
+  unsigned __int128 o = *a;
   if (o == c) *a = v;
   return o;
 }
@@ -87,6 +113,7 @@ inline unsigned __ballot_sync(unsigned, bool p) { return p ? 1u : 0u; }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
 inline int __shfl_up_sync(unsigned, int v, int) { return v; }
 inline int __ffs(unsigned v) { return __builtin_ffs(v); }
+inline int __clz(int v) { return v == 0 ? 32 : __builtin_clz((unsigned)v); }
 
 typedef int cudaError_t;
 typedef void *cudaStream_t;
