@@ -42,6 +42,18 @@ sys.path.insert(0, ROOT)
 
 METRIC = "output triangles/s at theta=20 deg, 1 B200 (learned vs plain); output vertex count"
 
+# Algorithmic bytes of the flip-step check kernel (k_check_flip2, the
+# kernelCheckFlipping of GPU_Refine/refine.cu:778-1070) per active triangle:
+# the list entry (4), the triangle's vertices, neighbours and subsegments
+# (3 x 12), the redundant flags of its vertices (3), its three points (48),
+# per edge the neighbour's flip flag, opposite vertex, its flag and point
+# (3 x 22), and the deferred-clear byte written back (1).
+CHECK_BYTES_PER_ITEM = 4 + 36 + 3 + 48 + 66 + 1
+# DRAM bytes (read + write) per active triangle of the same kernel, from
+# `ncu --set full` on its first launch of the 1,000,000-point clustered case
+# (profiles/k_check_flip2_clustered1M.md: 74.45 MB for 162,684 triangles).
+CHECK_DRAM_BYTES_PER_ITEM = 74.45e6 / 162684
+
 
 def parse():
     p = argparse.ArgumentParser()
@@ -217,6 +229,11 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     ms = ms_total / args.steps
+    # one more step with the device-side launch timer of the dominant kernel on
+    ctx.probe(True)
+    step()
+    probe = ctx.probe_read()
+    ctx.probe(False)
     from gpu_cdt_refine_b200 import replicas
     ms_max, tris_all = replicas.reduce_step(ms, nt_out, device=dev)
     value = tris_all / (ms_max / 1e3)
@@ -234,11 +251,17 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0:
         peak, peak_kind = measured_peak()
         s = stats[-1]
+        # dominant kernel: the flip-step check, timed on the device per launch
+        launches = max(int(probe["check_launches"]), 1)
+        items_per_launch = probe["check_items"] / launches
+        launch_s = probe["check_ms"] / 1e3 / launches
+        achieved = CHECK_BYTES_PER_ITEM * items_per_launch / launch_s / 1e9
+        traffic = (CHECK_DRAM_BYTES_PER_ITEM * items_per_launch if CHECK_DRAM_BYTES_PER_ITEM else None)
         # path-level algorithmic bytes (input + output mesh + one quality check of
         # every output triangle): 16 B/point, 24 B/triangle, 8 B/segment, 60 B/tri
         alg = (16 * cdt.numberofpoints + 24 * cdt.numberoftriangles + 8 * cdt.numberofsegments + 16 * np_out +
                24 * nt_out + 8 * ns_out + 60 * nt_out)
-        achieved = alg / (ms / 1e3) / 1e9
+        path_gbs = alg / (ms / 1e3) / 1e9
         line = {"metric": METRIC, "value": value, "unit": "triangles/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
@@ -250,8 +273,15 @@ def run_ours(args, rank, world, local_rank):
                 "host_syncs": int(s["host_syncs"]), "rounds": int(s["rounds"]),
                 "flip_steps": int(s["flip_steps"]),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                             "kernel": "whole refinement path (algorithmic bytes per output triangle)"},
+                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                             "kernel": "k_check_flip2 (flip-step check)",
+                             "bytes_per_item": CHECK_BYTES_PER_ITEM, "launches": launches,
+                             "items_per_launch": items_per_launch, "avg_launch_us": launch_s * 1e6,
+                             "share_of_step": probe["check_ms"] / ms,
+                             "first_launch_items": probe["first_items"],
+                             "timing": "per-launch device timer (%globaltimer, first block start to last block "
+                                       "end) in one extra probed step after the timed region",
+                             "path_achieved_gbs": path_gbs, "path_frac": path_gbs / peak},
                 "clocks": clk.summary(), "input_generation_s": gen_s}
         if args.cpu_baseline and world == 1:
             try:

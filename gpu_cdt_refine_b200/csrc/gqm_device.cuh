@@ -15,7 +15,8 @@
 //                         tagged with the launch epoch and the storing
 //                         thread's key (see s2t_store)
 //   s2seg int[Scap], enc int[Scap], segs int2[S_in]
-//   wbits uint32[Tcap/32], wcnt/wpre int[Tcap/1024]   flip winners of a step
+//   wbits uint32[Tcap/32], wcnt int[Tcap/1024], wsup int[Tcap/32768]
+//                         flip winners of a step (bitmap and counts)
 // Edge i of a triangle joins vertices i+1 and i+2 and faces vertex i; an
 // oriented triangle (t << 2 | i) names edge i of t (GPU_Refine/refine.cu:95-113).
 // Flags the reference keeps in one byte (GPU_Refine/refine.h:36-205) are split
@@ -44,10 +45,10 @@ struct Mesh {
   int *tpos;  // winner-slot of each triangle during a flip step
   int *fstamp, *tstamp;  // per-triangle generation stamps deduplicating the flip-step queues
   s2t_t *s2t;
-  // flip winners of the current step: one bit per triangle slot, winner counts
-  // per chunk of 1024 slots and their exclusive prefix (see win_rank)
+  // flip winners of the current step: one bit per triangle slot and winner
+  // counts per chunk of 1024 slots and per superchunk of 32768 (see win_rank)
   unsigned *wbits;
-  int *wcnt, *wpre;
+  int *wcnt, *wsup;
   int *s2seg, *enc;
   const int2 *segs;
   int *err;  // first error code raised on the device
@@ -103,13 +104,26 @@ __device__ __forceinline__ void s2t_store(const Mesh &M, int s, int v, uint32_t 
 // Position of flip winner `index` in the reference's winner list, which is
 // compacted in triangle order (kernelUpdatePhase1's pos, refine.cu:1312): the
 // number of this step's winners with a smaller slot.  The winners' own list
-// here is filled by atomics in any order, so the position comes from the
-// winner bitmap: the prefix of its 1024-slot chunk plus the bits before it.
+// here is filled by atomics in any order, so the position is counted from the
+// winner bitmap and its chunk counts.  Only stores into subseg2tri need it.
 __device__ __forceinline__ int win_rank(const Mesh &M, int index) {
-  const int w = index >> 5;
-  int r = M.wpre[index >> 10];
-  for (int i = w & ~31; i < w; ++i) r += __popc(M.wbits[i]);
+  const int w = index >> 5, c = index >> 10, sc = index >> 15;
+  int r = 0;
+  for (int i = 0; i < sc; ++i) r += M.wsup[i];
+  for (int i = sc << 5; i < c; ++i) r += M.wcnt[i];
+  for (int i = c << 5; i < w; ++i) r += __popc(M.wbits[i]);
   return r + __popc(M.wbits[w] & ((1u << (index & 31)) - 1u));
+}
+// enter / leave the winner bitmap and its counts
+__device__ __forceinline__ void win_mark(const Mesh &M, int index) {
+  atomicOr(M.wbits + (index >> 5), 1u << (index & 31));
+  atomicAdd(M.wcnt + (index >> 10), 1);
+  atomicAdd(M.wsup + (index >> 15), 1);
+}
+__device__ __forceinline__ void win_unmark(const Mesh &M, int index) {
+  atomicAnd(M.wbits + (index >> 5), ~(1u << (index & 31)));
+  atomicAdd(M.wcnt + (index >> 10), -1);
+  atomicAdd(M.wsup + (index >> 15), -1);
 }
 
 __device__ __forceinline__ void raise_err(const Mesh &M, int code) { atomicCAS(M.err, 0, code); }

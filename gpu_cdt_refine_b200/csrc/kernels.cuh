@@ -361,7 +361,19 @@ __device__ __forceinline__ void set_link(int *sl, int nOrg, int nDest, int nApex
 }
 
 // kernelUpdatePhase1, refine.cu:1295-1552
-__device__ void phase1_body(const Mesh &M, int pos, int index, int *sl, uint32_t epoch) {
+// The subseg2tri stores are not made here but collected in `ps` (their key
+// needs the winner's position in the reference's list, found afterwards).
+struct PendingS2T {
+  int n;
+  int s[6], v[6], slot[6];
+  __device__ __forceinline__ void add(int sg, int val, int sl) {
+    s[n] = sg;
+    v[n] = val;
+    slot[n] = sl;
+    n++;
+  }
+};
+__device__ void phase1_body(const Mesh &M, int pos, int index, int *sl, PendingS2T &ps) {
   {
     int ori = M.tfo[index];
     if (ori < 3) {
@@ -391,10 +403,10 @@ __device__ void phase1_body(const Mesh &M, int pos, int index, int *sl, uint32_t
       b.w = 0;
       M.tsg[index] = a;
       M.tsg[pOppTri] = b;
-      if (sOrg != -1) s2t_store(M, sOrg, (index << 2) | ori, epoch, wkey(win_rank(M, index), 0));
-      if (spDest != -1) s2t_store(M, spDest, (index << 2) | m3(ori + 1), epoch, wkey(win_rank(M, index), 1));
-      if (sApex != -1) s2t_store(M, sApex, (pOppTri << 2) | pOppOri, epoch, wkey(win_rank(M, index), 2));
-      if (spApex != -1) s2t_store(M, spApex, (pOppTri << 2) | m3(pOppOri + 2), epoch, wkey(win_rank(M, index), 3));
+      if (sOrg != -1) ps.add(sOrg, (index << 2) | ori, 0);
+      if (spDest != -1) ps.add(spDest, (index << 2) | m3(ori + 1), 1);
+      if (sApex != -1) ps.add(sApex, (pOppTri << 2) | pOppOri, 2);
+      if (spApex != -1) ps.add(spApex, (pOppTri << 2) | m3(pOppOri + 2), 3);
       M.tst[index] |= TS_CHECK;
       M.tst[pOppTri] |= TS_CHECK;
     } else if (ori < 6) {
@@ -421,9 +433,9 @@ __device__ void phase1_body(const Mesh &M, int pos, int index, int *sl, uint32_t
       setc(a, m3(ori + 2), sDest);
       a.w = 0;
       M.tsg[index] = a;
-      if (sOrg != -1) s2t_store(M, sOrg, (index << 2) | m3(ori + 1), epoch, wkey(win_rank(M, index), 4));
-      if (sApex != -1) s2t_store(M, sApex, (index << 2) | ori, epoch, wkey(win_rank(M, index), 5));
-      if (sDest != -1) s2t_store(M, sDest, (index << 2) | m3(ori + 2), epoch, wkey(win_rank(M, index), 6));
+      if (sOrg != -1) ps.add(sOrg, (index << 2) | m3(ori + 1), 4);
+      if (sApex != -1) ps.add(sApex, (index << 2) | ori, 5);
+      if (sDest != -1) ps.add(sDest, (index << 2) | m3(ori + 2), 6);
       M.tst[index] |= TS_CHECK;
       M.tst[t1] &= (uint8_t)~TS_NOTNULL;
       M.tst[t2] &= (uint8_t)~TS_NOTNULL;
@@ -492,12 +504,12 @@ __device__ void phase1_body(const Mesh &M, int pos, int index, int *sl, uint32_t
       b.w = 0;
       M.tsg[index] = a;
       M.tsg[t1] = b;
-      if (sOrg != -1) s2t_store(M, sOrg, (index << 2) | ori, epoch, wkey(win_rank(M, index), 7));
-      if (sDest != -1) s2t_store(M, sDest, (index << 2) | m3(ori + 1), epoch, wkey(win_rank(M, index), 8));
-      if (sApex != -1) s2t_store(M, sApex, (index << 2) | m3(ori + 2), epoch, wkey(win_rank(M, index), 9));
-      if (snOrg != -1) s2t_store(M, snOrg, (t1 << 2) | t1_ori, epoch, wkey(win_rank(M, index), 10));
-      if (snDest != -1) s2t_store(M, snDest, (t1 << 2) | m3(t1_ori + 1), epoch, wkey(win_rank(M, index), 11));
-      if (snApex != -1) s2t_store(M, snApex, (t1 << 2) | m3(t1_ori + 2), epoch, wkey(win_rank(M, index), 12));
+      if (sOrg != -1) ps.add(sOrg, (index << 2) | ori, 7);
+      if (sDest != -1) ps.add(sDest, (index << 2) | m3(ori + 1), 8);
+      if (sApex != -1) ps.add(sApex, (index << 2) | m3(ori + 2), 9);
+      if (snOrg != -1) ps.add(snOrg, (t1 << 2) | t1_ori, 10);
+      if (snDest != -1) ps.add(snDest, (t1 << 2) | m3(t1_ori + 1), 11);
+      if (snApex != -1) ps.add(snApex, (t1 << 2) | m3(t1_ori + 2), 12);
       M.tst[index] |= TS_CHECK;
       M.tst[t1] |= TS_CHECK;
       M.tst[pOppTri] &= (uint8_t)~TS_NOTNULL;
@@ -768,6 +780,7 @@ __global__ void k_mark_redundant(Mesh M, int *delmarker, const int *dellist, con
 struct KTimer {
   unsigned long long t0, t1;  // earliest block start / latest block end of the current launch
   unsigned long long total_ns, launches, items;
+  unsigned long long first_items[4];  // items of the first four launches since the reset
   unsigned blocks_done;
   int on;
 };
@@ -794,6 +807,7 @@ __device__ __forceinline__ void ktimer_end(KTimer *tm, unsigned long long start,
       __threadfence();
       volatile KTimer *v = tm;
       v->total_ns += v->t1 - v->t0;
+      if (v->launches < 4) v->first_items[v->launches] = (unsigned long long)items;
       v->launches += 1;
       v->items += (unsigned long long)items;
       v->t0 = ~0ull;
@@ -807,6 +821,7 @@ __global__ void k_ktimer_reset(KTimer *tm, int on) {
     tm->t0 = ~0ull;
     tm->t1 = 0;
     tm->total_ns = tm->launches = tm->items = 0;
+    for (int i = 0; i < 4; ++i) tm->first_items[i] = 0;
     tm->blocks_done = 0;
     tm->on = on;
   }
@@ -1130,52 +1145,66 @@ __global__ void k_flip_winner2(Mesh M, const int *act, const int *dn, const uint
     }
     if (w) {
       win[atomicAdd(winn, 1)] = index;
-      atomicOr(M.wbits + (index >> 5), 1u << (index & 31));
-      atomicAdd(M.wcnt + (index >> 10), 1);
+      win_mark(M, index);
     } else {
       M.tfo[index] = 15;
     }
   }
 }
 
-// Exclusive prefix of the per-chunk winner counts (one block), which clears
-// the counts for the next step.
-__global__ void k_win_prefix(Mesh M, int nchunks) {
-  __shared__ int part[1024];
-  __shared__ int carry;
-  const int nt = (int)blockDim.x, t = (int)threadIdx.x;  // nt <= 1024
-  if (t == 0) carry = 0;
-  __syncthreads();
-  for (int base = 0; base < nchunks; base += nt) {
-    const int i = base + t;
-    const int c = i < nchunks ? M.wcnt[i] : 0;
-    part[t] = c;
-    __syncthreads();
-    for (int off = 1; off < nt; off <<= 1) {
-      const int v = t >= off ? part[t - off] : 0;
-      __syncthreads();
-      part[t] += v;
-      __syncthreads();
-    }
-    if (i < nchunks) {
-      M.wpre[i] = carry + part[t] - c;
-      M.wcnt[i] = 0;
-    }
-    __syncthreads();
-    if (t == nt - 1) carry += part[nt - 1];
-    __syncthreads();
-  }
+// Position of winner `index` among this step's winners (win_rank), computed
+// by the 32 lanes of a warp together: lanes sum the superchunk counts, the
+// chunk counts of its superchunk and the bitmap words of its chunk.
+__device__ __forceinline__ int warp_win_rank(const Mesh &M, int index) {
+#ifdef GQM_HOST_EMU
+  return win_rank(M, index);
+#else
+  const int lane = (int)(threadIdx.x & 31u);
+  const int w = index >> 5, c = index >> 10, sc = index >> 15;
+  int r = 0;
+  for (int i = lane; i < sc; i += 32) r += M.wsup[i];
+  if ((sc << 5) + lane < c) r += M.wcnt[(sc << 5) + lane];
+  if ((c << 5) + lane < w) r += __popc(M.wbits[(c << 5) + lane]);
+  for (int o = 16; o; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+  return r + __popc(M.wbits[w] & ((1u << (index & 31)) - 1u));
+#endif
 }
 
 // kernelInitLinklist + kernelUpdatePhase1 in one launch: each winner's list
 // setup reads only triangles the winner owns, before its own phase-1 writes.
+// The loop keeps whole warps together (blockDim is a multiple of 32) so that
+// the lanes with subseg2tri stores can have their ranks found by the warp.
 __global__ void GQM_WALK_BOUNDS k_link_phase1(Mesh M, const int *win, const int *dn, int *ll, int *sl, const unsigned *ep) {
-  int n = *dn;
-  uint32_t epoch = *ep;
-  GS_LOOP(pos, n) {
-    int index = win[pos];
-    init_link_body(M, pos, index, ll);
-    phase1_body(M, pos, index, sl, epoch);
+  const int n = *dn;
+  const uint32_t epoch = *ep;
+  const int lane = (int)(threadIdx.x & 31u);
+  const int stride = (int)(gridDim.x * blockDim.x);
+  for (int base = (int)(blockIdx.x * blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
+    const int pos = base + lane;
+    const bool on = pos < n;
+    const int index = on ? win[pos] : -1;
+    PendingS2T ps;
+    ps.n = 0;
+    if (on) {
+      init_link_body(M, pos, index, ll);
+      phase1_body(M, pos, index, sl, ps);
+    }
+#ifdef GQM_HOST_EMU
+    if (ps.n) {
+      const int rank = warp_win_rank(M, index);
+      for (int i = 0; i < ps.n; ++i) s2t_store(M, ps.s[i], ps.v[i], epoch, wkey(rank, ps.slot[i]));
+    }
+#else
+    unsigned need = __ballot_sync(0xffffffffu, ps.n > 0);
+    while (need) {
+      const int l = __ffs(need) - 1;
+      need &= need - 1;
+      const int idx = __shfl_sync(0xffffffffu, index, l);
+      const int rank = warp_win_rank(M, idx);
+      if (lane == l)
+        for (int i = 0; i < ps.n; ++i) s2t_store(M, ps.s[i], ps.v[i], epoch, wkey(rank, ps.slot[i]));
+    }
+#endif
   }
 }
 
@@ -1191,7 +1220,7 @@ __global__ void k_phase3q(Mesh M, const int *win, const int *dn, const int *sl, 
   GS_LOOP(pos, n) {
     const int index = win[pos];
     phase3_body(M, pos, index, sl, f);
-    atomicAnd(M.wbits + (index >> 5), ~(1u << (index & 31)));  // phase 1 has read the bitmap
+    win_unmark(M, index);  // phase 1 has read the bitmap
   }
 }
 

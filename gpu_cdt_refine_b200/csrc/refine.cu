@@ -273,7 +273,7 @@ struct Refiner {
     void *ptrs[] = {M.pts, M.ps, M.pred, M.tv, M.tn, M.tsg, M.tst, M.tflip, M.tfo, M.flip0, M.tmark, M.tpos,
                     M.s2t, M.s2seg, M.enc, M.err, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
                     newidx, tail, center, emptyp, pnew, enclist, encl2, smark, mids, snap, segs, dcount, bc,
-                    dctr, dgc, dinput, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wpre};
+                    dctr, dgc, dinput, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wsup};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     if (hcount) cudaFreeHost(hcount);
@@ -416,11 +416,12 @@ struct Refiner {
         regrow(&sl, 6 * old, 6 * n) || regrow(&newidx, 0, n) || regrow(&tail, 0, std::max<long>(n, pphys)) ||
         regrow(&center, old, n) || regrow(&M.fstamp, old, n) || regrow(&M.tstamp, old, n) || regrow(&fq, 0, n) ||
         regrow(&tl, 0, n) || regrow(&clr, 0, n) || regrow(&M.wbits, 0, n / 32 + 1) ||
-        regrow(&M.wcnt, 0, n / 1024 + 1) || regrow(&M.wpre, 0, n / 1024 + 1))
+        regrow(&M.wcnt, 0, n / 1024 + 1) || regrow(&M.wsup, 0, n / 32768 + 1))
       return GQM_ERR_MEMORY;
     // winner bitmap and chunk counts are all zero between flip steps
     cudaMemsetAsync(M.wbits, 0, sizeof(unsigned) * (n / 32 + 1), st);
     cudaMemsetAsync(M.wcnt, 0, sizeof(int) * (n / 1024 + 1), st);
+    cudaMemsetAsync(M.wsup, 0, sizeof(int) * (n / 32768 + 1), st);
     if (n > old) {
       cudaMemsetAsync(M.tst + old, 0, n - old, st);
       cudaMemsetAsync(M.tflip + old, 0, n - old, st);
@@ -527,7 +528,6 @@ struct Refiner {
     else
       KL(k_check_flip2<0>, kStepGrid, 256)(M, act, &fc->nact, clr, T, ktm);
     KL(k_flip_winner2, kStepGrid, 256)(M, act, &fc->nact, clr, Q, win, &fc->winn);
-    KL(k_win_prefix, 1, 1024)(M, (int)(tphys / 1024 + 1));
     KL(k_link_phase1, kStepGrid, 256)(M, win, &fc->winn, ll, sl, &fc->epoch);
     KL(k_phase2, kStepGrid, 256)(M, win, &fc->winn, ll, sl);
     KL(k_phase3q, kStepGrid, 256)(M, win, &fc->winn, sl, Q);
@@ -858,6 +858,7 @@ struct Refiner {
     if (M.wbits) {  // left set only by a run that stopped inside a flip step
       cudaMemsetAsync(M.wbits, 0, sizeof(unsigned) * (tphys / 32 + 1), st);
       cudaMemsetAsync(M.wcnt, 0, sizeof(int) * (tphys / 1024 + 1), st);
+      cudaMemsetAsync(M.wsup, 0, sizeof(int) * (tphys / 32768 + 1), st);
     }
     cudaMemsetAsync(M.err, 0, sizeof(int), st);
     cudaMemsetAsync(dctr, 0, sizeof(unsigned long long) * 4, st);
@@ -1066,6 +1067,7 @@ int gqm_context_probe_read(gqm_context *ctx, gqm_probe *p) {
   p->check_launches = (long long)h.launches;
   p->check_items = (long long)h.items;
   p->check_ms = (double)h.total_ns * 1e-6;
+  for (int i = 0; i < 4; ++i) p->first_items[i] = (long long)h.first_items[i];
   p->loop_launches = r.probe_loops;
   p->loop_ms = r.probe_loop_ms;
   return GQM_OK;

@@ -52,6 +52,17 @@ class Stats(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Probe(ctypes.Structure):
+    _fields_ = [("check_launches", ctypes.c_longlong), ("check_items", ctypes.c_longlong),
+                ("check_ms", ctypes.c_double), ("loop_launches", ctypes.c_longlong), ("loop_ms", ctypes.c_double),
+                ("first_items", ctypes.c_longlong * 4)]
+
+    def as_dict(self):
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != "first_items"}
+        d["first_items"] = list(self.first_items)
+        return d
+
+
 class RefineError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"{msg} (status {status})")
@@ -96,6 +107,10 @@ def lib() -> ctypes.CDLL:
         L.gqm_context_flip_profile.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                                ctypes.POINTER(ctypes.c_longlong)]
         L.gqm_context_flip_profile.restype = ctypes.c_int
+        L.gqm_context_probe.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.gqm_context_probe.restype = ctypes.c_int
+        L.gqm_context_probe_read.argtypes = [ctypes.c_void_p, ctypes.POINTER(Probe)]
+        L.gqm_context_probe_read.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -253,6 +268,20 @@ class Context:
         if rc != 0:
             raise RefineError(rc, "flip profile")
         return list(st), list(it)
+
+    def probe(self, enable=True):
+        """Reset and enable (or disable) the launch timer of the flip-step check
+        kernel and the events around the flip-loop launches."""
+        rc = self._lib.gqm_context_probe(self._h, 1 if enable else 0)
+        if rc != 0:
+            raise RefineError(rc, "probe")
+
+    def probe_read(self) -> dict:
+        p = Probe()
+        rc = self._lib.gqm_context_probe_read(self._h, ctypes.byref(p))
+        if rc != 0:
+            raise RefineError(rc, "probe read")
+        return p.as_dict()
 
     def result(self, with_status=False):
         out = CdtOut()

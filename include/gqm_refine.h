@@ -125,6 +125,7 @@ typedef struct {
   double check_ms;          /* their summed execution time */
   long long loop_launches;  /* flip-loop graph launches */
   double loop_ms;           /* their summed time (CUDA events) */
+  long long first_items[4]; /* active triangles of the first four check launches */
 } gqm_probe;
 int gqm_context_probe(gqm_context *ctx, int enable);
 int gqm_context_probe_read(gqm_context *ctx, gqm_probe *p);
