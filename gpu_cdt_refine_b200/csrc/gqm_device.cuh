@@ -15,8 +15,8 @@
 //                         tagged with the launch epoch and the storing
 //                         thread's key (see s2t_store)
 //   s2seg int[Scap], enc int[Scap], segs int2[S_in]
-//   wbits uint32[Tcap/32], wcnt int[Tcap/1024], wsup int[Tcap/32768]
-//                         flip winners of a step (bitmap and counts)
+//   wbits uint32[Tcap/2^5], wcnt int[Tcap/2^10], wsup int[Tcap/2^15],
+//   wmeg int[Tcap/2^20]   flip winners of a step (bitmap and counts)
 // Edge i of a triangle joins vertices i+1 and i+2 and faces vertex i; an
 // oriented triangle (t << 2 | i) names edge i of t (GPU_Refine/refine.cu:95-113).
 // Flags the reference keeps in one byte (GPU_Refine/refine.h:36-205) are split
@@ -46,9 +46,9 @@ struct Mesh {
   int *fstamp, *tstamp;  // per-triangle generation stamps deduplicating the flip-step queues
   s2t_t *s2t;
   // flip winners of the current step: one bit per triangle slot and winner
-  // counts per chunk of 1024 slots and per superchunk of 32768 (see win_rank)
+  // counts per 2^10, 2^15 and 2^20 slots (see win_rank)
   unsigned *wbits;
-  int *wcnt, *wsup;
+  int *wcnt, *wsup, *wmeg;
   int *s2seg, *enc;
   const int2 *segs;
   int *err;  // first error code raised on the device
@@ -105,25 +105,39 @@ __device__ __forceinline__ void s2t_store(const Mesh &M, int s, int v, uint32_t 
 // compacted in triangle order (kernelUpdatePhase1's pos, refine.cu:1312): the
 // number of this step's winners with a smaller slot.  The winners' own list
 // here is filled by atomics in any order, so the position is counted from the
-// winner bitmap and its chunk counts.  Only stores into subseg2tri need it.
-__device__ __forceinline__ int win_rank(const Mesh &M, int index) {
-  const int w = index >> 5, c = index >> 10, sc = index >> 15;
+// winner bitmap and its counts per 2^10, 2^15 and 2^20 slots: at most 31
+// entries of each level (one 128-byte line each) plus the 2^20 counts before
+// the slot, all independent loads.  Only stores into subseg2tri need it.
+__device__ __forceinline__ int sum32(const int *a, int lo, int hi) {  // a[lo..hi), hi - lo < 32
   int r = 0;
-  for (int i = 0; i < sc; ++i) r += M.wsup[i];
-  for (int i = sc << 5; i < c; ++i) r += M.wcnt[i];
-  for (int i = c << 5; i < w; ++i) r += __popc(M.wbits[i]);
-  return r + __popc(M.wbits[w] & ((1u << (index & 31)) - 1u));
+#pragma unroll
+  for (int j = 0; j < 31; ++j)
+    if (lo + j < hi) r += a[lo + j];
+  return r;
+}
+__device__ __forceinline__ int win_rank(const Mesh &M, int index) {
+  const int w = index >> 5, c = index >> 10, sc = index >> 15, mg = index >> 20;
+  int r = 0;
+  for (int i = 0; i < mg; ++i) r += M.wmeg[i];
+  r += sum32(M.wsup, mg << 5, sc) + sum32(M.wcnt, sc << 5, c);
+  int b = 0;
+#pragma unroll
+  for (int j = 0; j < 31; ++j)
+    if ((c << 5) + j < w) b += __popc(M.wbits[(c << 5) + j]);
+  return r + b + __popc(M.wbits[w] & ((1u << (index & 31)) - 1u));
 }
 // enter / leave the winner bitmap and its counts
 __device__ __forceinline__ void win_mark(const Mesh &M, int index) {
   atomicOr(M.wbits + (index >> 5), 1u << (index & 31));
   atomicAdd(M.wcnt + (index >> 10), 1);
   atomicAdd(M.wsup + (index >> 15), 1);
+  atomicAdd(M.wmeg + (index >> 20), 1);
 }
 __device__ __forceinline__ void win_unmark(const Mesh &M, int index) {
   atomicAnd(M.wbits + (index >> 5), ~(1u << (index & 31)));
   atomicAdd(M.wcnt + (index >> 10), -1);
   atomicAdd(M.wsup + (index >> 15), -1);
+  atomicAdd(M.wmeg + (index >> 20), -1);
 }
 
 __device__ __forceinline__ void raise_err(const Mesh &M, int code) { atomicCAS(M.err, 0, code); }

@@ -12,11 +12,30 @@
 #ifndef GQM_WALK_MIN_BLOCKS
 #define GQM_WALK_MIN_BLOCKS 3
 #endif
+
+// Two compilations of the same kernels:
+//  * grid mode (default): every step below is a __global__ kernel whose
+//    grid-stride loop covers its items across the whole grid;
+//  * CTA mode (GQM_CTA_MODE, batch.cu): every step is a __device__ function
+//    that one thread block runs over one domain's items, the block's threads
+//    striding over them; the caller separates steps with __syncthreads().
+#ifdef GQM_CTA_MODE
+#define GQM_KERNEL __device__
+#define GQM_WALK_BOUNDS
+#define GQM_GTID ((int)threadIdx.x)
+#define GQM_GSIZE ((int)blockDim.x)
+#define GQM_BLOCK0 true
+#else
+#define GQM_KERNEL __global__
 #define GQM_WALK_BOUNDS __launch_bounds__(256, GQM_WALK_MIN_BLOCKS)
+#define GQM_GTID ((int)(blockIdx.x * blockDim.x + threadIdx.x))
+#define GQM_GSIZE ((int)(gridDim.x * blockDim.x))
+#define GQM_BLOCK0 (blockIdx.x == 0)
+#endif
 
 namespace gqm {
 
-#define GS_LOOP(i, n) for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
+#define GS_LOOP(i, n) for (int i = GQM_GTID; i < (n); i += GQM_GSIZE)
 
 // ============================================================================
 // Initialisation (refine.cu:5557-5747, 3105-3151)
@@ -50,7 +69,7 @@ __device__ __forceinline__ int incident_ori(const int *tri, int t, int n) {
 // [0, np), neighbours in [-1, nt), segment endpoints in [0, np) and distinct,
 // coordinates finite.  The reference trusts its input; a bad index here would
 // make the initialisation read outside the input arrays.
-__global__ void k_check_input(const double2 *pts, int np, const int *tri, const int *nbr, int nt,
+GQM_KERNEL void k_check_input(const double2 *pts, int np, const int *tri, const int *nbr, int nt,
                               const int *seg, int ns, int *err) {
   int bad = 0;
   GS_LOOP(i, np) {
@@ -71,7 +90,7 @@ __global__ void k_check_input(const double2 *pts, int np, const int *tri, const 
   if (bad) atomicCAS(err, 0, GQM_ERR_ARGUMENT);
 }
 
-__global__ void k_init_tris(Mesh M, const int *tri, const int *nbr, int nt, int tcap) {
+GQM_KERNEL void k_init_tris(Mesh M, const int *tri, const int *nbr, int nt, int tcap) {
   GS_LOOP(t, tcap) {
     if (t < nt) {
       M.tv[t] = make_int4(tri[3 * t], tri[3 * t + 1], tri[3 * t + 2], 0);
@@ -95,7 +114,7 @@ __global__ void k_init_tris(Mesh M, const int *tri, const int *nbr, int nt, int 
   }
 }
 
-__global__ void k_init_points(Mesh M, const double2 *pts, int np, int pcap) {
+GQM_KERNEL void k_init_points(Mesh M, const double2 *pts, int np, int pcap) {
   GS_LOOP(i, pcap) {
     if (i < np) {
       M.pts[i] = pts[i];
@@ -111,8 +130,8 @@ __global__ void k_init_points(Mesh M, const double2 *pts, int np, int pcap) {
 // cos^2(theta) exactly as the reference evaluates it on the device
 // (refine.cu:418, 123-124).
 #define GQM_PI 3.141592653589793238462643383279502884197169399375105820974944592308
-__global__ void k_goodcos(double theta, double *out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
+GQM_KERNEL void k_goodcos(double theta, double *out) {
+  if (threadIdx.x == 0 && GQM_BLOCK0) {
     double c = cos(theta * GQM_PI / 180.0);
     out[0] = c * c;
     out[1] = cos(theta * GQM_PI / 180.0) * cos(theta * GQM_PI / 180.0);
@@ -126,7 +145,7 @@ __device__ __forceinline__ unsigned long long seg_key(int a, int b) {
 __device__ __forceinline__ unsigned seg_hash(unsigned long long k, unsigned mask) {
   return (unsigned)((k * 0x9E3779B97F4A7C15ull) >> 24) & mask;
 }
-__global__ void k_seg_hash_insert(const int2 *segs, int ns, unsigned long long *keys, int *vals, unsigned mask) {
+GQM_KERNEL void k_seg_hash_insert(const int2 *segs, int ns, unsigned long long *keys, int *vals, unsigned mask) {
   GS_LOOP(s, ns) {
     unsigned long long k = seg_key(segs[s].x, segs[s].y);
     unsigned h = seg_hash(k, mask);
@@ -143,7 +162,7 @@ __global__ void k_seg_hash_insert(const int2 *segs, int ns, unsigned long long *
 // initSubsegs (refine.cu:5618-5747) for every triangle: edge (p0,p1) is
 // orientation 2, (p1,p2) 0, (p2,p0) 1; subseg2tri keeps the largest otri
 // (atomicMax), tri2subseg the largest matching subsegment.
-__global__ void k_init_subsegs(Mesh M, int nt, const unsigned long long *keys, const int *vals, unsigned mask,
+GQM_KERNEL void k_init_subsegs(Mesh M, int nt, const unsigned long long *keys, const int *vals, unsigned mask,
                                int *s2t_int) {
   GS_LOOP(t, nt) {
     int4 v = M.tv[t];
@@ -166,7 +185,7 @@ __global__ void k_init_subsegs(Mesh M, int nt, const unsigned long long *keys, c
     M.tsg[t] = sg;
   }
 }
-__global__ void k_pack_s2t(Mesh M, const int *s2t_int, int ns) {
+GQM_KERNEL void k_pack_s2t(Mesh M, const int *s2t_int, int ns) {
   GS_LOOP(s, ns) {
     M.s2t[s] = s2t_plain(s2t_int[s]);
     M.s2seg[s] = s;
@@ -174,7 +193,7 @@ __global__ void k_pack_s2t(Mesh M, const int *s2t_int, int ns) {
 }
 
 // kernelMarkAllEncsegs, refine.cu:3105-3151
-__global__ void k_mark_all_encsegs(Mesh M, int ns) {
+GQM_KERNEL void k_mark_all_encsegs(Mesh M, int ns) {
   GS_LOOP(s, ns) {
     int e = -1;
     int otri = s2t_get(M, s);
@@ -223,7 +242,7 @@ __device__ __forceinline__ double smallest_cos2(double2 pA, double2 pO, double2 
 
 // kernelMarkBadTriangles, refine.cu:376-497, over every triangle slot below
 // ntri that is not null and has CHECK set.
-__global__ void k_mark_bad(Mesh M, int ntri) {
+GQM_KERNEL void k_mark_bad(Mesh M, int ntri) {
   GS_LOOP(t, ntri) {
     uint8_t st = M.tst[t];
     if (!(st & TS_NOTNULL) || !(st & TS_CHECK)) continue;
@@ -530,7 +549,7 @@ __device__ __forceinline__ void p2_link(const Mesh &M, const int *ll, int *sl, i
 }
 
 // kernelUpdatePhase2, refine.cu:1598-1871
-__global__ void k_phase2(Mesh M, const int *win, const int *dn, const int *ll, int *sl) {
+GQM_KERNEL void k_phase2(Mesh M, const int *win, const int *dn, const int *ll, int *sl) {
   int n = *dn;
   int nlist = 4 * n;
   GS_LOOP(pos, n) {
@@ -725,7 +744,7 @@ __device__ void phase3_body(const Mesh &M, int pos, int index, const int *sl, co
 
 
 // kernelMarkReduantPoints, refine.cu:604-677
-__global__ void k_mark_redundant(Mesh M, int *delmarker, const int *dellist, const int *dn) {
+GQM_KERNEL void k_mark_redundant(Mesh M, int *delmarker, const int *dellist, const int *dn) {
   int n = *dn;
   GS_LOOP(pos, n) {
     int out = -1;
@@ -816,8 +835,8 @@ __device__ __forceinline__ void ktimer_end(KTimer *tm, unsigned long long start,
     }
   }
 }
-__global__ void k_ktimer_reset(KTimer *tm, int on) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+GQM_KERNEL void k_ktimer_reset(KTimer *tm, int on) {
+  if (GQM_BLOCK0 && threadIdx.x == 0) {
     tm->t0 = ~0ull;
     tm->t1 = 0;
     tm->total_ns = tm->launches = tm->items = 0;
@@ -897,8 +916,8 @@ __device__ __forceinline__ int flip_next(FlipCtl *c) {
 #ifdef GQM_HOST_EMU
 typedef int cudaGraphConditionalHandle;
 #endif
-__global__ void k_flip_prep(FlipCtl *c, cudaGraphConditionalHandle h, int use_graph) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+GQM_KERNEL void k_flip_prep(FlipCtl *c, cudaGraphConditionalHandle h, int use_graph) {
+  if (GQM_BLOCK0 && threadIdx.x == 0) {
     c->entry_steps = c->steps;
     int cond = flip_next(c);
 #ifndef GQM_HOST_EMU
@@ -909,8 +928,8 @@ __global__ void k_flip_prep(FlipCtl *c, cudaGraphConditionalHandle h, int use_gr
     (void)h;
   }
 }
-__global__ void k_flip_cond(FlipCtl *c, cudaGraphConditionalHandle h, int use_graph) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+GQM_KERNEL void k_flip_cond(FlipCtl *c, cudaGraphConditionalHandle h, int use_graph) {
+  if (GQM_BLOCK0 && threadIdx.x == 0) {
     int cond = flip_next(c);
 #ifndef GQM_HOST_EMU
     if (use_graph) cudaGraphSetConditional(h, cond);
@@ -920,17 +939,17 @@ __global__ void k_flip_cond(FlipCtl *c, cudaGraphConditionalHandle h, int use_gr
     (void)h;
   }
 }
-__global__ void k_bump_epoch(FlipCtl *c) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) c->epoch++;
+GQM_KERNEL void k_bump_epoch(FlipCtl *c) {
+  if (GQM_BLOCK0 && threadIdx.x == 0) c->epoch++;
 }
 // per-run reset of the control block; gen and epoch keep growing across runs
 // so that stamps and subseg2tri tags left by earlier runs never collide
-__global__ void k_ctl_reset(FlipCtl *c, long long cap, int *errp) {
-  if (blockIdx.x == 0 && threadIdx.x < kFlipProfileBins) {
+GQM_KERNEL void k_ctl_reset(FlipCtl *c, long long cap, int *errp) {
+  if (GQM_BLOCK0 && threadIdx.x < kFlipProfileBins) {
     c->prof_steps[threadIdx.x] = 0;
     c->prof_items[threadIdx.x] = 0;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (GQM_BLOCK0 && threadIdx.x == 0) {
     c->steps = 0;
     c->entry_steps = 0;
     c->cap_hit = 0;
@@ -942,14 +961,14 @@ __global__ void k_ctl_reset(FlipCtl *c, long long cap, int *errp) {
 
 
 // reset tmark / tfo before the first step of a flip-flop
-__global__ void k_flip_entry_reset(Mesh M, int ntri) {
+GQM_KERNEL void k_flip_entry_reset(Mesh M, int ntri) {
   GS_LOOP(t, ntri) {
     M.tmark[t] = kMaxInt;
     M.tfo[t] = 15;
   }
 }
 // A = queue entries whose flag is still set on a live triangle
-__global__ void k_flip_filter(Mesh M, const int *q, const int *qn, int *act, int *actn) {
+GQM_KERNEL void k_flip_filter(Mesh M, const int *q, const int *qn, int *act, int *actn) {
   int n = *qn;
   GS_LOOP(k, n) {
     int t = q[k];
@@ -958,17 +977,17 @@ __global__ void k_flip_filter(Mesh M, const int *q, const int *qn, int *act, int
 }
 // tmark of the triangles claimed in this step back to "unclaimed"; also
 // empties A for the filter that follows (A is not read after the winners).
-__global__ void k_flip_reset_touched(Mesh M, const int *tl, const int *tn, int *nact) {
+GQM_KERNEL void k_flip_reset_touched(Mesh M, const int *tl, const int *tn, int *nact) {
   int n = *tn;
   GS_LOOP(k, n) M.tmark[tl[k]] = kMaxInt;
-  if (blockIdx.x == 0 && threadIdx.x == 0) *nact = 0;
+  if (GQM_BLOCK0 && threadIdx.x == 0) *nact = 0;
 }
 
 // kernelCheckFlipping (refine.cu:778-1070) on A.  No flag is cleared here
 // (the decision is kept in clr[k] and applied by k_flip_winner2), so the
 // neighbour flags read below are the ones the step started with.
 template <int PRED>
-__global__ void GQM_WALK_BOUNDS k_check_flip2(Mesh M, const int *act, const int *dn, uint8_t *clr, TouchL T,
+GQM_KERNEL void GQM_WALK_BOUNDS k_check_flip2(Mesh M, const int *act, const int *dn, uint8_t *clr, TouchL T,
                                               KTimer *tm) {
   const int timed = tm->on;
   const unsigned long long start = timed ? global_ns() : 0;
@@ -1104,7 +1123,7 @@ __global__ void GQM_WALK_BOUNDS k_check_flip2(Mesh M, const int *act, const int 
 
 // kernelMarkFlipWinner (refine.cu:1072-1170) on A; applies the deferred flag
 // clears, re-queues the triangles that keep their flag, collects winners.
-__global__ void k_flip_winner2(Mesh M, const int *act, const int *dn, const uint8_t *clr, FlipQ Q, int *win,
+GQM_KERNEL void k_flip_winner2(Mesh M, const int *act, const int *dn, const uint8_t *clr, FlipQ Q, int *win,
                                int *winn) {
   int n = *dn;
   GS_LOOP(k, n) {
@@ -1152,59 +1171,22 @@ __global__ void k_flip_winner2(Mesh M, const int *act, const int *dn, const uint
   }
 }
 
-// Position of winner `index` among this step's winners (win_rank), computed
-// by the 32 lanes of a warp together: lanes sum the superchunk counts, the
-// chunk counts of its superchunk and the bitmap words of its chunk.
-__device__ __forceinline__ int warp_win_rank(const Mesh &M, int index) {
-#ifdef GQM_HOST_EMU
-  return win_rank(M, index);
-#else
-  const int lane = (int)(threadIdx.x & 31u);
-  const int w = index >> 5, c = index >> 10, sc = index >> 15;
-  int r = 0;
-  for (int i = lane; i < sc; i += 32) r += M.wsup[i];
-  if ((sc << 5) + lane < c) r += M.wcnt[(sc << 5) + lane];
-  if ((c << 5) + lane < w) r += __popc(M.wbits[(c << 5) + lane]);
-  for (int o = 16; o; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-  return r + __popc(M.wbits[w] & ((1u << (index & 31)) - 1u));
-#endif
-}
-
 // kernelInitLinklist + kernelUpdatePhase1 in one launch: each winner's list
 // setup reads only triangles the winner owns, before its own phase-1 writes.
-// The loop keeps whole warps together (blockDim is a multiple of 32) so that
-// the lanes with subseg2tri stores can have their ranks found by the warp.
-__global__ void GQM_WALK_BOUNDS k_link_phase1(Mesh M, const int *win, const int *dn, int *ll, int *sl, const unsigned *ep) {
+// The subseg2tri stores of phase 1 are made last, keyed by the winner's rank.
+GQM_KERNEL void GQM_WALK_BOUNDS k_link_phase1(Mesh M, const int *win, const int *dn, int *ll, int *sl, const unsigned *ep) {
   const int n = *dn;
   const uint32_t epoch = *ep;
-  const int lane = (int)(threadIdx.x & 31u);
-  const int stride = (int)(gridDim.x * blockDim.x);
-  for (int base = (int)(blockIdx.x * blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
-    const int pos = base + lane;
-    const bool on = pos < n;
-    const int index = on ? win[pos] : -1;
+  GS_LOOP(pos, n) {
+    const int index = win[pos];
     PendingS2T ps;
     ps.n = 0;
-    if (on) {
-      init_link_body(M, pos, index, ll);
-      phase1_body(M, pos, index, sl, ps);
-    }
-#ifdef GQM_HOST_EMU
+    init_link_body(M, pos, index, ll);
+    phase1_body(M, pos, index, sl, ps);
     if (ps.n) {
-      const int rank = warp_win_rank(M, index);
+      const int rank = win_rank(M, index);
       for (int i = 0; i < ps.n; ++i) s2t_store(M, ps.s[i], ps.v[i], epoch, wkey(rank, ps.slot[i]));
     }
-#else
-    unsigned need = __ballot_sync(0xffffffffu, ps.n > 0);
-    while (need) {
-      const int l = __ffs(need) - 1;
-      need &= need - 1;
-      const int idx = __shfl_sync(0xffffffffu, index, l);
-      const int rank = warp_win_rank(M, idx);
-      if (lane == l)
-        for (int i = 0; i < ps.n; ++i) s2t_store(M, ps.s[i], ps.v[i], epoch, wkey(rank, ps.slot[i]));
-    }
-#endif
   }
 }
 
@@ -1214,7 +1196,7 @@ struct QueueFlag {
   const FlipQ *Q;
   __device__ void operator()(int t) const { push_flag(*M, *Q, t); }
 };
-__global__ void k_phase3q(Mesh M, const int *win, const int *dn, const int *sl, FlipQ Q) {
+GQM_KERNEL void k_phase3q(Mesh M, const int *win, const int *dn, const int *sl, FlipQ Q) {
   int n = *dn;
   QueueFlag f{&M, &Q};
   GS_LOOP(pos, n) {
@@ -1238,7 +1220,7 @@ __device__ void mark_fan_q(const Mesh &M, const FlipQ &Q, int triIndex, int triO
     }
   } while (cur > -1 && cur != triIndex);
 }
-__global__ void k_mark_red_steiner_q(Mesh M, const int *tl, const int *dn, FlipQ Q) {
+GQM_KERNEL void k_mark_red_steiner_q(Mesh M, const int *tl, const int *dn, FlipQ Q) {
   int n = *dn;
   GS_LOOP(k, n) {
     int index = tl[k];
@@ -1264,7 +1246,7 @@ __device__ __forceinline__ void reset_tri_and_nbrs(const Mesh &M, int t, bool ma
   if (nb.z != -1) M.tfo[dtri(nb.z)] = 15;
 }
 // kernelResetMidInsertionMarker, refine.cu:2492-2542
-__global__ void k_reset_mid(Mesh M, const int *mids, const int *dn, const int *imark) {
+GQM_KERNEL void k_reset_mid(Mesh M, const int *mids, const int *dn, const int *imark) {
   int n = *dn;
   GS_LOOP(pos, n) {
     int sindex = imark[mids[pos]];
@@ -1276,7 +1258,7 @@ __global__ void k_reset_mid(Mesh M, const int *mids, const int *dn, const int *i
   }
 }
 // kernelMarkMidInsertion, refine.cu:2544-2579
-__global__ void k_mark_mid(Mesh M, const int *mids, const int *dn, const int *imark) {
+GQM_KERNEL void k_mark_mid(Mesh M, const int *mids, const int *dn, const int *imark) {
   int n = *dn;
   GS_LOOP(pos, n) {
     int sindex = imark[mids[pos]];
@@ -1290,13 +1272,13 @@ __global__ void k_mark_mid(Mesh M, const int *mids, const int *dn, const int *im
 // Snapshot of subseg2tri for every candidate before any winner writes
 // (the reference reads it at refine.cu:2636 in the same kernel that rewrites
 // it at 2844-2850).
-__global__ void k_mid_snapshot(Mesh M, const int *mids, const int *dn, const int *imark, int *snap) {
+GQM_KERNEL void k_mid_snapshot(Mesh M, const int *mids, const int *dn, const int *imark, int *snap) {
   int n = *dn;
   GS_LOOP(pos, n) snap[pos] = s2t_get(M, imark[mids[pos]]);
 }
 
 // kernelInsertMidPoints, refine.cu:2594-2927 (debug printing left out)
-__global__ void GQM_WALK_BOUNDS k_insert_mid(Mesh M, const int *mids, const int *dn, int *imark, const int *snap, const int *pslots,
+GQM_KERNEL void GQM_WALK_BOUNDS k_insert_mid(Mesh M, const int *mids, const int *dn, int *imark, const int *snap, const int *pslots,
                              const int *tslots, int nsub, const unsigned *ep, unsigned long long *counter) {
   int n = *dn;
   uint32_t epoch = *ep;
@@ -1455,7 +1437,7 @@ __device__ void relink_outer(const Mesh &M, const int *tri, int iteration) {
 }
 
 // kernelUpdateMidNeighbors, refine.cu:2929-3070
-__global__ void k_update_mid_nbrs(Mesh M, const int *mids, const int *dn, const int *imark, const int *enclist) {
+GQM_KERNEL void k_update_mid_nbrs(Mesh M, const int *mids, const int *dn, const int *imark, const int *enclist) {
   int n = *dn;
   GS_LOOP(pos, n) {
     int tindex = mids[pos];
@@ -1473,7 +1455,7 @@ __global__ void k_update_mid_nbrs(Mesh M, const int *mids, const int *dn, const 
 }
 
 // kernelUpdatePStatus2Old, refine.cu:3072-3083
-__global__ void k_points_old(Mesh M, int npts) {
+GQM_KERNEL void k_points_old(Mesh M, int npts) {
   GS_LOOP(i, npts) {
     uint8_t s = M.ps[i];
     if (!(s & PS_DELETED)) M.ps[i] = (uint8_t)(s & ~PS_NEW);
@@ -1523,7 +1505,7 @@ __device__ __forceinline__ double2 circumcenter(double2 vApex, double2 vOrg, dou
   return make_double2(vOrg.x + dx, vOrg.y + dy);
 }
 
-__global__ void k_circumcenter(Mesh M, const int *bad, const int *dn, double offc, int offcenter, double2 *center) {
+GQM_KERNEL void k_circumcenter(Mesh M, const int *bad, const int *dn, double offc, int offcenter, double2 *center) {
   int n = *dn;
   GS_LOOP(k, n) {
     int4 v = M.tv[bad[k]];
@@ -1533,7 +1515,7 @@ __global__ void k_circumcenter(Mesh M, const int *bad, const int *dn, double off
 
 // kernelLocateSinkPoints, refine.cu:3908-4184
 template <int PRED>
-__global__ void k_locate(Mesh M, const int *bad, const int *dn, const double2 *center, int *sinks) {
+GQM_KERNEL void k_locate(Mesh M, const int *bad, const int *dn, const double2 *center, int *sinks) {
   int n = *dn;
   GS_LOOP(k, n) {
     int index = bad[k];
@@ -1624,7 +1606,7 @@ __global__ void k_locate(Mesh M, const int *bad, const int *dn, const double2 *c
 }
 
 // kernelRemoveLosers, refine.cu:4186-4235
-__global__ void k_remove_losers(Mesh M, const int *bad, const int *dn, const int *sinks, int *imark) {
+GQM_KERNEL void k_remove_losers(Mesh M, const int *bad, const int *dn, const int *sinks, int *imark) {
   int n = *dn;
   GS_LOOP(k, n) {
     if (imark[k] < 0) continue;
@@ -1717,7 +1699,7 @@ __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, i
 // an oversized cavity makes its candidate an unconditional winner (negated
 // index).  cavn[k] = stored cavity size (0 for an oversized one).
 template <int PRED>
-__global__ void GQM_WALK_BOUNDS k_cavity_mark(Mesh M, const int *dn, const int *sinks, const double2 *center, const int *imark,
+GQM_KERNEL void GQM_WALK_BOUNDS k_cavity_mark(Mesh M, const int *dn, const int *sinks, const double2 *center, const int *imark,
                               int *ilist, int *cav, int *cavn, int stride) {
   int n = *dn;
   GS_LOOP(k, n) {
@@ -1730,7 +1712,7 @@ __global__ void GQM_WALK_BOUNDS k_cavity_mark(Mesh M, const int *dn, const int *
 }
 // kernelCheckCavities: a candidate loses if any triangle of its cavity was
 // claimed by a smaller bad index.
-__global__ void k_cavity_check(Mesh M, const int *dn, const int *cav, const int *cavn, int stride, int *imark,
+GQM_KERNEL void k_cavity_check(Mesh M, const int *dn, const int *cav, const int *cavn, int stride, int *imark,
                                const int *ilist) {
   int n = *dn;
   GS_LOOP(k, n) {
@@ -1747,7 +1729,7 @@ __global__ void k_cavity_check(Mesh M, const int *dn, const int *cav, const int 
 }
 
 // kernelMarkSteinerOnsegs, refine.cu:5061-5089
-__global__ void k_mark_onsegs(Mesh M, const int *wl, const int *dn, const int *sinks, int *encl2) {
+GQM_KERNEL void k_mark_onsegs(Mesh M, const int *wl, const int *dn, const int *sinks, int *encl2) {
   int n = *dn;
   GS_LOOP(w, n) {
     int sk = sinks[wl[w]];
@@ -1759,7 +1741,7 @@ __global__ void k_mark_onsegs(Mesh M, const int *wl, const int *dn, const int *s
   }
 }
 // kernelResetSteinerInsertionMarker, refine.cu:4601-4649
-__global__ void k_reset_steiner(Mesh M, const int *wl, const int *dn, const int *sinks) {
+GQM_KERNEL void k_reset_steiner(Mesh M, const int *wl, const int *dn, const int *sinks) {
   int n = *dn;
   GS_LOOP(w, n) {
     int sk = sinks[wl[w]];
@@ -1773,7 +1755,7 @@ __global__ void k_reset_steiner(Mesh M, const int *wl, const int *dn, const int 
 }
 
 // kernelInsertSteinerPoints, refine.cu:4651-4900
-__global__ void k_insert_steiner(Mesh M, const int *wl, const int *dn, const int *sinks, const double2 *center,
+GQM_KERNEL void k_insert_steiner(Mesh M, const int *wl, const int *dn, const int *sinks, const double2 *center,
                                  const int *pslots, const int *tslots, const unsigned *ep,
                                  unsigned long long *counter) {
   int n = *dn;
@@ -1867,7 +1849,7 @@ __global__ void k_insert_steiner(Mesh M, const int *wl, const int *dn, const int
 }
 
 // kernelUpdateSteinerNeighbors, refine.cu:4902-5059
-__global__ void k_update_steiner_nbrs(Mesh M, const int *wl, const int *dn, const int *sinks) {
+GQM_KERNEL void k_update_steiner_nbrs(Mesh M, const int *wl, const int *dn, const int *sinks) {
   int n = *dn;
   GS_LOOP(pos, n) {
     int tindex = wl[pos];
@@ -1895,14 +1877,14 @@ __global__ void k_update_steiner_nbrs(Mesh M, const int *wl, const int *dn, cons
 }
 
 // kernelUpdateSteinerOnsegs, refine.cu:5091-5105 (over all subsegments)
-__global__ void k_onsegs_to_enc(Mesh M, const int *encl2, int ns) {
+GQM_KERNEL void k_onsegs_to_enc(Mesh M, const int *encl2, int ns) {
   GS_LOOP(s, ns) if (encl2[s] >= 0) M.enc[s] = 1;
 }
 
 // ============================================================================
 // Output compaction (refine.cu:5758-6484)
 // ============================================================================
-__global__ void k_compact_tris_move(Mesh M, const int *tail, const int *empty, const int *dn, int *newidx) {
+GQM_KERNEL void k_compact_tris_move(Mesh M, const int *tail, const int *empty, const int *dn, int *newidx) {
   int n = *dn;
   GS_LOOP(k, n) {
     int from = tail[k], to = empty[k];
@@ -1914,14 +1896,14 @@ __global__ void k_compact_tris_move(Mesh M, const int *tail, const int *empty, c
     newidx[from] = to;
   }
 }
-__global__ void k_newidx_init(const Mesh M, int *newidx, int n, int newn, const uint8_t *flag, uint8_t deadbit,
+GQM_KERNEL void k_newidx_init(const Mesh M, int *newidx, int n, int newn, const uint8_t *flag, uint8_t deadbit,
                               bool dead_when_set) {
   GS_LOOP(i, n) {
     bool dead = dead_when_set ? (flag[i] & deadbit) != 0 : (flag[i] & deadbit) == 0;
     newidx[i] = dead ? -1 : (i < newn ? i : -2);
   }
 }
-__global__ void k_fix_nbrs(Mesh M, const int *newidx, int newn) {
+GQM_KERNEL void k_fix_nbrs(Mesh M, const int *newidx, int newn) {
   GS_LOOP(t, newn) {
     int4 nb = M.tn[t];
     if (nb.x >= 0) nb.x = etri(newidx[dtri(nb.x)], dori(nb.x));
@@ -1930,13 +1912,13 @@ __global__ void k_fix_nbrs(Mesh M, const int *newidx, int newn) {
     M.tn[t] = nb;
   }
 }
-__global__ void k_fix_s2t(Mesh M, const int *newidx, int ns) {
+GQM_KERNEL void k_fix_s2t(Mesh M, const int *newidx, int ns) {
   GS_LOOP(s, ns) {
     int o = s2t_get(M, s);
     if (o >= 0) M.s2t[s] = s2t_plain(etri(newidx[dtri(o)], dori(o)));
   }
 }
-__global__ void k_compact_pts_move(Mesh M, const int *tail, const int *empty, const int *dn, int *newidx) {
+GQM_KERNEL void k_compact_pts_move(Mesh M, const int *tail, const int *empty, const int *dn, int *newidx) {
   int n = *dn;
   GS_LOOP(k, n) {
     int from = tail[k], to = empty[k];
@@ -1946,7 +1928,7 @@ __global__ void k_compact_pts_move(Mesh M, const int *tail, const int *empty, co
     newidx[from] = to;
   }
 }
-__global__ void k_fix_tri_vertices(Mesh M, const int *newidx, int nt) {
+GQM_KERNEL void k_fix_tri_vertices(Mesh M, const int *newidx, int nt) {
   GS_LOOP(t, nt) {
     int4 v = M.tv[t];
     v.x = newidx[v.x];
@@ -1956,7 +1938,7 @@ __global__ void k_fix_tri_vertices(Mesh M, const int *newidx, int nt) {
   }
 }
 // plain output arrays (trianglelist, neighborlist via decode, segmentlist)
-__global__ void k_emit_output(Mesh M, int nt, int ns, int *tri, int *nbr, int *seg, uint8_t *tstat) {
+GQM_KERNEL void k_emit_output(Mesh M, int nt, int ns, int *tri, int *nbr, int *seg, uint8_t *tstat) {
   GS_LOOP(i, max(nt, ns)) {
     if (i < nt) {
       int4 v = M.tv[i], nb = M.tn[i];
@@ -1981,7 +1963,7 @@ __global__ void k_emit_output(Mesh M, int nt, int ns, int *tri, int *nbr, int *s
     }
   }
 }
-__global__ void k_emit_pstatus(Mesh M, int np, uint8_t *pstat) {
+GQM_KERNEL void k_emit_pstatus(Mesh M, int np, uint8_t *pstat) {
   GS_LOOP(i, np) pstat[i] = (uint8_t)((M.ps[i] & 15) | (M.pred[i] ? 16 : 0));
 }
 

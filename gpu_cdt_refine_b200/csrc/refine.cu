@@ -273,7 +273,7 @@ struct Refiner {
     void *ptrs[] = {M.pts, M.ps, M.pred, M.tv, M.tn, M.tsg, M.tst, M.tflip, M.tfo, M.flip0, M.tmark, M.tpos,
                     M.s2t, M.s2seg, M.enc, M.err, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
                     newidx, tail, center, emptyp, pnew, enclist, encl2, smark, mids, snap, segs, dcount, bc,
-                    dctr, dgc, dinput, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wsup};
+                    dctr, dgc, dinput, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wsup, M.wmeg};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     if (hcount) cudaFreeHost(hcount);
@@ -416,12 +416,14 @@ struct Refiner {
         regrow(&sl, 6 * old, 6 * n) || regrow(&newidx, 0, n) || regrow(&tail, 0, std::max<long>(n, pphys)) ||
         regrow(&center, old, n) || regrow(&M.fstamp, old, n) || regrow(&M.tstamp, old, n) || regrow(&fq, 0, n) ||
         regrow(&tl, 0, n) || regrow(&clr, 0, n) || regrow(&M.wbits, 0, n / 32 + 1) ||
-        regrow(&M.wcnt, 0, n / 1024 + 1) || regrow(&M.wsup, 0, n / 32768 + 1))
+        regrow(&M.wcnt, 0, n / 1024 + 1) || regrow(&M.wsup, 0, n / 32768 + 1) ||
+        regrow(&M.wmeg, 0, n / 1048576 + 1))
       return GQM_ERR_MEMORY;
     // winner bitmap and chunk counts are all zero between flip steps
     cudaMemsetAsync(M.wbits, 0, sizeof(unsigned) * (n / 32 + 1), st);
     cudaMemsetAsync(M.wcnt, 0, sizeof(int) * (n / 1024 + 1), st);
     cudaMemsetAsync(M.wsup, 0, sizeof(int) * (n / 32768 + 1), st);
+    cudaMemsetAsync(M.wmeg, 0, sizeof(int) * (n / 1048576 + 1), st);
     if (n > old) {
       cudaMemsetAsync(M.tst + old, 0, n - old, st);
       cudaMemsetAsync(M.tflip + old, 0, n - old, st);
@@ -859,6 +861,7 @@ struct Refiner {
       cudaMemsetAsync(M.wbits, 0, sizeof(unsigned) * (tphys / 32 + 1), st);
       cudaMemsetAsync(M.wcnt, 0, sizeof(int) * (tphys / 1024 + 1), st);
       cudaMemsetAsync(M.wsup, 0, sizeof(int) * (tphys / 32768 + 1), st);
+      cudaMemsetAsync(M.wmeg, 0, sizeof(int) * (tphys / 1048576 + 1), st);
     }
     cudaMemsetAsync(M.err, 0, sizeof(int), st);
     cudaMemsetAsync(dctr, 0, sizeof(unsigned long long) * 4, st);
