@@ -2,7 +2,8 @@
 
     python -m gpu_cdt_refine_b200.build
 
-libgqm_b200.so : refine.cu (kernels, driver, C ABI) + legacy.cpp (C++ drop-in)
+libgqm_b200.so : refine.cu (kernels, driver, C ABI) + batch.cu (persistent
+                 batched engine) + legacy.cpp (C++ drop-in)
 libgqm_host.so : cdt_build.cpp + synth.cpp + certify.cpp
 
 Every floating-point operation of the refiner is rounded on its own:
@@ -45,15 +46,26 @@ def build_host(force=False):
 
 def build_cuda(force=False, extra=None):
     out = os.path.join(HERE, "libgqm_b200.so")
-    srcs = [os.path.join(CSRC, "refine.cu"), os.path.join(CSRC, "legacy.cpp")]
+    srcs = [os.path.join(CSRC, "refine.cu"), os.path.join(CSRC, "batch.cu"), os.path.join(CSRC, "legacy.cpp")]
     deps = srcs + [os.path.join(CSRC, f) for f in ("kernels.cuh", "gqm_device.cuh", "predicates.h")] + [
         os.path.join(INC, "gqm_refine.h"), os.path.join(INC, "gqm_triangulateio.h")]
-    if force or _stale(out, deps):
-        cmd = [NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
-                               "-Xcompiler", "-ffp-contract=off", "-shared", "-I" + INC, "-o", out] + srcs
-        if extra:
-            cmd[1:1] = extra
-        _run(cmd)
+    if not (force or _stale(out, deps)):
+        return out
+    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler",
+                    "-ffp-contract=off", "-I" + INC] + list(extra or [])
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    # the translation units compile in parallel, then one link
+    procs, objs = [], []
+    for src in srcs:
+        obj = os.path.join(objdir, os.path.basename(src) + ".o")
+        cmd = [NVCC] + flags + ["-c", src, "-o", obj]
+        print(" ".join(cmd), flush=True)
+        procs.append(subprocess.Popen(cmd))
+        objs.append(obj)
+    if any(p.wait() != 0 for p in procs):
+        raise RuntimeError("nvcc failed")
+    _run([NVCC] + ARCH + ["-shared", "-o", out] + objs)
     return out
 
 

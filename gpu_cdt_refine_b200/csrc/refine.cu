@@ -1188,6 +1188,7 @@ const char *gqm_status_string(int s) {
     case GQM_ERR_CUDA: return "CUDA runtime error";
     case GQM_ERR_NO_DEVICE: return "no CUDA device";
     case GQM_ERR_MEMORY: return "device allocation failed";
+    case GQM_ERR_ARENA: return "a batched domain outgrew its scratch arena";
     case GQM_ERR_TOO_LARGE: return "result larger than the no-allocation staging array";
     default: return "unknown status";
   }

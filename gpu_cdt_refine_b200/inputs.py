@@ -110,3 +110,30 @@ def adversarial(seed: int = 20261206, g: int = 700, nc: int = 200, nseg: int = 2
     cand = cand[rng.permutation(cand.shape[0])]
     seg = filter_segments(pts, cand, nseg)
     return build_cdt(pts, seg)
+
+
+def batch_domain(seed: int, nmin: int = 200, nmax: int = 50_000):
+    """One domain of the batched workload: N log-uniform in [nmin, nmax],
+    uniform points or a mixture of 1-8 isotropic Gaussians, segments 5% of N,
+    theta drawn from {15, 18, 20} degrees.  Returns (CDT, theta)."""
+    rng = np.random.default_rng(seed)
+    n = int(round(np.exp(rng.uniform(np.log(nmin), np.log(nmax)))))
+    theta = float(rng.choice([15.0, 18.0, 20.0]))
+    if rng.random() < 0.5:
+        pts = uniform_points(n, 0.0, 1000.0, seed)
+    else:
+        pts = cluster_points(n, int(rng.integers(1, 9)), 1000.0, 5.0, 100.0, 0.0, seed)
+    seg = pick_segments(pts, max(1, n // 20), seed + 1)
+    return build_cdt(pts, seg), theta
+
+
+def batch_domains(count: int = 4096, seed: int = 20261207, nmin: int = 200, nmax: int = 50_000, threads: int = 0):
+    """The batched workload: `count` independent domains (batch_domain with
+    seeds seed, seed+1, ...).  The native generators release the GIL, so
+    `threads` host threads build domains concurrently (0: one per core)."""
+    import os
+    from concurrent.futures import ThreadPoolExecutor
+    nthreads = threads or max(1, os.cpu_count() or 1)
+    with ThreadPoolExecutor(nthreads) as ex:
+        res = list(ex.map(lambda k: batch_domain(seed + 2 * k, nmin, nmax), range(count)))
+    return [r[0] for r in res], [r[1] for r in res]

@@ -63,6 +63,20 @@ class Probe(ctypes.Structure):
         return d
 
 
+class BatchOptions(ctypes.Structure):
+    _fields_ = [("threads_per_block", ctypes.c_int), ("blocks_per_sm", ctypes.c_int),
+                ("memory_fraction", ctypes.c_double)]
+
+
+class BatchReport(ctypes.Structure):
+    _fields_ = [("grid", ctypes.c_int), ("threads_per_block", ctypes.c_int), ("blocks_per_sm", ctypes.c_int),
+                ("fallbacks", ctypes.c_int), ("arena_bytes", ctypes.c_longlong), ("kernel_ms", ctypes.c_double),
+                ("h2d_ms", ctypes.c_double), ("d2h_ms", ctypes.c_double), ("total_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class RefineError(RuntimeError):
     def __init__(self, status, msg):
         super().__init__(f"{msg} (status {status})")
@@ -107,6 +121,17 @@ def lib() -> ctypes.CDLL:
         L.gqm_context_flip_profile.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong),
                                                ctypes.POINTER(ctypes.c_longlong)]
         L.gqm_context_flip_profile.restype = ctypes.c_int
+        L.gqm_refine_batch_persistent.argtypes = [ctypes.c_int, ctypes.POINTER(CdtIn), ctypes.POINTER(CdtOut),
+                                                  ctypes.POINTER(Options), ctypes.POINTER(Stats),
+                                                  ctypes.POINTER(BatchOptions), ctypes.POINTER(BatchReport),
+                                                  ctypes.POINTER(ctypes.c_int)]
+        L.gqm_refine_batch_persistent.restype = ctypes.c_int
+        L.gqm_batch_autotune.argtypes = [ctypes.c_int, ctypes.POINTER(CdtIn), ctypes.POINTER(Options),
+                                         ctypes.POINTER(BatchOptions), ctypes.POINTER(ctypes.c_double)]
+        L.gqm_batch_autotune.restype = ctypes.c_int
+        L.gqm_batch_variants.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+        L.gqm_batch_variants.restype = ctypes.c_int
+        L.gqm_batch_release.argtypes = [ctypes.c_int]
         L.gqm_context_probe.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.gqm_context_probe.restype = ctypes.c_int
         L.gqm_context_probe_read.argtypes = [ctypes.c_void_p, ctypes.POINTER(Probe)]
@@ -193,6 +218,69 @@ def refine_batch(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, predicates=P
         for i in range(n):
             L.gqm_free_result(ctypes.byref(outs[i]))
     return res, [sts[i].as_dict() for i in range(n)]
+
+
+def _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds, keep):
+    n = len(cdts)
+    if np.isscalar(thetas):
+        thetas = [float(thetas)] * n
+    if np.isscalar(predicates):
+        predicates = [int(predicates)] * n
+    ins = (CdtIn * n)(*[_cdt_in(c, keep) for c in cdts])
+    opts = (Options * n)(*[make_options(t, insertpolicy, mode, p, device, max_rounds)
+                           for t, p in zip(thetas, predicates)])
+    return ins, opts
+
+
+def refine_batch_persistent(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0,
+                            threads_per_block=0, blocks_per_sm=0, max_rounds=0, with_report=False):
+    """Refine independent CDTs in one persistent launch
+    (gqm_refine_batch_persistent); returns (list of CDT, list of stats dicts)
+    and, with with_report, the call's report as a third item."""
+    L = lib()
+    n = len(cdts)
+    keep = []
+    ins, opts = _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds, keep)
+    outs = (CdtOut * n)()
+    sts = (Stats * n)()
+    bo = BatchOptions(int(threads_per_block), int(blocks_per_sm), 0.0)
+    rep = BatchReport()
+    bad = ctypes.c_int(-1)
+    rc = L.gqm_refine_batch_persistent(n, ins, outs, opts, sts, ctypes.byref(bo), ctypes.byref(rep),
+                                       ctypes.byref(bad))
+    try:
+        if rc != 0:
+            raise RefineError(rc, f"domain {bad.value}: " + L.gqm_status_string(rc).decode())
+        res = [_take(outs[i]) for i in range(n)]
+    finally:
+        for i in range(n):
+            L.gqm_free_result(ctypes.byref(outs[i]))
+    stats = [sts[i].as_dict() for i in range(n)]
+    if with_report:
+        return res, stats, rep.as_dict()
+    return res, stats
+
+
+def batch_variants():
+    """The compiled (threads per block, blocks per SM) pairs of the batch kernel."""
+    L = lib()
+    t, b = (ctypes.c_int * 16)(), (ctypes.c_int * 16)()
+    n = L.gqm_batch_variants(t, b, 16)
+    return [(t[i], b[i]) for i in range(n)]
+
+
+def batch_autotune(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0):
+    """Time every batch kernel variant on `cdts` and keep the fastest for later
+    calls on `device`; returns ((threads, blocks per SM), {variant: kernel ms})."""
+    L = lib()
+    keep = []
+    ins, opts = _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, 0, keep)
+    chosen = BatchOptions()
+    ms = (ctypes.c_double * 16)()
+    rc = L.gqm_batch_autotune(len(cdts), ins, opts, ctypes.byref(chosen), ms)
+    if rc != 0:
+        raise RefineError(rc, "autotune: " + L.gqm_status_string(rc).decode())
+    return (chosen.threads_per_block, chosen.blocks_per_sm), {v: ms[i] for i, v in enumerate(batch_variants())}
 
 
 def GPU_Refine_Quality(input: CDT, theta: float, insertpolicy=Offcenter, deletepolicy=Connected, mode=1,

@@ -32,6 +32,7 @@ extern "C" {
 #define GQM_ERR_CUDA (-10)        /* a CUDA runtime call failed */
 #define GQM_ERR_NO_DEVICE (-11)   /* no CUDA device */
 #define GQM_ERR_MEMORY (-12)      /* device allocation failed */
+#define GQM_ERR_ARENA (-14)       /* a batched domain outgrew its block's scratch arena */
 
 /* InsertPolicy (GPU_Refine/refine.h:32) */
 #define GQM_CIRCUMCENTER 0
@@ -172,6 +173,45 @@ int gqm_context_result_noalloc(gqm_context *ctx, gqm_cdt_out *out);
  * Returns GQM_OK or the first failing domain's status (*failed_domain set). */
 int gqm_refine_batch(int ndomains, const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt,
                      gqm_stats *stats, int workers, int *failed_domain);
+
+/* Persistent batched refinement (no counterpart in the reference, which
+ * refines one CDT per call).  One kernel launch refines every domain: each
+ * thread block takes the next domain from a queue ordered largest first and
+ * runs the whole refinement of it (rounds, flip-flop loops, compaction) on the
+ * device, in a scratch arena of its own sized for the largest domain.  Each
+ * domain's result is the one gqm_refine would return for it.  A domain whose
+ * mesh outgrows its arena (GQM_ERR_ARENA) is refined again by the
+ * single-domain GPU path; report->fallbacks counts those.  All domains must
+ * name the same device.  Device and pinned host buffers are kept per device
+ * between calls (grow only) and released by gqm_batch_release. */
+typedef struct {
+  int threads_per_block; /* 128, 256 or 512; 0 = the autotuned choice */
+  int blocks_per_sm;     /* resident blocks per SM asked of the compiler; 0 = autotuned */
+  double memory_fraction;/* share of the free device memory the call may take; 0 = 0.8 */
+} gqm_batch_options;
+typedef struct {
+  int grid;              /* blocks launched */
+  int threads_per_block;
+  int blocks_per_sm;
+  int fallbacks;         /* domains re-run by the single-domain path */
+  long long arena_bytes; /* scratch arena of one block */
+  double kernel_ms;      /* the persistent launches (CUDA events) */
+  double h2d_ms, d2h_ms; /* input upload; output download and unpacking */
+  double total_ms;       /* the whole call */
+} gqm_batch_report;
+void gqm_default_batch_options(gqm_batch_options *b);
+int gqm_refine_batch_persistent(int ndomains, const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt,
+                                gqm_stats *stats, const gqm_batch_options *bopt, gqm_batch_report *report,
+                                int *failed_domain);
+/* Autotuner of the persistent batch: times every compiled (threads per block,
+ * blocks per SM) variant on the given sample of domains, keeps the fastest as
+ * the autotuned choice of that device for later calls, and returns it in
+ * *chosen (and each variant's kernel time in ms_per_variant[k], k < the value
+ * returned by gqm_batch_variants, when not NULL). */
+int gqm_batch_variants(int *threads, int *blocks_per_sm, int max);
+int gqm_batch_autotune(int ndomains, const gqm_cdt_in *in, const gqm_options *opt, gqm_batch_options *chosen,
+                       double *ms_per_variant);
+void gqm_batch_release(int device);
 
 const char *gqm_status_string(int status);
 int gqm_version(void);

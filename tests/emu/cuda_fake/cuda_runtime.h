@@ -112,6 +112,7 @@ inline int __shfl_down_sync(unsigned, int v, int) { return v; }
 inline unsigned __ballot_sync(unsigned, bool p) { return p ? 1u : 0u; }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
 inline int __shfl_up_sync(unsigned, int v, int) { return v; }
+inline int __shfl_sync(unsigned, int v, int) { return v; }
 inline int __ffs(unsigned v) { return __builtin_ffs(v); }
 inline int __clz(int v) { return v == 0 ? 32 : __builtin_clz((unsigned)v); }
 

@@ -90,3 +90,50 @@ def test_emulated_batch(emulated):
         want, info = oracle_py.refine(d, th, 1, 1)
         _same(g, want)
         assert st["rounds"] == info["rounds"]
+
+
+def _persistent_domains():
+    doms = [inputs.plain_small(seed=320 + i, n=n, nseg=max(4, n // 20)) for i, n in enumerate([300, 1500, 700, 2500])]
+    doms.append(inputs.clustered(seed=329, n=2000, nseg=100))
+    return doms
+
+
+def test_emulated_persistent_batch_matches_oracle(emulated):
+    """The persistent batch engine (csrc/batch.cu: one block refines a whole
+    domain, the driver running on the device) gives each domain the oracle's
+    result byte for byte, for mixed angles, modes and insertion policies."""
+    doms = _persistent_domains()
+    cfg = [(15.0, 1, 1), (20.0, 1, 0), (18.0, 0, 1), (20.0, 0, 0), (20.0, 1, 1)]
+    for (theta, policy, mode), d in zip(cfg, doms):
+        got, st = refine.refine_batch_persistent([d], theta, policy, mode)
+        want, info = oracle_py.refine(d, theta, policy, mode)
+        _same(got[0], want)
+        assert st[0]["rounds"] == info["rounds"]
+    got, st, rep = refine.refine_batch_persistent(doms, [c[0] for c in cfg], with_report=True)
+    assert rep["fallbacks"] == 0
+    for (theta, _, _), d, g in zip(cfg, doms, got):
+        want, _ = oracle_py.refine(d, theta, 1, 1)
+        _same(g, want)
+
+
+def test_emulated_persistent_batch_exact_predicates(emulated):
+    """Domains with exact predicates run in their own persistent launch and
+    match the single-domain path with exact predicates."""
+    doms = _persistent_domains()[:3]
+    preds = [refine.PRED_EXACT, refine.PRED_REFERENCE, refine.PRED_EXACT]
+    got, _ = refine.refine_batch_persistent(doms, 20.0, predicates=preds)
+    for d, p, g in zip(doms, preds, got):
+        one, _ = refine.refine(d, 20.0, predicates=p)
+        _same(g, one)
+
+
+@pytest.mark.parametrize("emulated", ["libgqm_emu_tight.so"], indirect=True)
+def test_emulated_persistent_batch_arena_fallback(emulated):
+    """Arenas with no room to grow: domains that outgrow them are refined again
+    by the single-domain path, and every result is still the oracle's."""
+    doms = _persistent_domains()
+    got, _, rep = refine.refine_batch_persistent(doms, 20.0, with_report=True)
+    assert rep["fallbacks"] > 0
+    for d, g in zip(doms, got):
+        want, _ = oracle_py.refine(d, 20.0, 1, 1)
+        _same(g, want)
