@@ -66,6 +66,10 @@ def parse():
     p.add_argument("--seed", type=int, default=20261205)
     p.add_argument("--cpu-baseline", type=int, default=1, help="time the CPU baseline (rank 0, N=1)")
     p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--batch-domains", type=int, default=4096,
+                   help="also time the batched workload with this many domains (0: skip)")
+    p.add_argument("--batch-sample", type=int, default=64,
+                   help="domains refined one call each to time the per-domain path")
     return p.parse_args()
 
 
@@ -149,6 +153,42 @@ def cpu_sample(args):
     input on one core)."""
     from gpu_cdt_refine_b200 import inputs
     return inputs.clustered(seed=args.seed + 7, n=max(args.points // 8, 1000), nseg=max(args.segments // 8, 50))
+
+
+def run_batch_workload(args, local_rank):
+    """The batched workload (independent domains, N log-uniform in [200, 50000],
+    uniform or 1-8 Gaussian clusters, segments 5% of N, theta from {15, 18, 20},
+    Ruppert, Offcenter) through the persistent engine, against single-domain
+    calls on a seeded sample of the same domains (time scaled to all domains)."""
+    from gpu_cdt_refine_b200 import inputs, refine
+    t0 = time.time()
+    doms, thetas = inputs.batch_domains(args.batch_domains)
+    gen_s = time.time() - t0
+    rng = np.random.default_rng(7)
+    n = len(doms)
+    tune = sorted(rng.choice(n, min(256, n), replace=False).tolist())
+    chosen, tune_ms = refine.batch_autotune([doms[i] for i in tune], [thetas[i] for i in tune], device=local_rank)
+    refine.refine_batch_persistent(doms, thetas, device=local_rank)  # warm-up (buffers grow once)
+    t0 = time.perf_counter()
+    got, _, rep = refine.refine_batch_persistent(doms, thetas, device=local_rank, with_report=True)
+    call_ms = (time.perf_counter() - t0) * 1e3
+    tris = sum(g.numberoftriangles for g in got)
+    samp = sorted(rng.choice(n, min(args.batch_sample, n), replace=False).tolist())
+    refine.refine(doms[samp[0]], thetas[samp[0]], device=local_rank)
+    t0 = time.perf_counter()
+    for i in samp:
+        refine.refine(doms[i], thetas[i], device=local_rank)
+    single_ms = (time.perf_counter() - t0) * 1e3 * n / len(samp)
+    return {"workload": f"{n} independent domains, N log-uniform [200, 50000], uniform or 1-8 Gaussian clusters, "
+                        f"segments 5% of N, theta in {{15, 18, 20}}, Ruppert, Offcenter",
+            "domains": n, "points_in": int(sum(d.numberofpoints for d in doms)), "output_triangles": int(tris),
+            "kernel_ms": rep["kernel_ms"], "call_ms": call_ms, "report": rep,
+            "triangles_per_s_call": tris / (call_ms / 1e3), "triangles_per_s_kernel": tris / (rep["kernel_ms"] / 1e3),
+            "variant": list(chosen), "autotune_ms": {f"{k[0]}x{k[1]}": v for k, v in tune_ms.items()},
+            "per_domain_calls_ms": single_ms,
+            "per_domain_sample": f"{len(samp)} seeded domains, one gqm_refine call each (host arrays in and out), "
+                                 f"time scaled by {n}/{len(samp)}",
+            "generation_s": gen_s}
 
 
 def time_triangle(cdt, reps, theta=20.0, mode=1):
@@ -283,6 +323,8 @@ def run_ours(args, rank, world, local_rank):
                                        "end) in one extra probed step after the timed region",
                              "path_achieved_gbs": path_gbs, "path_frac": path_gbs / peak},
                 "clocks": clk.summary(), "input_generation_s": gen_s}
+        if args.batch_domains > 0 and world == 1:
+            line["batch"] = run_batch_workload(args, local_rank)
         if args.cpu_baseline and world == 1:
             try:
                 smp = cpu_sample(args)

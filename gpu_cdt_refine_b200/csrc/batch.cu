@@ -27,6 +27,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../../include/gqm_refine.h"
@@ -766,6 +767,24 @@ int grow_host(char **p, size_t *cap, size_t need) {
 }
 size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// f(k) for k in [0, n) on the host's cores (packing and unpacking of the
+// domains' arrays are independent memcpy's)
+template <class F>
+void parallel_for(int n, F f) {
+  int nt = (int)std::thread::hardware_concurrency();
+  nt = std::max(1, std::min(nt, 32));
+  if (n < 64 || nt == 1) {
+    for (int k = 0; k < n; ++k) f(k);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&, t] {
+      for (int k = t; k < n; k += nt) f(k);
+    });
+  for (auto &th : pool) th.join();
+}
+
 int check_domain(const gqm_cdt_in *in, const gqm_options *opt) {
   if (!in || !opt) return GQM_ERR_ARGUMENT;
   if (in->numberofpoints < 3 || in->numberoftriangles < 1 || in->numberofsegments < 0) return GQM_ERR_ARGUMENT;
@@ -840,16 +859,20 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
   }
   // inputs packed into pinned memory, one upload
   std::vector<Job> jobs(n);
-  for (int k = 0; k < n; ++k) {
-    const int d = ids[k];
-    const gqm_cdt_in &D = in[d];
+  parallel_for(n, [&](int k) {
+    const gqm_cdt_in &D = in[ids[k]];
     char *h = C.h_in + in_off[k];
-    char *g = C.d_in + in_off[k];
     const size_t bp = up256(16ull * D.numberofpoints), bt = up256(12ull * D.numberoftriangles);
     memcpy(h, D.pointlist, 16ull * D.numberofpoints);
     memcpy(h + bp, D.trianglelist, 12ull * D.numberoftriangles);
     memcpy(h + bp + bt, D.neighborlist, 12ull * D.numberoftriangles);
     if (D.numberofsegments) memcpy(h + bp + 2 * bt, D.segmentlist, 8ull * D.numberofsegments);
+  });
+  for (int k = 0; k < n; ++k) {
+    const int d = ids[k];
+    const gqm_cdt_in &D = in[d];
+    char *g = C.d_in + in_off[k];
+    const size_t bp = up256(16ull * D.numberofpoints), bt = up256(12ull * D.numberoftriangles);
     Job &J = jobs[k];
     memset(&J, 0, sizeof(J));
     J.pts = reinterpret_cast<const double2 *>(g);
@@ -909,6 +932,7 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
     if (used && cudaMemcpy(C.h_out, C.d_out, (size_t)used, cudaMemcpyDeviceToHost) != cudaSuccess)
       return GQM_ERR_CUDA;
   }
+  int alloc_fail = 0;
   for (int k = 0; k < n; ++k) {
     const int d = ids[k];
     const Job &J = jobs[k];
@@ -928,8 +952,6 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
       s.device_ms = kms;
     }
     if (!keep_outputs) continue;
-    const OutLayout L = out_layout(J.out_np, J.out_nt, J.out_ns);
-    const char *o = C.h_out + J.ooff;
     gqm_cdt_out &R = out[d];
     R.numberofpoints = J.out_np;
     R.numberoftriangles = J.out_nt;
@@ -940,17 +962,24 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
     R.segmentlist = (int *)malloc(8ull * J.out_ns + 16);
     R.pstatus = (unsigned char *)malloc((size_t)J.out_np + 16);
     R.tstatus = (unsigned char *)malloc((size_t)J.out_nt + 16);
-    if (!R.pointlist || !R.trianglelist || !R.neighborlist || !R.segmentlist || !R.pstatus || !R.tstatus) {
-      gqm_free_result(&R);
-      return GQM_ERR_MEMORY;
-    }
-    memcpy(R.pointlist, o + L.pts, 16ull * J.out_np);
-    memcpy(R.trianglelist, o + L.tri, 12ull * J.out_nt);
-    memcpy(R.neighborlist, o + L.nbr, 12ull * J.out_nt);
-    memcpy(R.segmentlist, o + L.seg, 8ull * J.out_ns);
-    memcpy(R.pstatus, o + L.ps, (size_t)J.out_np);
-    memcpy(R.tstatus, o + L.ts, (size_t)J.out_nt);
+    if (!R.pointlist || !R.trianglelist || !R.neighborlist || !R.segmentlist || !R.pstatus || !R.tstatus)
+      alloc_fail = 1;
   }
+  if (alloc_fail) return GQM_ERR_MEMORY;  // the caller releases every out[]
+  if (keep_outputs)
+    parallel_for(n, [&](int k) {
+      const Job &J = jobs[k];
+      if (J.status != GQM_OK) return;
+      const OutLayout L = out_layout(J.out_np, J.out_nt, J.out_ns);
+      const char *o = C.h_out + J.ooff;
+      gqm_cdt_out &R = out[ids[k]];
+      memcpy(R.pointlist, o + L.pts, 16ull * J.out_np);
+      memcpy(R.trianglelist, o + L.tri, 12ull * J.out_nt);
+      memcpy(R.neighborlist, o + L.nbr, 12ull * J.out_nt);
+      memcpy(R.segmentlist, o + L.seg, 8ull * J.out_ns);
+      memcpy(R.pstatus, o + L.ps, (size_t)J.out_np);
+      memcpy(R.tstatus, o + L.ts, (size_t)J.out_nt);
+    });
   if (rep) {
     rep->grid = (int)grid;
     rep->threads_per_block = V.threads;
@@ -1024,7 +1053,11 @@ int batch_call(int nd, const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options
     for (int i = 0; i < nd; ++i)
       if ((opt[i].predicates ? 1 : 0) == pred) ids.push_back(i);
     rc = run_batch(C, ids, in, out, opt, stats, var, frac, status.data(), rep, keep);
-    if (rc) return rc;
+    if (rc) {
+      if (keep)
+        for (int j = 0; j < nd; ++j) gqm_free_result(&out[j]);
+      return rc;
+    }
   }
   // domains that outgrew their arena: the single-domain path
   for (int i = 0; i < nd; ++i) {
