@@ -3,7 +3,8 @@
     python -m gpu_cdt_refine_b200.build
 
 libgqm_b200.so : refine.cu (kernels, driver, C ABI) + batch.cu (persistent
-                 batched engine) + legacy.cpp (C++ drop-in)
+                 batched engine) + learned.cu (placement network training and
+                 inference) + legacy.cpp (C++ drop-in)
 libgqm_host.so : cdt_build.cpp + synth.cpp + certify.cpp
 
 Every floating-point operation of the refiner is rounded on its own:
@@ -46,8 +47,8 @@ def build_host(force=False):
 
 def build_cuda(force=False, extra=None):
     out = os.path.join(HERE, "libgqm_b200.so")
-    srcs = [os.path.join(CSRC, "refine.cu"), os.path.join(CSRC, "batch.cu"), os.path.join(CSRC, "legacy.cpp")]
-    deps = srcs + [os.path.join(CSRC, f) for f in ("kernels.cuh", "gqm_device.cuh", "predicates.h")] + [
+    srcs = [os.path.join(CSRC, f) for f in ("refine.cu", "batch.cu", "learned.cu", "legacy.cpp")]
+    deps = srcs + [os.path.join(CSRC, f) for f in ("kernels.cuh", "gqm_device.cuh", "predicates.h", "learned.cuh")] + [
         os.path.join(INC, "gqm_refine.h"), os.path.join(INC, "gqm_triangulateio.h")]
     if not (force or _stale(out, deps)):
         return out

@@ -130,7 +130,8 @@ struct Job {
   const int *tri, *nbr;
   const int2 *seg;
   int np, nt, ns;
-  int offcenter, offconstant, mode, pred;
+  int offcenter, offconstant, mode, pred, placement;
+  MlpDev mlp;  // GQM_PLACE_LEARNED: the network on the device
   double theta;
   long long max_rounds;
   // outputs: each finished domain takes its space from one shared region
@@ -141,7 +142,7 @@ struct Job {
   unsigned long long ooff;  // offset of this domain's output block
   // results
   int status, out_np, out_nt, out_ns, rounds;
-  long long flip_steps, steiner, midpoints, bad_total, exact_fallbacks;
+  long long flip_steps, steiner, midpoints, bad_total, exact_fallbacks, learned_candidates, learned_used;
   double goodcos2;
 };
 
@@ -286,7 +287,7 @@ enum { C_LIST0 = 0, C_LIST1, C_LIST2, C_MISC };
 struct Shared {
   Scratch S;
   FlipCtl fc;
-  unsigned long long ctr[4];  // Steiner points, midpoints, (unused), (unused)
+  unsigned long long ctr[6];  // Steiner points, midpoints, -, -, learned candidates, learned points
   double gc[2];
   int cnt[8];
   int scan[33];
@@ -301,7 +302,8 @@ struct Cta {
   long pcap, tcap;
   int last_point, last_triangle, last_subseg;
   int nempty_p, nempty_t, lenp, lent;
-  int offcenter, offconstant;
+  int offcenter, offconstant, placement;
+  MlpDev mlp;
   long long max_rounds;
 
   __device__ bool lead() const { return threadIdx.x == 0; }
@@ -474,6 +476,10 @@ struct Cta {
     k_circumcenter(S.M, S.bad, dn, (double)offconstant, offcenter, S.center);
     cta_fill(S.M.tmark, last_triangle, kMaxInt);
     SYNC();
+    if (placement == GQM_PLACE_LEARNED) {
+      k_learned_place(S.M, S.bad, dn, mlp, S.center, sh.ctr + 4);
+      SYNC();
+    }
     k_locate<PRED>(S.M, S.bad, dn, S.center, S.sinks);
     SYNC();
     k_remove_losers(S.M, S.bad, dn, S.sinks, S.imark);
@@ -546,6 +552,8 @@ struct Cta {
     c = caps_of(np, nt, ns);
     offcenter = J.offcenter;
     offconstant = J.offconstant;
+    placement = J.placement;
+    mlp = J.mlp;
     max_rounds = J.max_rounds;
     pcap = np + c.pointblock;
     tcap = nt + c.triblock;
@@ -553,7 +561,7 @@ struct Cta {
       S.M.segs = J.seg;
       S.M.err = &sh.err;
       sh.err = 0;
-      for (int i = 0; i < 4; ++i) sh.ctr[i] = 0;
+      for (int i = 0; i < 6; ++i) sh.ctr[i] = 0;
       FlipCtl &fc = sh.fc;
       fc.gen = 0;
       fc.epoch = 0;
@@ -662,6 +670,8 @@ struct Cta {
       J.steiner = (long long)sh.ctr[0];
       J.midpoints = (long long)sh.ctr[1];
       J.exact_fallbacks = (long long)sh.ctr[2];
+      J.learned_candidates = (long long)sh.ctr[4];
+      J.learned_used = (long long)sh.ctr[5];
     }
     return rc;
   }
@@ -791,6 +801,7 @@ int check_domain(const gqm_cdt_in *in, const gqm_options *opt) {
   if (!in->pointlist || !in->trianglelist || !in->neighborlist) return GQM_ERR_ARGUMENT;
   if (in->numberofsegments > 0 && !in->segmentlist) return GQM_ERR_ARGUMENT;
   if (!(opt->theta > 0.0 && opt->theta < 60.0)) return GQM_ERR_ARGUMENT;
+  if (opt->placement != GQM_PLACE_PLAIN && (opt->placement != GQM_PLACE_LEARNED || !opt->mlp)) return GQM_ERR_ARGUMENT;
   return GQM_OK;
 }
 
@@ -900,6 +911,33 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
     J.ocap = out_bound;
     J.status = GQM_ERR_CUDA;  // overwritten by the block that refines it
   }
+  // networks of the learned placement: one device copy per distinct array
+  std::vector<const float *> nets;
+  for (int k = 0; k < n; ++k) {
+    const gqm_options &o = opt[ids[k]];
+    if (o.placement == GQM_PLACE_LEARNED && std::find(nets.begin(), nets.end(), o.mlp) == nets.end())
+      nets.push_back(o.mlp);
+  }
+  char *dnet = nullptr;
+  const size_t net_bytes = up256(sizeof(uint16_t) * kMlpW) + up256(sizeof(float) * kMlpB);
+  if (!nets.empty()) {
+    if (cudaMalloc((void **)&dnet, net_bytes * nets.size()) != cudaSuccess) return GQM_ERR_MEMORY;
+    std::vector<char> h(net_bytes * nets.size());
+    for (size_t i = 0; i < nets.size(); ++i)
+      mlp_pack(nets[i], reinterpret_cast<uint16_t *>(h.data() + i * net_bytes),
+               reinterpret_cast<float *>(h.data() + i * net_bytes + up256(sizeof(uint16_t) * kMlpW)));
+    cudaMemcpy(dnet, h.data(), h.size(), cudaMemcpyHostToDevice);
+  }
+  for (int k = 0; k < n; ++k) {
+    const gqm_options &o = opt[ids[k]];
+    jobs[k].placement = o.placement == GQM_PLACE_LEARNED ? GQM_PLACE_LEARNED : GQM_PLACE_PLAIN;
+    if (jobs[k].placement == GQM_PLACE_LEARNED) {
+      const size_t i = (size_t)(std::find(nets.begin(), nets.end(), o.mlp) - nets.begin());
+      char *base = dnet + i * net_bytes;
+      jobs[k].mlp = mlp_dev(reinterpret_cast<uint16_t *>(base),
+                            reinterpret_cast<float *>(base + up256(sizeof(uint16_t) * kMlpW)));
+    }
+  }
   // largest first
   std::vector<int> order(n);
   for (int k = 0; k < n; ++k) order[k] = k;
@@ -919,9 +957,13 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
   V.fn<<<(unsigned)grid, V.threads, 0, C.st>>>(C.d_jobs, C.d_order, n, C.d_next, C.d_arena, arena, jobs[0].pred);
 #endif
   cudaEventRecord(C.e1, C.st);
-  if (cudaStreamSynchronize(C.st) != cudaSuccess || cudaGetLastError() != cudaSuccess) return GQM_ERR_CUDA;
+  if (cudaStreamSynchronize(C.st) != cudaSuccess || cudaGetLastError() != cudaSuccess) {
+    if (dnet) cudaFree(dnet);
+    return GQM_ERR_CUDA;
+  }
   float kms = 0.0f;
   cudaEventElapsedTime(&kms, C.e0, C.e1);
+  if (dnet) cudaFree(dnet);
   // results: the job table, then the used part of the output region
   auto t1 = std::chrono::steady_clock::now();
   unsigned long long used = 0;
@@ -947,6 +989,8 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
       s.midpoints_inserted = J.midpoints;
       s.bad_total = J.bad_total;
       s.exact_fallbacks = J.exact_fallbacks;
+      s.learned_candidates = J.learned_candidates;
+      s.learned_used = J.learned_used;
       s.goodcos2 = J.goodcos2;
       s.kernel_launches = 1;
       s.device_ms = kms;

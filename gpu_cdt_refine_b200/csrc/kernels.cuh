@@ -5,6 +5,7 @@
 // launch never waits for the host to learn a count.
 #pragma once
 #include "gqm_device.cuh"
+#include "learned.cuh"
 
 // Register budget of the latency-bound walk kernels (flip checks, cavity
 // walks, link updates): ask for at least this many resident 256-thread blocks
@@ -1965,6 +1966,163 @@ GQM_KERNEL void k_emit_output(Mesh M, int nt, int ns, int *tri, int *nbr, int *s
 }
 GQM_KERNEL void k_emit_pstatus(Mesh M, int np, uint8_t *pstat) {
   GS_LOOP(i, np) pstat[i] = (uint8_t)((M.ps[i] & 15) | (M.pred[i] ? 16 : 0));
+}
+
+// ---------------------------------------------------------------------------
+// The placement step and the collection of training data
+// ---------------------------------------------------------------------------
+#ifdef GQM_CTA_MODE
+#define GQM_BID 0
+#define GQM_NB 1
+#else
+#define GQM_BID ((int)blockIdx.x)
+#define GQM_NB ((int)gridDim.x)
+#endif
+
+// Learned placement over the bad triangles, after k_circumcenter has written
+// the plain centers: two warps per block, 32 candidates per warp and pass.
+// ctr[0] counts candidates, ctr[1] the points the network placed.
+GQM_KERNEL void k_learned_place(Mesh M, const int *bad, const int *dn, MlpDev P, double2 *center,
+                                unsigned long long *ctr) {
+#ifdef GQM_HOST_EMU
+  const int n = *dn;
+  for (int k = 0; k < n; ++k) {
+    const int t = bad[k];
+    const int4 v = M.tv[t];
+    const double2 coff = center[k];
+    const double2 cc = circumcenter(M.pts[v.x], M.pts[v.y], M.pts[v.z], 0.0, false);
+    if (coff.x == cc.x && coff.y == cc.y) continue;
+    float f[kFeat];
+    features_of(M, t, bisector_of(M, t), 0.0, f);
+    const float y = mlp_forward_row(P, f);
+    ctr[0]++;
+    if (y > 0.0f && y < 1.0f) {
+      const double2 p = make_double2(coff.x + (double)y * (cc.x - coff.x), coff.y + (double)y * (cc.y - coff.y));
+      if (!encroaches_near(M, t, p)) {
+        center[k] = p;
+        ctr[1]++;
+      }
+    }
+  }
+#else
+  __shared__ MlpInferSmem sm[2];
+  const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31u);
+  if (warp >= 2) return;
+  MlpInferSmem &s = sm[warp];
+  const int n = *dn;
+  for (int g0 = (GQM_BID * 2 + warp) * 32; g0 < n; g0 += GQM_NB * 2 * 32) {
+    const int k = g0 + lane;
+    bool cand = false;
+    int t = -1;
+    double2 coff = make_double2(0.0, 0.0), cc = coff;
+    if (k < n) {
+      t = bad[k];
+      const int4 v = M.tv[t];
+      coff = center[k];
+      cc = circumcenter(M.pts[v.x], M.pts[v.y], M.pts[v.z], 0.0, false);
+      cand = (coff.x != cc.x || coff.y != cc.y);
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, cand);
+    if (!m) continue;
+    float f[kFeat];
+    if (cand) {
+      const Bisector B = bisector_of(M, t);
+      features_of(M, t, B, 0.0, f);
+    } else {
+      for (int j = 0; j < kFeat; ++j) f[j] = 0.0f;
+    }
+    for (int j = 0; j < kFeat; ++j) s.x[lane * kFeat + j] = f2bf(f[j]);
+    const float y = mlp_forward_warp(P, s.x, s.h, s.a1, nullptr);
+    bool used = false;
+    if (cand && y > 0.0f && y < 1.0f) {
+      const double2 p = make_double2(coff.x + (double)y * (cc.x - coff.x), coff.y + (double)y * (cc.y - coff.y));
+      if (!encroaches_near(M, t, p)) {
+        center[k] = p;
+        used = true;
+      }
+    }
+    const unsigned u = __ballot_sync(0xffffffffu, used);
+    if (lane == 0) {
+      atomicAdd(ctr, (unsigned long long)__popc(m));
+      atomicAdd(ctr + 1, (unsigned long long)__popc(u));
+    }
+  }
+#endif
+}
+
+// Number of triangles with an angle below theta among those that point c
+// would form with the boundary of its Delaunay cavity (the triangles whose
+// circumcircle contains c, reached from t0 without crossing a subsegment);
+// 100 when the cavity has more than 64 triangles.
+__device__ inline int star_bad_count(const Mesh &M, int t0, double2 c) {
+  int list[64];
+  int n = 0, nbad = 0;
+  list[n++] = t0;
+  for (int i = 0; i < n; ++i) {
+    const int tri = list[i];
+    const int4 v = M.tv[tri], nb = M.tn[tri], sg = M.tsg[tri];
+    const int vv[3] = {v.x, v.y, v.z};
+    for (int e = 0; e < 3; ++e) {
+      bool boundary = comp(sg, e) >= 0 || comp(nb, e) < 0;
+      if (!boundary) {
+        const int nt = dtri(comp(nb, e));
+        bool seen = false;
+        for (int j = 0; j < n && !seen; ++j) seen = (list[j] == nt);
+        if (seen) continue;
+        const int4 w = M.tv[nt];
+        const double2 a = M.pts[w.x], b = M.pts[w.y], d = M.pts[w.z];
+        if (gqm_incircle_det_ref(a.x, a.y, b.x, b.y, d.x, d.y, c.x, c.y) > 0.0) {
+          if (n == 64) return 100;
+          list[n++] = nt;
+          continue;
+        }
+        boundary = true;
+      }
+      // star triangle (c, u, w) on the boundary edge
+      const double2 u = M.pts[vv[(e + 1) % 3]], w = M.pts[vv[(e + 2) % 3]];
+      const double l0 = (u.x - w.x) * (u.x - w.x) + (u.y - w.y) * (u.y - w.y);
+      const double l1 = (c.x - w.x) * (c.x - w.x) + (c.y - w.y) * (c.y - w.y);
+      const double l2 = (c.x - u.x) * (c.x - u.x) + (c.y - u.y) * (c.y - u.y);
+      // smallest angle is opposite the shortest side: cos^2 by the law of cosines
+      double a2 = l0, b2 = l1, c2 = l2;
+      if (b2 < a2) { const double tt = a2; a2 = b2; b2 = tt; }
+      if (c2 < a2) { const double tt = a2; a2 = c2; c2 = tt; }
+      const double num = b2 + c2 - a2;
+      const double cos2 = (num * num) / (4.0 * b2 * c2);
+      if (num > 0.0 && cos2 > M.gc2) nbad++;
+    }
+  }
+  return nbad;
+}
+
+// Training rows: features and target t of every learned-placement candidate
+// among the bad triangles (centers hold the plain points).
+GQM_KERNEL void k_collect(Mesh M, const int *bad, const int *dn, const double2 *center, float *feat, float *target,
+                          unsigned long long *count, unsigned long long cap) {
+  const int n = *dn;
+  GS_LOOP(k, n) {
+    const int t = bad[k];
+    const int4 v = M.tv[t];
+    const double2 coff = center[k];
+    const double2 cc = circumcenter(M.pts[v.x], M.pts[v.y], M.pts[v.z], 0.0, false);
+    if (coff.x == cc.x && coff.y == cc.y) continue;
+    int best = 1 << 30, bj = 0;
+    for (int j = 0; j <= 8; ++j) {
+      const double tj = j / 8.0;
+      const double2 p = make_double2(coff.x + tj * (cc.x - coff.x), coff.y + tj * (cc.y - coff.y));
+      if (j > 0 && encroaches_near(M, t, p)) continue;
+      const int c = star_bad_count(M, t, p);
+      if (c < best) {  // a point beyond the off-center only when it is strictly better
+        best = c;
+        bj = j;
+      }
+    }
+    const unsigned long long row = atomicAdd(count, 1ull);
+    if (row >= cap) continue;
+    const Bisector B = bisector_of(M, t);
+    features_of(M, t, B, 0.0, feat + row * kFeat);
+    target[row] = bj / 8.0f;
+  }
 }
 
 }  // namespace gqm

@@ -46,6 +46,19 @@ struct MlpDev {
   const uint16_t *w1, *w2, *w3;
   const float *b1, *b2, *b3;
 };
+// Packed device form: weights w1 | w2 | w3 (bf16), biases b1 | b2 | b3 (fp32).
+constexpr int kMlpW = kHid * kFeat + kHid * kHid + kHid, kMlpB = 2 * kHid + 1;
+__host__ __device__ inline MlpDev mlp_dev(const uint16_t *w, const float *b) {
+  return MlpDev{w, w + kHid * kFeat, w + kHid * kFeat + kHid * kHid, b, b + kHid, b + 2 * kHid};
+}
+inline void mlp_pack(const float *params, uint16_t *w, float *b) {
+  for (int i = 0; i < kHid * kFeat; ++i) w[i] = f2bf(params[kOffW1 + i]);
+  for (int i = 0; i < kHid * kHid; ++i) w[kHid * kFeat + i] = f2bf(params[kOffW2 + i]);
+  for (int i = 0; i < kHid; ++i) w[kHid * kFeat + kHid * kHid + i] = f2bf(params[kOffW3 + i]);
+  for (int i = 0; i < kHid; ++i) b[i] = params[kOffB1 + i];
+  for (int i = 0; i < kHid; ++i) b[kHid + i] = params[kOffB2 + i];
+  b[2 * kHid] = params[kOffB3];
+}
 
 // ---------------------------------------------------------------------------
 // Warp GEMM on shared-memory operands: C[i][j] (+)= sum_k A(i,k) B(k,j) with
@@ -100,46 +113,63 @@ __device__ inline void warp_gemm(int M, int N, int K, const uint16_t *a, int ai,
 #endif
 }
 
-// Per-warp shared workspace of the network over 32 rows (one per lane).
-struct MlpWarpSmem {
-  uint16_t x[32 * kFeat];  // inputs, bf16
-  float h[32 * kHid];      // pre-activations (fp32)
-  uint16_t a1[32 * kHid];  // layer-1 activations, bf16
-  uint16_t a2[32 * kHid];  // layer-2 activations, bf16
-};
-
-// Forward pass of 32 rows (row r = lane r); x already in s.x.  Returns this
-// lane's output.  Weights are read from global memory (bf16, L1-resident).
-__device__ inline float mlp_forward_warp(const MlpDev &P, MlpWarpSmem &s) {
+// Forward pass of 32 rows (row r = lane r) held in x (bf16, 32 x 32) in shared
+// memory; h (fp32, 32 x 64) and a1 (bf16, 32 x 64) are shared scratch, a2
+// (bf16, 32 x 64) keeps the second layer's activations when not null.
+// Returns this lane's output.  Weights are read from global memory (bf16).
+__device__ inline float mlp_forward_warp(const MlpDev &P, const uint16_t *x, float *h, uint16_t *a1, uint16_t *a2) {
   const int lane = (int)(threadIdx.x & 31u);
   __syncwarp();
   // layer 1: h = x W1^T
-  warp_gemm(32, kHid, kFeat, s.x, kFeat, 1, P.w1, 1, kFeat, s.h, kHid, 1, false);
+  warp_gemm(32, kHid, kFeat, x, kFeat, 1, P.w1, 1, kFeat, h, kHid, 1, false);
   __syncwarp();
   for (int j = 0; j < kHid; ++j) {
-    const float v = s.h[lane * kHid + j] + P.b1[j];
-    s.a1[lane * kHid + j] = f2bf(v > 0.0f ? v : 0.0f);
+    const float v = h[lane * kHid + j] + P.b1[j];
+    a1[lane * kHid + j] = f2bf(v > 0.0f ? v : 0.0f);
   }
   __syncwarp();
   // layer 2: h = a1 W2^T
-  warp_gemm(32, kHid, kHid, s.a1, kHid, 1, P.w2, 1, kHid, s.h, kHid, 1, false);
+  warp_gemm(32, kHid, kHid, a1, kHid, 1, P.w2, 1, kHid, h, kHid, 1, false);
   __syncwarp();
   float y = P.b3[0];
   for (int j = 0; j < kHid; ++j) {
-    const float v = s.h[lane * kHid + j] + P.b2[j];
+    const float v = h[lane * kHid + j] + P.b2[j];
     const uint16_t hb = f2bf(v > 0.0f ? v : 0.0f);
-    s.a2[lane * kHid + j] = hb;
+    if (a2) a2[lane * kHid + j] = hb;
     y += bf2f(hb) * bf2f(P.w3[j]);
   }
   __syncwarp();
   return y;
 }
+// The same network for one row with scalar arithmetic (the CPU emulation of
+// the tests runs kernels one thread at a time, without warps).
+__host__ __device__ inline float mlp_forward_row(const MlpDev &P, const float *f) {
+  float a1[kHid], y = P.b3[0];
+  for (int j = 0; j < kHid; ++j) {
+    float z = 0.0f;
+    for (int k = 0; k < kFeat; ++k) z += bf2f(f2bf(f[k])) * bf2f(P.w1[j * kFeat + k]);
+    z += P.b1[j];
+    a1[j] = bf2f(f2bf(z > 0.0f ? z : 0.0f));
+  }
+  for (int j = 0; j < kHid; ++j) {
+    float z = 0.0f;
+    for (int k = 0; k < kHid; ++k) z += a1[k] * bf2f(P.w2[j * kHid + k]);
+    z += P.b2[j];
+    y += bf2f(f2bf(z > 0.0f ? z : 0.0f)) * bf2f(P.w3[j]);
+  }
+  return y;
+}
+struct MlpInferSmem {
+  uint16_t x[32 * kFeat];
+  float h[32 * kHid];
+  uint16_t a1[32 * kHid];
+};
 
 // ---------------------------------------------------------------------------
-// Features of a bad triangle (scale free): angles, edge ratios, the
-// circumcenter's and off-center's positions on the bisector, the neighbours'
-// shapes, subsegment flags and the distance to the nearest subsegment over
-// the shortest edge.  The triangle is taken with its shortest edge first
+// Features of a bad triangle (scale free, bounded to [-20, 20]): angles, log
+// edge ratios, the circumcenter's position on the bisector (log and asinh),
+// the neighbours' shapes and apex positions (asinh), subsegment flags and the
+// distance to the nearest subsegment over the shortest edge (at most 10).  The triangle is taken with its shortest edge first
 // (org, dest) and the apex opposite it, as computeCircumcenter does.
 // ---------------------------------------------------------------------------
 __device__ inline double tri_angle(double2 p, double2 a, double2 b) {  // angle at p
@@ -208,7 +238,7 @@ __device__ inline void features_of(const Mesh &M, int t, const Bisector &B, doub
   f[k++] = (float)log(ld);
   f[k++] = (float)log(B.s_cc > 1e-12 ? B.s_cc : 1e-12);
   f[k++] = (float)offc;
-  f[k++] = (float)(B.s_cc - offc);
+  f[k++] = (float)asinh(B.s_cc - offc);
   f[k++] = (float)M.gc2;
   // neighbours across the three edges, shortest edge first
   double dmin = 10.0;
@@ -232,8 +262,8 @@ __device__ inline void features_of(const Mesh &M, int t, const Bisector &B, doub
     f[k++] = (float)fmin(a0, fmin(a1, a2));
     f[k++] = (float)tri_angle(q[ni], q[(ni + 1) % 3], q[(ni + 2) % 3]);  // opposite the shared edge
     const double2 x = q[ni];
-    f[k++] = (float)(((x.x - B.mid.x) * B.nrm.x + (x.y - B.mid.y) * B.nrm.y) / B.len);
-    f[k++] = (float)(((x.x - B.mid.x) * (B.d.x - B.o.x) + (x.y - B.mid.y) * (B.d.y - B.o.y)) / (B.len * B.len));
+    f[k++] = (float)asinh(((x.x - B.mid.x) * B.nrm.x + (x.y - B.mid.y) * B.nrm.y) / B.len);
+    f[k++] = (float)asinh(((x.x - B.mid.x) * (B.d.x - B.o.x) + (x.y - B.mid.y) * (B.d.y - B.o.y)) / (B.len * B.len));
     const int4 ns = M.tsg[nt];
     for (int j = 0; j < 3; ++j) {
       const int s2 = comp(ns, j);
@@ -243,6 +273,7 @@ __device__ inline void features_of(const Mesh &M, int t, const Bisector &B, doub
   f[k++] = (float)dmin;
   while (k < kFeat - 1) f[k++] = 0.0f;
   f[kFeat - 1] = 1.0f;
+  for (int j = 0; j < kFeat; ++j) f[j] = fminf(20.0f, fmaxf(-20.0f, f[j]));  // bounded inputs
 }
 
 // Does point c encroach (diametral circle, Ruppert) a subsegment on the edges

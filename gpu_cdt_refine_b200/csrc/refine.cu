@@ -220,12 +220,19 @@ struct Refiner {
   int *dcount = nullptr;  // [16] list sizes on the device
   int *hcount = nullptr;  // pinned mirror
   int *bc = nullptr;      // compaction block counts
-  unsigned long long *dctr = nullptr;  // [4] event counters
+  unsigned long long *dctr = nullptr;  // [8] event counters (Steiner, midpoints, -, -, learned candidates, used)
   double *dgc = nullptr;
   int *dinput = nullptr;  // staging for host inputs
   size_t dinput_bytes = 0;
   // options
   int pred_mode = 0, mode = 1, offcenter = 1, offconstant = 0;
+  // learned Steiner placement: the network on the device
+  int placement = GQM_PLACE_PLAIN;
+  uint16_t *mlp_w = nullptr;
+  float *mlp_b = nullptr;
+  // training-data collection (gqm_learn_collect): device rows and their count
+  float *col_feat = nullptr, *col_tgt = nullptr;
+  unsigned long long *col_cnt = nullptr, col_cap = 0;
   double theta = 20.0;
   long long max_rounds = 1000000;
   gqm_stats stats{};
@@ -273,7 +280,7 @@ struct Refiner {
     void *ptrs[] = {M.pts, M.ps, M.pred, M.tv, M.tn, M.tsg, M.tst, M.tflip, M.tfo, M.flip0, M.tmark, M.tpos,
                     M.s2t, M.s2seg, M.enc, M.err, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
                     newidx, tail, center, emptyp, pnew, enclist, encl2, smark, mids, snap, segs, dcount, bc,
-                    dctr, dgc, dinput, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wsup, M.wmeg};
+                    dctr, dgc, dinput, mlp_w, mlp_b, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wsup, M.wmeg};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     if (hcount) cudaFreeHost(hcount);
@@ -284,6 +291,8 @@ struct Refiner {
     clr = nullptr;
     fc = nullptr;
     ktm = nullptr;
+    mlp_w = nullptr;
+    mlp_b = nullptr;
     for (cudaEvent_t e : loop_ev) cudaEventDestroy(e);
     loop_ev.clear();
     loop_ev_used = 0;
@@ -312,7 +321,7 @@ struct Refiner {
     if (!ev0) cudaEventCreate(&ev0);
     if (!ev1) cudaEventCreate(&ev1);
     if (!dcount) {
-      if (dalloc(&dcount, 16) || dalloc(&bc, kMaxCompactBlocks + 1) || dalloc(&dctr, 4) || dalloc(&dgc, 2) ||
+      if (dalloc(&dcount, 16) || dalloc(&bc, kMaxCompactBlocks + 1) || dalloc(&dctr, 8) || dalloc(&dgc, 2) ||
           dalloc(&M.err, 1) || dalloc(&fc, 1) || dalloc(&ktm, 1))
         return GQM_ERR_MEMORY;
       cudaMemsetAsync(fc, 0, sizeof(FlipCtl), st);
@@ -710,6 +719,12 @@ struct Refiner {
     LAUNCH(k_copy, nbad, imark, bad, dn);
     LAUNCH(k_copy, nbad, ilist, bad, dn);
     LAUNCH(k_circumcenter, nbad, M, bad, dn, (double)offconstant, offcenter, center);
+    if (col_feat) LAUNCH(k_collect, nbad, M, bad, dn, center, col_feat, col_tgt, col_cnt, col_cap);
+    if (placement == GQM_PLACE_LEARNED) {  // two warps of a block take 64 candidates per pass
+      KL(k_learned_place, std::max(1, std::min((nbad + 63) / 64, 148 * 8)), 64)(M, bad, dn, mlp_dev(mlp_w, mlp_b),
+                                                                                center, dctr + 4);
+      stats.kernel_launches++;
+    }
     LAUNCH(k_fill, last_triangle, M.tmark, last_triangle, kMaxInt);
     if (pred_mode)
       LAUNCH(k_locate<1>, nbad, M, bad, dn, center, sinks);
@@ -790,6 +805,16 @@ struct Refiner {
     theta = opt->theta;
     mode = opt->mode ? 1 : 0;
     pred_mode = opt->predicates ? 1 : 0;
+    placement = opt->placement == GQM_PLACE_LEARNED ? GQM_PLACE_LEARNED : GQM_PLACE_PLAIN;
+    if (placement == GQM_PLACE_LEARNED) {
+      if (!mlp_w && (dalloc(&mlp_w, kMlpW) || dalloc(&mlp_b, kMlpB))) return GQM_ERR_MEMORY;
+      std::vector<uint16_t> hw(kMlpW);
+      std::vector<float> hb(kMlpB);
+      mlp_pack(opt->mlp, hw.data(), hb.data());
+      cudaMemcpyAsync(mlp_w, hw.data(), sizeof(uint16_t) * kMlpW, cudaMemcpyHostToDevice, st);
+      cudaMemcpyAsync(mlp_b, hb.data(), sizeof(float) * kMlpB, cudaMemcpyHostToDevice, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_ERR_CUDA;
+    }
     max_rounds = opt->max_rounds > 0 ? opt->max_rounds : 1000000;
     offcenter = 0;
     double offc = 0.0;
@@ -864,7 +889,7 @@ struct Refiner {
       cudaMemsetAsync(M.wmeg, 0, sizeof(int) * (tphys / 1048576 + 1), st);
     }
     cudaMemsetAsync(M.err, 0, sizeof(int), st);
-    cudaMemsetAsync(dctr, 0, sizeof(unsigned long long) * 4, st);
+    cudaMemsetAsync(dctr, 0, sizeof(unsigned long long) * 8, st);
     KL(k_ctl_reset, 1, 32)(fc, 64 * max_rounds, M.err);
     LAUNCH(k_check_input, std::max(np, nt), (const double2 *)dpts, np, dtri_in, dnbr_in, nt, dseg_in, ns, M.err);
     rc = check_device_error();
@@ -940,8 +965,10 @@ struct Refiner {
     cudaEventElapsedTime(&ms, ev0, ev1);
     stats.device_ms = ms;
     collect_loop_events();
-    unsigned long long hc[4];
+    unsigned long long hc[8];
     cudaMemcpy(hc, dctr, sizeof(hc), cudaMemcpyDeviceToHost);
+    stats.learned_candidates = (long long)hc[4];
+    stats.learned_used = (long long)hc[5];
     FlipCtl hf;
     cudaMemcpy(&hf, fc, sizeof(hf), cudaMemcpyDeviceToHost);
     stats.flip_steps = hf.steps;
@@ -1008,6 +1035,8 @@ void gqm_default_options(gqm_options *o) {
   o->predicates = GQM_PRED_REFERENCE;
   o->device = 0;
   o->max_rounds = 0;
+  o->placement = GQM_PLACE_PLAIN;
+  o->mlp = nullptr;
 }
 
 static int validate(const gqm_cdt_in *in, const gqm_options *opt) {
@@ -1016,6 +1045,7 @@ static int validate(const gqm_cdt_in *in, const gqm_options *opt) {
   if (!in->pointlist || !in->trianglelist || !in->neighborlist) return GQM_ERR_ARGUMENT;
   if (in->numberofsegments > 0 && !in->segmentlist) return GQM_ERR_ARGUMENT;
   if (!(opt->theta > 0.0 && opt->theta < 60.0)) return GQM_ERR_ARGUMENT;
+  if (opt->placement != GQM_PLACE_PLAIN && (opt->placement != GQM_PLACE_LEARNED || !opt->mlp)) return GQM_ERR_ARGUMENT;
   return GQM_OK;
 }
 
@@ -1082,6 +1112,45 @@ int gqm_context_flip_profile(gqm_context *ctx, long long *steps, long long *item
     items[b] = ctx->r.flip_prof_items[b];
   }
   return GQM_OK;
+}
+int gqm_learn_collect(const gqm_cdt_in *in, const gqm_options *opt, float *features, float *targets, long long cap,
+                      long long *count) {
+  if (!in || !opt || cap < 0 || (cap > 0 && (!features || !targets))) return GQM_ERR_ARGUMENT;
+  gqm_options o = *opt;
+  o.placement = GQM_PLACE_PLAIN;  // the rows describe the plain refinement
+  o.mlp = nullptr;
+  int rc = validate(in, &o);
+  if (rc) return rc;
+  gqm_context *ctx = nullptr;
+  rc = gqm_context_create(o.device, &ctx);
+  if (rc) return rc;
+  gqm::Refiner &r = ctx->r;
+  const size_t rows = (size_t)(cap > 0 ? cap : 1);
+  if (r.dalloc(&r.col_feat, rows * gqm::kFeat) || r.dalloc(&r.col_tgt, rows) || r.dalloc(&r.col_cnt, 1)) {
+    rc = GQM_ERR_MEMORY;
+  } else {
+    cudaMemset(r.col_cnt, 0, sizeof(unsigned long long));
+    r.col_cap = (unsigned long long)cap;
+    gqm_stats st;
+    rc = gqm_context_run(ctx, in, 0, &o, &st);
+    unsigned long long n = 0;
+    if (!rc && cudaMemcpy(&n, r.col_cnt, sizeof(n), cudaMemcpyDeviceToHost) != cudaSuccess) rc = GQM_ERR_CUDA;
+    if (!rc) {
+      const long long m = (long long)std::min<unsigned long long>(n, (unsigned long long)cap);
+      if (m > 0 && (cudaMemcpy(features, r.col_feat, sizeof(float) * gqm::kFeat * m, cudaMemcpyDeviceToHost) !=
+                        cudaSuccess ||
+                    cudaMemcpy(targets, r.col_tgt, sizeof(float) * m, cudaMemcpyDeviceToHost) != cudaSuccess))
+        rc = GQM_ERR_CUDA;
+      if (count) *count = m;
+    }
+  }
+  if (r.col_feat) cudaFree(r.col_feat);
+  if (r.col_tgt) cudaFree(r.col_tgt);
+  if (r.col_cnt) cudaFree(r.col_cnt);
+  r.col_feat = r.col_tgt = nullptr;
+  r.col_cnt = nullptr;
+  gqm_context_destroy(ctx);
+  return rc;
 }
 int gqm_context_result_sizes(gqm_context *ctx, int *np, int *nt, int *ns) {
   if (!ctx || !ctx->r.have_result) return GQM_ERR_ARGUMENT;

@@ -38,7 +38,8 @@ class CdtOut(ctypes.Structure):
 
 class Options(ctypes.Structure):
     _fields_ = [("theta", ctypes.c_double), ("insert_policy", ctypes.c_int), ("mode", ctypes.c_int),
-                ("predicates", ctypes.c_int), ("device", ctypes.c_int), ("max_rounds", ctypes.c_longlong)]
+                ("predicates", ctypes.c_int), ("device", ctypes.c_int), ("max_rounds", ctypes.c_longlong),
+                ("placement", ctypes.c_int), ("mlp", ctypes.c_void_p)]
 
 
 class Stats(ctypes.Structure):
@@ -46,7 +47,8 @@ class Stats(ctypes.Structure):
                 ("steiner_inserted", ctypes.c_longlong), ("midpoints_inserted", ctypes.c_longlong),
                 ("bad_total", ctypes.c_longlong), ("host_syncs", ctypes.c_longlong),
                 ("kernel_launches", ctypes.c_longlong), ("exact_fallbacks", ctypes.c_longlong),
-                ("goodcos2", ctypes.c_double), ("device_ms", ctypes.c_double)]
+                ("goodcos2", ctypes.c_double), ("device_ms", ctypes.c_double),
+                ("learned_candidates", ctypes.c_longlong), ("learned_used", ctypes.c_longlong)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -132,6 +134,18 @@ def lib() -> ctypes.CDLL:
         L.gqm_batch_variants.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), ctypes.c_int]
         L.gqm_batch_variants.restype = ctypes.c_int
         L.gqm_batch_release.argtypes = [ctypes.c_int]
+        fp = ctypes.POINTER(ctypes.c_float)
+        L.gqm_learn_collect.argtypes = [ctypes.POINTER(CdtIn), ctypes.POINTER(Options), fp, fp, ctypes.c_longlong,
+                                        ctypes.POINTER(ctypes.c_longlong)]
+        L.gqm_learn_collect.restype = ctypes.c_int
+        if hasattr(L, "gqm_mlp_infer"):  # absent from the CPU emulation build of the tests
+            L.gqm_mlp_infer.argtypes = [ctypes.c_int, fp, fp, ctypes.c_longlong, fp]
+            L.gqm_mlp_infer.restype = ctypes.c_int
+            L.gqm_mlp_grad.argtypes = [ctypes.c_int, fp, fp, fp, ctypes.c_longlong, fp, fp]
+            L.gqm_mlp_grad.restype = ctypes.c_int
+            L.gqm_mlp_train.argtypes = [ctypes.c_int, fp, fp, fp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_float, ctypes.c_uint, fp]
+            L.gqm_mlp_train.restype = ctypes.c_int
         L.gqm_context_probe.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.gqm_context_probe.restype = ctypes.c_int
         L.gqm_context_probe_read.argtypes = [ctypes.c_void_p, ctypes.POINTER(Probe)]
@@ -140,8 +154,15 @@ def lib() -> ctypes.CDLL:
     return _lib
 
 
+PLACE_PLAIN, PLACE_LEARNED = 0, 1
+MLP_FEATURES, MLP_PARAMS = 32, 6337
+
+
 def make_options(theta=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0,
-                 max_rounds=0) -> Options:
+                 max_rounds=0, mlp=None) -> Options:
+    """Options of one refinement.  mlp: a float32 array of MLP_PARAMS network
+    parameters selects the learned Steiner placement (the caller keeps the
+    array alive while the options are in use)."""
     o = Options()
     lib().gqm_default_options(ctypes.byref(o))
     o.theta = float(theta)
@@ -150,6 +171,11 @@ def make_options(theta=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REF
     o.predicates = int(predicates)
     o.device = int(device)
     o.max_rounds = int(max_rounds)
+    if mlp is not None:
+        if mlp.dtype != np.float32 or mlp.shape != (MLP_PARAMS,) or not mlp.flags.c_contiguous:
+            raise ValueError("mlp must be a contiguous float32 array of MLP_PARAMS values")
+        o.placement = PLACE_LEARNED
+        o.mlp = mlp.ctypes.data
     return o
 
 
@@ -175,14 +201,14 @@ def _take(out: CdtOut, with_status=False):
 
 
 def refine(cdt: CDT, theta=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0,
-           max_rounds=0, with_status=False):
+           max_rounds=0, with_status=False, mlp=None):
     """Refine a CDT on the GPU; returns (CDT, stats dict) or (CDT, ps, ts, stats)."""
     L = lib()
     keep = []
     cin = _cdt_in(cdt, keep)
     out = CdtOut()
     st = Stats()
-    opt = make_options(theta, insertpolicy, mode, predicates, device, max_rounds)
+    opt = make_options(theta, insertpolicy, mode, predicates, device, max_rounds, mlp)
     rc = L.gqm_refine(ctypes.byref(cin), ctypes.byref(out), ctypes.byref(opt), ctypes.byref(st))
     if rc != 0:
         raise RefineError(rc, L.gqm_status_string(rc).decode())
@@ -220,27 +246,27 @@ def refine_batch(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, predicates=P
     return res, [sts[i].as_dict() for i in range(n)]
 
 
-def _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds, keep):
+def _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds, keep, mlp=None):
     n = len(cdts)
     if np.isscalar(thetas):
         thetas = [float(thetas)] * n
     if np.isscalar(predicates):
         predicates = [int(predicates)] * n
     ins = (CdtIn * n)(*[_cdt_in(c, keep) for c in cdts])
-    opts = (Options * n)(*[make_options(t, insertpolicy, mode, p, device, max_rounds)
+    opts = (Options * n)(*[make_options(t, insertpolicy, mode, p, device, max_rounds, mlp)
                            for t, p in zip(thetas, predicates)])
     return ins, opts
 
 
 def refine_batch_persistent(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0,
-                            threads_per_block=0, blocks_per_sm=0, max_rounds=0, with_report=False):
+                            threads_per_block=0, blocks_per_sm=0, max_rounds=0, with_report=False, mlp=None):
     """Refine independent CDTs in one persistent launch
     (gqm_refine_batch_persistent); returns (list of CDT, list of stats dicts)
     and, with with_report, the call's report as a third item."""
     L = lib()
     n = len(cdts)
     keep = []
-    ins, opts = _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds, keep)
+    ins, opts = _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds, keep, mlp)
     outs = (CdtOut * n)()
     sts = (Stats * n)()
     bo = BatchOptions(int(threads_per_block), int(blocks_per_sm), 0.0)
@@ -281,6 +307,82 @@ def batch_autotune(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, predicates
     if rc != 0:
         raise RefineError(rc, "autotune: " + L.gqm_status_string(rc).decode())
     return (chosen.threads_per_block, chosen.blocks_per_sm), {v: ms[i] for i, v in enumerate(batch_variants())}
+
+
+# --- learned Steiner placement ----------------------------------------------
+
+def _fp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def mlp_init(seed=0, t0=0.5):
+    """Initial network parameters (He-scaled normal weights, zero biases, output
+    bias t0) as a float32 array of MLP_PARAMS values."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(MLP_PARAMS, np.float32)
+    o = 0
+    p[o:o + 64 * 32] = rng.normal(0, np.sqrt(2.0 / 32), 64 * 32)
+    o += 64 * 32 + 64
+    p[o:o + 64 * 64] = rng.normal(0, np.sqrt(2.0 / 64), 64 * 64)
+    o += 64 * 64 + 64
+    p[o:o + 64] = rng.normal(0, np.sqrt(1.0 / 64), 64) * 0.1
+    p[-1] = t0
+    return p
+
+
+def learn_collect(cdt: CDT, theta=20.0, insertpolicy=Offcenter, mode=1, device=0, cap=1_000_000):
+    """Training rows from a plain refinement of `cdt` (gqm_learn_collect):
+    (features [n, 32] float32, targets [n] float32)."""
+    L = lib()
+    keep = []
+    cin = _cdt_in(cdt, keep)
+    opt = make_options(theta, insertpolicy, mode, PRED_REFERENCE, device)
+    feat = np.zeros((cap, MLP_FEATURES), np.float32)
+    tgt = np.zeros(cap, np.float32)
+    cnt = ctypes.c_longlong(0)
+    rc = L.gqm_learn_collect(ctypes.byref(cin), ctypes.byref(opt), _fp(feat), _fp(tgt), int(cap), ctypes.byref(cnt))
+    if rc != 0:
+        raise RefineError(rc, "learn_collect: " + L.gqm_status_string(rc).decode())
+    return feat[:cnt.value].copy(), tgt[:cnt.value].copy()
+
+
+def mlp_infer(params, features, device=0):
+    L = lib()
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(features, np.float32)
+    out = np.zeros(x.shape[0], np.float32)
+    rc = L.gqm_mlp_infer(int(device), _fp(p), _fp(x), x.shape[0], _fp(out))
+    if rc != 0:
+        raise RefineError(rc, "mlp_infer")
+    return out
+
+
+def mlp_grad(params, features, targets, device=0):
+    """(loss, gradient) of the mean squared error on the GPU."""
+    L = lib()
+    p = np.ascontiguousarray(params, np.float32)
+    x = np.ascontiguousarray(features, np.float32)
+    t = np.ascontiguousarray(targets, np.float32)
+    g = np.zeros(MLP_PARAMS, np.float32)
+    loss = np.zeros(1, np.float32)
+    rc = L.gqm_mlp_grad(int(device), _fp(p), _fp(x), _fp(t), x.shape[0], _fp(loss), _fp(g))
+    if rc != 0:
+        raise RefineError(rc, "mlp_grad")
+    return float(loss[0]), g
+
+
+def mlp_train(params, features, targets, epochs=20, batch=256, lr=1e-3, seed=0, device=0):
+    """Adam training on the GPU; returns (trained params, last epoch's loss)."""
+    L = lib()
+    p = np.array(params, np.float32, copy=True)
+    x = np.ascontiguousarray(features, np.float32)
+    t = np.ascontiguousarray(targets, np.float32)
+    loss = np.zeros(1, np.float32)
+    rc = L.gqm_mlp_train(int(device), _fp(p), _fp(x), _fp(t), x.shape[0], int(epochs), int(batch), float(lr),
+                         int(seed), _fp(loss))
+    if rc != 0:
+        raise RefineError(rc, "mlp_train")
+    return p, float(loss[0])
 
 
 def GPU_Refine_Quality(input: CDT, theta: float, insertpolicy=Offcenter, deletepolicy=Connected, mode=1,

@@ -40,6 +40,10 @@ extern "C" {
 /* refinement mode (GPU_Refine/refine.cu:131: run_mode != 0 is Ruppert) */
 #define GQM_CHEW 0
 #define GQM_RUPPERT 1
+/* Steiner placement (no counterpart in the reference beyond the plain rule) */
+#define GQM_PLACE_PLAIN 0   /* off-center / circumcenter as GPU_Refine/refine.cu:3780-3868 */
+#define GQM_PLACE_LEARNED 1 /* a point between the off-center and the circumcenter chosen by a small
+                               network, with the plain off-center as the fallback (see below) */
 /* predicate arithmetic */
 #define GQM_PRED_REFERENCE 0 /* the reference's effective FP64 arithmetic (bit-exact parity) */
 #define GQM_PRED_EXACT 1     /* exact orient2d/incircle (adaptive filter + expansions) */
@@ -79,6 +83,8 @@ typedef struct {
   int predicates;       /* GQM_PRED_REFERENCE / GQM_PRED_EXACT */
   int device;           /* CUDA device ordinal */
   long long max_rounds; /* bound on every refinement loop; 0 = default (1e6) */
+  int placement;        /* GQM_PLACE_PLAIN (the reference's rule) / GQM_PLACE_LEARNED */
+  const float *mlp;     /* GQM_PLACE_LEARNED: host array of GQM_MLP_PARAMS network parameters */
 } gqm_options;
 
 typedef struct {
@@ -92,6 +98,8 @@ typedef struct {
   long long exact_fallbacks;    /* predicate evaluations that needed the expansion path */
   double goodcos2;              /* cos^2(theta) as evaluated on the device */
   double device_ms;             /* device time of the refinement (CUDA events) */
+  long long learned_candidates; /* GQM_PLACE_LEARNED: Steiner points where the rule could apply */
+  long long learned_used;       /* ... of which the network's point was inserted */
 } gqm_stats;
 
 /* Default options: theta 20, Offcenter, Ruppert, reference predicates, device 0. */
@@ -212,6 +220,39 @@ int gqm_batch_variants(int *threads, int *blocks_per_sm, int max);
 int gqm_batch_autotune(int ndomains, const gqm_cdt_in *in, const gqm_options *opt, gqm_batch_options *chosen,
                        double *ms_per_variant);
 void gqm_batch_release(int device);
+
+/* Learned Steiner placement (no counterpart in the reference).  Where the
+ * reference inserts an off-center (a point on the bisector of the bad
+ * triangle's shortest edge, nearer than the circumcenter), GQM_PLACE_LEARNED
+ * inserts the point at  s_off + t (s_cc - s_off)  on that bisector instead,
+ * t = the network's output for the triangle's 32 features; the off-center is
+ * kept when t <= 0 or t >= 1 or when the point would encroach a subsegment of
+ * the triangle or its neighbours.  The network is 32 -> 64 -> 64 -> 1 with
+ * ReLU, bf16 weights and fp32 accumulation on the tensor cores.  Parameters
+ * are GQM_MLP_PARAMS floats: W1[64][32], b1[64], W2[64][64], b2[64], w3[64],
+ * b3 (weights are rounded to bf16 on the device). */
+#define GQM_MLP_FEATURES 32
+#define GQM_MLP_PARAMS 6337
+/* Training data from a plain refinement of `in` (opt->placement is ignored):
+ * for every bad triangle where the learned rule applies, its features
+ * (GQM_MLP_FEATURES floats) and a target t in [0, 1]: of nine points
+ * t = 0, 1/8, ..., 1 on the bisector, the one whose new triangles (the point
+ * joined to its Delaunay cavity's boundary) include the fewest with an angle
+ * below theta, ties to the smaller t (the off-center unless a point beyond it
+ * is strictly better); points that encroach a subsegment are excluded.  Up to `cap` rows; *count gets the number written. */
+int gqm_learn_collect(const gqm_cdt_in *in, const gqm_options *opt, float *features, float *targets,
+                      long long cap, long long *count);
+/* Network output (the unclamped t) for n feature rows. */
+int gqm_mlp_infer(int device, const float *params, const float *features, long long n, float *out);
+/* Mean squared error of the network on n rows and its gradient with respect
+ * to every parameter (the GPU forward and backward kernels). */
+int gqm_mlp_grad(int device, const float *params, const float *features, const float *targets, long long n,
+                 float *loss, float *grad);
+/* Adam training of params (in place) on n rows: `epochs` passes in
+ * mini-batches of `batch` rows (a multiple of 64), learning rate lr, rows
+ * shuffled with `seed`; *loss gets the last epoch's mean loss. */
+int gqm_mlp_train(int device, float *params, const float *features, const float *targets, long long n,
+                  int epochs, int batch, float lr, unsigned seed, float *loss);
 
 const char *gqm_status_string(int status);
 int gqm_version(void);

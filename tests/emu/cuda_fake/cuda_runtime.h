@@ -108,6 +108,7 @@ inline int atomicAdd(int *a, int v) {
   return o;
 }
 inline void __syncthreads() {}
+inline void __syncwarp(unsigned = 0xffffffffu) {}
 inline int __shfl_down_sync(unsigned, int v, int) { return v; }
 inline unsigned __ballot_sync(unsigned, bool p) { return p ? 1u : 0u; }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
@@ -138,6 +139,10 @@ inline cudaError_t cudaMemcpyAsync(void *d, const void *s, size_t n, cudaMemcpyK
   return cudaSuccess;
 }
 inline cudaError_t cudaMemcpy(void *d, const void *s, size_t n, cudaMemcpyKind k) { return cudaMemcpyAsync(d, s, n, k); }
+inline cudaError_t cudaMemset(void *d, int v, size_t n) {
+  memset(d, v, n);
+  return cudaSuccess;
+}
 inline cudaError_t cudaMemsetAsync(void *d, int v, size_t n, cudaStream_t = nullptr) {
   memset(d, v, n);
   return cudaSuccess;

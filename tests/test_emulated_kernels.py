@@ -137,3 +137,47 @@ def test_emulated_persistent_batch_arena_fallback(emulated):
     for d, g in zip(doms, got):
         want, _ = oracle_py.refine(d, 20.0, 1, 1)
         _same(g, want)
+
+
+def _const_net(t):
+    """A network whose output is the constant t (all weights zero)."""
+    p = np.zeros(refine.MLP_PARAMS, np.float32)
+    p[-1] = t
+    return p
+
+
+def test_emulated_learned_clamp_gives_plain(emulated):
+    """Learned placement whose output is clamped (t <= 0 or t >= 1) keeps
+    every off-center: the result is the plain refinement's, byte for byte."""
+    cdt = inputs.plain_small(seed=331, n=2000, nseg=100)
+    plain, _ = refine.refine(cdt, 20.0)
+    for t in (-0.5, 1.5):
+        got, st = refine.refine(cdt, 20.0, mlp=_const_net(t))
+        _same(got, plain)
+        assert st["learned_candidates"] > 0 and st["learned_used"] == 0
+
+
+def test_emulated_learned_places_and_certifies(emulated):
+    """A network answering t = 0.5 moves the candidates halfway to the
+    circumcenter; the refined mesh is still a certified CDT at theta."""
+    from gpu_cdt_refine_b200.certify import certify
+    cdt = inputs.plain_small(seed=332, n=3000, nseg=150)
+    got, st = refine.refine(cdt, 20.0, mlp=_const_net(0.5))
+    assert 0 < st["learned_used"] <= st["learned_candidates"]
+    cert = certify(got, cdt, 20.0)
+    assert cert["ok"] and cert["triangles_below_theta"] == 0, cert
+    # the persistent batch engine applies the same rule
+    gb, sb = refine.refine_batch_persistent([cdt], 20.0, mlp=_const_net(0.5))
+    _same(gb[0], got)
+    assert sb[0]["learned_used"] == st["learned_used"]
+
+
+def test_emulated_learn_collect(emulated):
+    """Training rows from a plain run: finite features, targets on the 1/8
+    grid of [0, 1], one row per off-center candidate of every round."""
+    cdt = inputs.plain_small(seed=333, n=2000, nseg=100)
+    feat, tgt = refine.learn_collect(cdt, 20.0, cap=100000)
+    _, st = refine.refine(cdt, 20.0, mlp=_const_net(-1.0))
+    assert feat.shape == (st["learned_candidates"], refine.MLP_FEATURES)
+    assert np.isfinite(feat).all() and np.all(feat[:, -1] == 1.0)
+    assert np.all((tgt >= 0) & (tgt <= 1)) and np.allclose(tgt * 8, np.round(tgt * 8))
