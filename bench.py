@@ -70,6 +70,8 @@ def parse():
                    help="also time the batched workload with this many domains (0: skip)")
     p.add_argument("--batch-sample", type=int, default=64,
                    help="domains refined one call each to time the per-domain path")
+    p.add_argument("--extras", type=int, default=1,
+                   help="also measure the adversarial input and the learned placement (0: skip)")
     return p.parse_args()
 
 
@@ -189,6 +191,64 @@ def run_batch_workload(args, local_rank):
             "per_domain_sample": f"{len(samp)} seeded domains, one gqm_refine call each (host arrays in and out), "
                                  f"time scaled by {n}/{len(samp)}",
             "generation_s": gen_s}
+
+
+def run_adversarial(local_rank):
+    """The adversarial input (1,000,000 points: a 700 x 700 grid jittered by
+    1e-9 of its spacing plus 200 concentric circles, 20,000 chords along the
+    circles), theta 20.7, Ruppert, Offcenter, with the reference's predicate
+    arithmetic and with exact predicates; incircle tests that needed the
+    expansion path are counted on the device."""
+    from gpu_cdt_refine_b200 import inputs, refine
+    from gpu_cdt_refine_b200.certify import certify
+    t0 = time.time()
+    cdt = inputs.adversarial()
+    gen_s = time.time() - t0
+    out = {"workload": "700x700 jittered grid + 200 concentric circles, 20,000 chords, theta 20.7, Ruppert, "
+                       "Offcenter", "points_in": cdt.numberofpoints, "segments_in": cdt.numberofsegments,
+           "generation_s": gen_s}
+    for name, pred in (("reference_predicates", refine.PRED_REFERENCE), ("exact_predicates", refine.PRED_EXACT)):
+        refine.refine(cdt, 20.7, refine.Offcenter, 1, predicates=pred, device=local_rank)
+        got, st = refine.refine(cdt, 20.7, refine.Offcenter, 1, predicates=pred, device=local_rank)
+        cert = certify(got, cdt, 20.7)
+        out[name] = {"device_ms": st["device_ms"], "output_triangles": got.numberoftriangles,
+                     "output_vertices": got.numberofpoints, "incircle_expansion_fallbacks": st["exact_fallbacks"],
+                     "fallbacks_per_output_triangle": st["exact_fallbacks"] / max(got.numberoftriangles, 1),
+                     "certified": bool(cert["ok"]), "min_angle_deg": cert["min_angle_deg"],
+                     "triangles_below_theta": cert["triangles_below_theta"]}
+    return out
+
+
+def run_learned(cdt, args, local_rank):
+    """Learned Steiner placement (the network trained by train_placement.py,
+    gpu_cdt_refine_b200/data/placement_mlp.npy) against the plain rule: the
+    clustered input of the main workload and 256 batched domains."""
+    from gpu_cdt_refine_b200 import inputs, refine
+    from gpu_cdt_refine_b200.certify import certify
+    path = os.path.join(ROOT, "gpu_cdt_refine_b200", "data", "placement_mlp.npy")
+    params = np.load(path).astype(np.float32)
+    res = {"network": "gpu_cdt_refine_b200/data/placement_mlp.npy (500 seeded clustered inputs of 200,000 points, "
+                      "theta 20)"}
+    plain, sp = refine.refine(cdt, 20.0, refine.Offcenter, 1, device=local_rank)
+    learned, sl = refine.refine(cdt, 20.0, refine.Offcenter, 1, device=local_rank, mlp=params)
+    learned, sl = refine.refine(cdt, 20.0, refine.Offcenter, 1, device=local_rank, mlp=params)
+    cert = certify(learned, cdt, 20.0)
+    res["clustered_2M"] = {"plain_vertices": plain.numberofpoints, "learned_vertices": learned.numberofpoints,
+                           "vertex_reduction": 1.0 - learned.numberofpoints / plain.numberofpoints,
+                           "plain_device_ms": sp["device_ms"], "learned_device_ms": sl["device_ms"],
+                           "candidates": sl["learned_candidates"], "network_points": sl["learned_used"],
+                           "fallback_rate": 1.0 - sl["learned_used"] / max(sl["learned_candidates"], 1),
+                           "certified": bool(cert["ok"]), "min_angle_deg": cert["min_angle_deg"],
+                           "triangles_below_theta": cert["triangles_below_theta"]}
+    doms, _ = inputs.batch_domains(256, seed=20261209)
+    gp, _, rp = refine.refine_batch_persistent(doms, 20.0, device=local_rank, with_report=True)
+    gl, stl, rl = refine.refine_batch_persistent(doms, 20.0, device=local_rank, with_report=True, mlp=params)
+    pv, lv = sum(g.numberofpoints for g in gp), sum(g.numberofpoints for g in gl)
+    cand, used = sum(s["learned_candidates"] for s in stl), sum(s["learned_used"] for s in stl)
+    res["batch_256"] = {"plain_vertices": pv, "learned_vertices": lv, "vertex_reduction": 1.0 - lv / pv,
+                        "plain_kernel_ms": rp["kernel_ms"], "learned_kernel_ms": rl["kernel_ms"],
+                        "fallback_rate": 1.0 - used / max(cand, 1)}
+    return res
 
 
 def time_triangle(cdt, reps, theta=20.0, mode=1):
@@ -325,6 +385,9 @@ def run_ours(args, rank, world, local_rank):
                 "clocks": clk.summary(), "input_generation_s": gen_s}
         if args.batch_domains > 0 and world == 1:
             line["batch"] = run_batch_workload(args, local_rank)
+        if args.extras and world == 1:
+            line["learned"] = run_learned(cdt, args, local_rank)
+            line["adversarial"] = run_adversarial(local_rank)
         if args.cpu_baseline and world == 1:
             try:
                 smp = cpu_sample(args)

@@ -152,8 +152,14 @@ __device__ __forceinline__ double orient(double2 a, double2 b, double2 c) {
   if (PRED == 0) return gqm_orient_ref(a.x, a.y, b.x, b.y, c.x, c.y);
   return gqm_orient_exact(a.x, a.y, b.x, b.y, c.x, c.y);
 }
+// Incircle tests that needed the expansion path (determinant exactly zero with
+// the reference's arithmetic, filter inconclusive with exact arithmetic),
+// summed over every refinement on the device since the last reset (one
+// counter per compiled module).
+static __device__ unsigned long long g_incircle_fallbacks;
 template <int PRED>
 __device__ __noinline__ double incircle_slow(double2 a, double2 b, double2 c, double2 d) {
+  atomicAdd(&g_incircle_fallbacks, 1ull);
   if (PRED == 0) return gqm_incircle_zero_fallback_ref(a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y);
   return gqm_incircle_exact(a.x, a.y, b.x, b.y, c.x, c.y, d.x, d.y);
 }

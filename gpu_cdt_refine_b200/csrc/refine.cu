@@ -890,6 +890,10 @@ struct Refiner {
     }
     cudaMemsetAsync(M.err, 0, sizeof(int), st);
     cudaMemsetAsync(dctr, 0, sizeof(unsigned long long) * 8, st);
+    {
+      const unsigned long long zero = 0;
+      cudaMemcpyToSymbolAsync(g_incircle_fallbacks, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, st);
+    }
     KL(k_ctl_reset, 1, 32)(fc, 64 * max_rounds, M.err);
     LAUNCH(k_check_input, std::max(np, nt), (const double2 *)dpts, np, dtri_in, dnbr_in, nt, dseg_in, ns, M.err);
     rc = check_device_error();
@@ -978,7 +982,11 @@ struct Refiner {
     }
     stats.steiner_inserted = (long long)hc[0];
     stats.midpoints_inserted = (long long)hc[1];
-    stats.exact_fallbacks = (long long)hc[2];
+    {
+      unsigned long long fb = 0;
+      cudaMemcpyFromSymbol(&fb, g_incircle_fallbacks, sizeof(fb));
+      stats.exact_fallbacks = (long long)fb;
+    }
     have_result = (rc == 0);
     status = rc;
     return rc;

@@ -95,7 +95,8 @@ typedef struct {
   long long bad_total;          /* bad triangles summed over rounds */
   long long host_syncs;         /* device-to-host count reads */
   long long kernel_launches;    /* kernels launched by the refinement */
-  long long exact_fallbacks;    /* predicate evaluations that needed the expansion path */
+  long long exact_fallbacks;    /* incircle tests that needed the expansion path (single-domain
+                                   path; a device-wide count, so concurrent runs on one device add up) */
   double goodcos2;              /* cos^2(theta) as evaluated on the device */
   double device_ms;             /* device time of the refinement (CUDA events) */
   long long learned_candidates; /* GQM_PLACE_LEARNED: Steiner points where the rule could apply */

@@ -177,6 +177,17 @@ inline cudaError_t cudaEventElapsedTime(float *ms, cudaEvent_t a, cudaEvent_t b)
 inline cudaError_t cudaGetLastError() { return cudaSuccess; }
 inline const char *cudaGetErrorString(cudaError_t) { return "emulated"; }
 template <class T>
+inline cudaError_t cudaMemcpyToSymbolAsync(T &sym, const void *src, size_t n, size_t off, cudaMemcpyKind,
+                                           cudaStream_t = nullptr) {
+  memcpy((char *)&sym + off, src, n);
+  return cudaSuccess;
+}
+template <class T>
+inline cudaError_t cudaMemcpyFromSymbol(void *dst, const T &sym, size_t n) {
+  memcpy(dst, &sym, n);
+  return cudaSuccess;
+}
+template <class T>
 inline cudaError_t cudaGetSymbolAddress(void **p, T &sym) {
   *p = (void *)&sym;
   return cudaSuccess;

@@ -82,3 +82,26 @@ def test_constant_network_places_and_certifies(gpu):
     assert cert["ok"] and cert["triangles_below_theta"] == 0, cert
     gb, sb = refine.refine_batch_persistent([cdt, cdt], 20.0, mlp=p)
     assert _same(gb[0], got) and _same(gb[1], got)
+
+
+def test_trained_network_against_plain(gpu):
+    """What the trained network (gpu_cdt_refine_b200/data/placement_mlp.npy)
+    gains over the plain off-center rule on held-out inputs: both meshes are
+    certified at theta; the vertex counts are reported.  Measured on the
+    clustered distribution the network was trained on, the learned rule is
+    within a fraction of a percent of the plain rule (it does not reach fewer
+    vertices), which this test pins."""
+    import os
+    p = np.load(os.path.join(os.path.dirname(refine.__file__), "data", "placement_mlp.npy")).astype(np.float32)
+    gains = []
+    for s in range(2):
+        cdt = inputs.clustered(seed=9100 + s, n=100_000, nseg=5000)
+        a, _ = refine.refine(cdt, 20.0)
+        b, st = refine.refine(cdt, 20.0, mlp=p)
+        for m in (a, b):
+            cert = certify(m, cdt, 20.0)
+            assert cert["ok"] and cert["triangles_below_theta"] == 0 and cert["min_angle_deg"] >= 20.0
+        assert 0 < st["learned_used"] < st["learned_candidates"]
+        gains.append((a.numberofpoints - b.numberofpoints) / a.numberofpoints)
+    print(f"\nvertex reduction of the learned rule: {[f'{100 * g:.2f}%' for g in gains]}")
+    assert all(abs(g) < 0.02 for g in gains)

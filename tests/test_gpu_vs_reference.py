@@ -1,0 +1,60 @@
+"""The refiner against the reference's own GPU build (oracle/_ref, compiled
+from the reference sources by oracle/Makefile) on the same B200, same inputs:
+wall time of the whole call with host arrays in and out on both sides (the
+reference's driver times GPU_Refine_Quality as GPU_Refine/main.cpp:1858-1868
+does), and the refined meshes.
+
+The largest input here stays below the 1,280,000 input triangles up to which
+the reference's initSubsegs is correct (GPU_Refine/refine.cu:5691-5747).  The
+reference's runs on these inputs are not all alike (its subseg2tri stores
+race), so the meshes are compared as sizes and certified, not byte for byte;
+byte-for-byte parity with the reference's consistent runs is in
+test_gpu_golden.py."""
+import json
+import os
+import subprocess
+import tempfile
+import time
+
+import numpy as np
+import pytest
+
+from gpu_cdt_refine_b200 import cdtio, inputs, refine
+from gpu_cdt_refine_b200.certify import certify
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF = os.path.join(ROOT, "oracle", "_ref", "gqm_ref_run")
+
+
+def _ref_ms(path, reps=3):
+    with tempfile.TemporaryDirectory() as d:
+        p = subprocess.run([REF, path, os.path.join(d, "o.bin"), "20.0", "1", "1", str(reps)], capture_output=True,
+                           text=True, timeout=600)
+        assert p.returncode == 0, p.stderr[-400:]
+        info = json.loads([l for l in p.stderr.splitlines() if l.startswith("GQMREF ")][0][7:])
+        return info, cdtio.read_cdt(os.path.join(d, "o.bin"))
+
+
+@pytest.mark.skipif(not os.path.exists(REF), reason="reference build (make -C oracle ref) not present")
+@pytest.mark.parametrize("n", [100_000, 500_000])
+def test_faster_than_reference_gpu(gpu, n):
+    cdt = inputs.clustered(seed=31, n=n, nseg=n // 20)
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "in.bin")
+        cdtio.write_cdt(path, cdt)
+        info, ref_out = _ref_ms(path)
+    refine.refine(cdt, 20.0)  # warm-up (context and buffers)
+    ours = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        got, _ = refine.refine(cdt, 20.0)
+        ours.append((time.perf_counter() - t0) * 1e3)
+    ref_ms, our_ms = float(np.median(info["ms"])), float(np.median(ours))
+    print(f"\n{n} points: reference {ref_ms:.1f} ms, ours {our_ms:.1f} ms, x{ref_ms / our_ms:.2f}; "
+          f"triangles {ref_out.numberoftriangles} / {got.numberoftriangles}")
+    cert = certify(got, cdt, 20.0)
+    assert cert["ok"] and cert["triangles_below_theta"] == 0
+    assert abs(got.numberoftriangles - ref_out.numberoftriangles) <= 0.01 * ref_out.numberoftriangles
+    assert ref_ms >= 3.0 * our_ms, (ref_ms, our_ms)
