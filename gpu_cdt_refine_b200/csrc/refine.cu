@@ -16,6 +16,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
+#include <initializer_list>
 #include <mutex>
 #include <thread>
 #include <vector>
@@ -175,6 +176,32 @@ __global__ void k_set_count(int *dst, int v) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *dst = v;
 }
 
+// Host memcpy of a few large arrays on the host's cores (staging to and from
+// pinned memory): every copy is cut into pieces of 8 MB shared by the threads.
+struct HostCopy {
+  void *dst;
+  const void *src;
+  size_t bytes;
+};
+static void host_copy(std::initializer_list<HostCopy> list) {
+  constexpr size_t kPiece = 8u << 20;
+  std::vector<HostCopy> pieces;
+  for (const HostCopy &c : list)
+    for (size_t o = 0; o < c.bytes; o += kPiece)
+      pieces.push_back({(char *)c.dst + o, (const char *)c.src + o, std::min(kPiece, c.bytes - o)});
+  int nt = (int)std::min<size_t>(pieces.size(), std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  if (nt <= 1) {
+    for (const HostCopy &c : pieces) memcpy(c.dst, c.src, c.bytes);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back([&, t] {
+      for (size_t k = t; k < pieces.size(); k += nt) memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
+    });
+  for (auto &th : pool) th.join();
+}
+
 // ============================================================================
 // Refiner
 // ============================================================================
@@ -224,6 +251,12 @@ struct Refiner {
   double *dgc = nullptr;
   int *dinput = nullptr;  // staging for host inputs
   size_t dinput_bytes = 0;
+  // kept between runs (grow only): pinned host staging of inputs and results,
+  // the device result block, segment copy and the initSubsegs hash
+  char *h_stage = nullptr, *d_out = nullptr;
+  size_t h_stage_cap = 0, d_out_cap = 0, segs_cap = 0, hash_cap = 0;
+  unsigned long long *hkeys = nullptr;
+  int *hvals = nullptr, *s2ti = nullptr;
   // options
   int pred_mode = 0, mode = 1, offcenter = 1, offconstant = 0;
   // learned Steiner placement: the network on the device
@@ -250,6 +283,31 @@ struct Refiner {
   static cudaError_t dalloc(T **p, size_t n) {
     *p = nullptr;
     return cudaMalloc((void **)p, sizeof(T) * std::max<size_t>(n, 1));
+  }
+  // grow-only buffers kept between runs
+  int grow_pinned(size_t need) {
+    if (need <= h_stage_cap) return GQM_OK;
+    if (h_stage) cudaFreeHost(h_stage);
+    h_stage = nullptr;
+    h_stage_cap = 0;
+    if (cudaMallocHost((void **)&h_stage, need) != cudaSuccess) {
+      h_stage = nullptr;
+      return GQM_ERR_MEMORY;
+    }
+    h_stage_cap = need;
+    return GQM_OK;
+  }
+  template <class T>
+  int grow_dev(T **q, size_t *cap, size_t n) {
+    if (n <= *cap && *q) return GQM_OK;
+    if (*q) cudaFree(*q);
+    *cap = 0;
+    if (dalloc(q, n) != cudaSuccess) {
+      *q = nullptr;
+      return GQM_ERR_MEMORY;
+    }
+    *cap = n;
+    return GQM_OK;
   }
   // grow a device array to n elements, keeping its first `keep` elements
   template <class T>
@@ -306,6 +364,13 @@ struct Refiner {
     dgc = nullptr;
     dinput = nullptr;
     dinput_bytes = 0;
+    if (h_stage) cudaFreeHost(h_stage);
+    for (void *q : {(void *)d_out, (void *)hkeys, (void *)hvals, (void *)s2ti})
+      if (q) cudaFree(q);
+    h_stage = d_out = nullptr;
+    hkeys = nullptr;
+    hvals = s2ti = nullptr;
+    h_stage_cap = d_out_cap = segs_cap = hash_cap = 0;
     pphys = tphys = sphys = 0;
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -861,10 +926,13 @@ struct Refiner {
       int *t0 = (int *)(base + sizeof(double) * 2 * np);
       int *n0 = t0 + 3L * nt;
       int *s0 = n0 + 3L * nt;
-      cudaMemcpyAsync(p0, in->pointlist, sizeof(double) * 2 * np, cudaMemcpyHostToDevice, st);
-      cudaMemcpyAsync(t0, in->trianglelist, sizeof(int) * 3 * nt, cudaMemcpyHostToDevice, st);
-      cudaMemcpyAsync(n0, in->neighborlist, sizeof(int) * 3 * nt, cudaMemcpyHostToDevice, st);
-      if (ns) cudaMemcpyAsync(s0, in->segmentlist, sizeof(int) * 2 * ns, cudaMemcpyHostToDevice, st);
+      // the caller's arrays are packed into pinned memory on the host's cores,
+      // then uploaded with one copy
+      if (grow_pinned(need)) return GQM_ERR_MEMORY;
+      const size_t bp = sizeof(double) * 2 * np, bt = sizeof(int) * 3 * nt, bs = sizeof(int) * 2 * ns;
+      host_copy({{h_stage, in->pointlist, bp}, {h_stage + bp, in->trianglelist, bt},
+                 {h_stage + bp + bt, in->neighborlist, bt}, {h_stage + bp + 2 * bt, in->segmentlist, bs}});
+      cudaMemcpyAsync(base, h_stage, bp + 2 * bt + bs, cudaMemcpyHostToDevice, st);
       dpts = p0;
       dtri_in = t0;
       dnbr_in = n0;
@@ -876,9 +944,7 @@ struct Refiner {
       dseg_in = in->segmentlist;
     }
     cudaEventRecord(ev0, st);
-    if (segs) cudaFree(segs);
-    segs = nullptr;
-    if (dalloc(&segs, ns + 1)) return GQM_ERR_MEMORY;
+    if (grow_dev(&segs, &segs_cap, (size_t)ns + 1)) return GQM_ERR_MEMORY;
     if (ns) cudaMemcpyAsync(segs, dseg_in, sizeof(int2) * ns, cudaMemcpyDeviceToDevice, st);
     M.segs = segs;
     cudaMemsetAsync(M.s2t, 0, sizeof(s2t_t) * sphys, st);
@@ -912,18 +978,22 @@ struct Refiner {
     {
       unsigned hsz = 1;
       while (hsz < 2u * (unsigned)ns + 16) hsz <<= 1;
-      unsigned long long *keys = nullptr;
-      int *vals = nullptr, *s2ti = nullptr;
-      if (dalloc(&keys, hsz) || dalloc(&vals, hsz) || dalloc(&s2ti, ns + 1)) return GQM_ERR_MEMORY;
-      cudaMemsetAsync(keys, 0xff, sizeof(unsigned long long) * hsz, st);
+      if (hsz > hash_cap) {
+        if (grow_dev(&hkeys, &hash_cap, hsz)) return GQM_ERR_MEMORY;
+        size_t c2 = 0;
+        if (hvals) cudaFree(hvals);
+        hvals = nullptr;
+        if (grow_dev(&hvals, &c2, hsz)) return GQM_ERR_MEMORY;
+        c2 = 0;
+        if (s2ti) cudaFree(s2ti);
+        s2ti = nullptr;
+        if (grow_dev(&s2ti, &c2, hsz)) return GQM_ERR_MEMORY;
+      }
+      cudaMemsetAsync(hkeys, 0xff, sizeof(unsigned long long) * hsz, st);
       cudaMemsetAsync(s2ti, 0xff, sizeof(int) * (ns + 1), st);
-      LAUNCH(k_seg_hash_insert, ns, segs, ns, keys, vals, hsz - 1);
-      LAUNCH(k_init_subsegs, nt, M, nt, keys, vals, hsz - 1, s2ti);
+      LAUNCH(k_seg_hash_insert, ns, segs, ns, hkeys, hvals, hsz - 1);
+      LAUNCH(k_init_subsegs, nt, M, nt, hkeys, hvals, hsz - 1, s2ti);
       LAUNCH(k_pack_s2t, ns, M, s2ti, ns);
-      cudaStreamSynchronize(st);
-      cudaFree(keys);
-      cudaFree(vals);
-      cudaFree(s2ti);
     }
     last_point = np;
     last_triangle = nt;
@@ -995,36 +1065,42 @@ struct Refiner {
   int result(gqm_cdt_out *out) {
     if (!have_result) return GQM_ERR_ARGUMENT;
     memset(out, 0, sizeof(*out));
-    int np = out_np, nt = out_nt, ns = out_ns;
-    int *dtri = nullptr, *dnbr = nullptr, *dseg = nullptr;
-    uint8_t *dts = nullptr, *dps = nullptr;
-    if (dalloc(&dtri, 3L * nt) || dalloc(&dnbr, 3L * nt) || dalloc(&dseg, 2L * ns) || dalloc(&dts, nt) ||
-        dalloc(&dps, np))
-      return GQM_ERR_MEMORY;
-    LAUNCH(k_emit_output, std::max(nt, ns), M, nt, ns, dtri, dnbr, dseg, dts);
-    LAUNCH(k_emit_pstatus, np, M, np, dps);
-    out->numberofpoints = np;
-    out->numberoftriangles = nt;
-    out->numberofsegments = ns;
+    const long np = out_np, nt = out_nt, ns = out_ns;
+    // one block on the device: points | triangles | neighbours | segments |
+    // point status | triangle status, each on 16 bytes; one download into
+    // pinned memory, then copies into the caller's arrays on the host's cores
+    auto up16 = [](size_t x) { return (x + 15) & ~(size_t)15; };
+    const size_t o_tri = up16(16 * (size_t)np), o_nbr = o_tri + up16(12 * (size_t)nt),
+                 o_seg = o_nbr + up16(12 * (size_t)nt), o_ps = o_seg + up16(8 * (size_t)ns),
+                 o_ts = o_ps + up16((size_t)np), bytes = o_ts + up16((size_t)nt);
+    if (grow_dev(&d_out, &d_out_cap, bytes) || grow_pinned(bytes)) return GQM_ERR_MEMORY;
+    cudaMemcpyAsync(d_out, M.pts, 16 * (size_t)np, cudaMemcpyDeviceToDevice, st);
+    LAUNCH(k_emit_output, std::max(nt, ns), M, (int)nt, (int)ns, (int *)(d_out + o_tri), (int *)(d_out + o_nbr),
+           (int *)(d_out + o_seg), (uint8_t *)(d_out + o_ts));
+    LAUNCH(k_emit_pstatus, np, M, (int)np, (uint8_t *)(d_out + o_ps));
+    cudaMemcpyAsync(h_stage, d_out, bytes, cudaMemcpyDeviceToHost, st);
+    out->numberofpoints = (int)np;
+    out->numberoftriangles = (int)nt;
+    out->numberofsegments = (int)ns;
     out->pointlist = (double *)malloc(sizeof(double) * 2 * (size_t)np + 16);
     out->trianglelist = (int *)malloc(sizeof(int) * 3 * (size_t)nt + 16);
     out->neighborlist = (int *)malloc(sizeof(int) * 3 * (size_t)nt + 16);
     out->segmentlist = (int *)malloc(sizeof(int) * 2 * (size_t)ns + 16);
     out->pstatus = (unsigned char *)malloc((size_t)np + 16);
     out->tstatus = (unsigned char *)malloc((size_t)nt + 16);
-    cudaMemcpyAsync(out->pointlist, M.pts, sizeof(double) * 2 * (size_t)np, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(out->trianglelist, dtri, sizeof(int) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(out->neighborlist, dnbr, sizeof(int) * 3 * (size_t)nt, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(out->segmentlist, dseg, sizeof(int) * 2 * (size_t)ns, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(out->pstatus, dps, (size_t)np, cudaMemcpyDeviceToHost, st);
-    cudaMemcpyAsync(out->tstatus, dts, (size_t)nt, cudaMemcpyDeviceToHost, st);
-    cudaError_t ce = cudaStreamSynchronize(st);
-    cudaFree(dtri);
-    cudaFree(dnbr);
-    cudaFree(dseg);
-    cudaFree(dts);
-    cudaFree(dps);
-    return ce == cudaSuccess ? GQM_OK : GQM_ERR_CUDA;
+    const cudaError_t ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess || !out->pointlist || !out->trianglelist || !out->neighborlist || !out->segmentlist ||
+        !out->pstatus || !out->tstatus) {
+      for (void *q : {(void *)out->pointlist, (void *)out->trianglelist, (void *)out->neighborlist,
+                      (void *)out->segmentlist, (void *)out->pstatus, (void *)out->tstatus})
+        free(q);
+      memset(out, 0, sizeof(*out));
+      return ce != cudaSuccess ? GQM_ERR_CUDA : GQM_ERR_MEMORY;
+    }
+    host_copy({{out->pointlist, h_stage, 16 * (size_t)np}, {out->trianglelist, h_stage + o_tri, 12 * (size_t)nt},
+               {out->neighborlist, h_stage + o_nbr, 12 * (size_t)nt}, {out->segmentlist, h_stage + o_seg, 8 * (size_t)ns},
+               {out->pstatus, h_stage + o_ps, (size_t)np}, {out->tstatus, h_stage + o_ts, (size_t)nt}});
+    return GQM_OK;
   }
 };
 

@@ -187,8 +187,43 @@ def _cdt_in(cdt: CDT, keep):
                  arrs[3].shape[0], arrs[3].ctypes.data)
 
 
-def _take(out: CdtOut, with_status=False):
+class _Owner:
+    """Owns one gqm_cdt_out; releases it (gqm_free_result) when the last numpy
+    array viewing its memory is gone."""
+
+    def __init__(self, L, out: CdtOut):
+        self._L, self._out = L, out
+
+    def __del__(self):
+        try:
+            self._L.gqm_free_result(ctypes.byref(self._out))
+        except Exception:
+            pass
+
+
+def _view(owner, ptr, n, ctype, dtype):
+    if n == 0 or not ptr:
+        return np.zeros(0, dtype)
+    buf = (ctype * n).from_address(ctypes.addressof(ptr.contents))
+    buf._owner = owner  # the library's memory lives as long as the array
+    return np.frombuffer(buf, dtype=dtype)
+
+
+def _take(out: CdtOut, with_status=False, L=None):
+    """numpy arrays of a result.  With L (the library), the arrays view the
+    library's own memory and take over its release (no copy): the caller must
+    then not call gqm_free_result on `out`.  Without L they are copies."""
     np_, nt_, ns_ = out.numberofpoints, out.numberoftriangles, out.numberofsegments
+    if L is not None:
+        own = _Owner(L, out)
+        res = CDT(_view(own, out.pointlist, 2 * np_, ctypes.c_double, np.float64),
+                  _view(own, out.trianglelist, 3 * nt_, ctypes.c_int, np.int32),
+                  _view(own, out.neighborlist, 3 * nt_, ctypes.c_int, np.int32),
+                  _view(own, out.segmentlist, 2 * ns_, ctypes.c_int, np.int32))
+        if not with_status:
+            return res
+        return (res, _view(own, out.pstatus, np_, ctypes.c_ubyte, np.uint8),
+                _view(own, out.tstatus, nt_, ctypes.c_ubyte, np.uint8))
     res = CDT(np.ctypeslib.as_array(out.pointlist, shape=(2 * np_,)).copy() if np_ else np.zeros(0),
               np.ctypeslib.as_array(out.trianglelist, shape=(3 * nt_,)).copy() if nt_ else np.zeros(0, np.int32),
               np.ctypeslib.as_array(out.neighborlist, shape=(3 * nt_,)).copy() if nt_ else np.zeros(0, np.int32),
@@ -212,10 +247,7 @@ def refine(cdt: CDT, theta=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED
     rc = L.gqm_refine(ctypes.byref(cin), ctypes.byref(out), ctypes.byref(opt), ctypes.byref(st))
     if rc != 0:
         raise RefineError(rc, L.gqm_status_string(rc).decode())
-    try:
-        got = _take(out, with_status)
-    finally:
-        L.gqm_free_result(ctypes.byref(out))
+    got = _take(out, with_status, L)  # the arrays own the library's memory from here
     if with_status:
         return (*got, st.as_dict())
     return got, st.as_dict()
@@ -236,13 +268,11 @@ def refine_batch(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, predicates=P
     sts = (Stats * n)()
     bad = ctypes.c_int(-1)
     rc = L.gqm_refine_batch(n, ins, outs, opts, sts, int(workers), ctypes.byref(bad))
-    try:
-        if rc != 0:
-            raise RefineError(rc, f"domain {bad.value}: " + L.gqm_status_string(rc).decode())
-        res = [_take(outs[i]) for i in range(n)]
-    finally:
+    if rc != 0:
         for i in range(n):
             L.gqm_free_result(ctypes.byref(outs[i]))
+        raise RefineError(rc, f"domain {bad.value}: " + L.gqm_status_string(rc).decode())
+    res = [_take(outs[i], L=L) for i in range(n)]  # each result owns its domain's memory
     return res, [sts[i].as_dict() for i in range(n)]
 
 
@@ -274,13 +304,11 @@ def refine_batch_persistent(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, p
     bad = ctypes.c_int(-1)
     rc = L.gqm_refine_batch_persistent(n, ins, outs, opts, sts, ctypes.byref(bo), ctypes.byref(rep),
                                        ctypes.byref(bad))
-    try:
-        if rc != 0:
-            raise RefineError(rc, f"domain {bad.value}: " + L.gqm_status_string(rc).decode())
-        res = [_take(outs[i]) for i in range(n)]
-    finally:
+    if rc != 0:
         for i in range(n):
             L.gqm_free_result(ctypes.byref(outs[i]))
+        raise RefineError(rc, f"domain {bad.value}: " + L.gqm_status_string(rc).decode())
+    res = [_take(outs[i], L=L) for i in range(n)]  # each result owns its domain's memory
     stats = [sts[i].as_dict() for i in range(n)]
     if with_report:
         return res, stats, rep.as_dict()
