@@ -1046,6 +1046,9 @@ struct Refiner {
     FlipCtl hf;
     cudaMemcpy(&hf, fc, sizeof(hf), cudaMemcpyDeviceToHost);
     stats.flip_steps = hf.steps;
+    // each graph launch counted one kernel (its loop-entry kernel); the nine
+    // kernels of every flip step it ran are added here
+    if (use_graph) stats.kernel_launches += 9LL * hf.steps;
     for (int b = 0; b < kFlipProfileBins; ++b) {
       flip_prof_steps[b] = (long long)hf.prof_steps[b];
       flip_prof_items[b] = (long long)hf.prof_items[b];

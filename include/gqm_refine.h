@@ -94,7 +94,7 @@ typedef struct {
   long long midpoints_inserted; /* subsegment split points inserted */
   long long bad_total;          /* bad triangles summed over rounds */
   long long host_syncs;         /* device-to-host count reads */
-  long long kernel_launches;    /* kernels launched by the refinement */
+  long long kernel_launches;    /* kernels run by the refinement, those inside the flip-loop graphs included */
   long long exact_fallbacks;    /* incircle tests that needed the expansion path (single-domain
                                    path; a device-wide count, so concurrent runs on one device add up) */
   double goodcos2;              /* cos^2(theta) as evaluated on the device */
