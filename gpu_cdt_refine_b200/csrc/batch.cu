@@ -383,6 +383,7 @@ struct Cta {
     int n = compact(PNotNullFlag{S.M.tst, S.M.tflip}, Ident{}, 0, ntri, S.act);
     if (lead()) {
       fc->nact = n;
+      fc->nact_next = 0;
       fc->entry_steps = fc->steps;
       flip_next(fc);
     }
@@ -402,11 +403,13 @@ struct Cta {
       SYNC();
       k_mark_red_steiner_q(S.M, S.tl, &fc->tn, Q);
       SYNC();
-      k_flip_reset_touched(S.M, S.tl, &fc->tn, &fc->nact);
+      k_flip_reset_filter(S.M, S.tl, &fc->tn, S.fq, &fc->qn, S.act, &fc->nact_next);
       SYNC();
-      k_flip_filter(S.M, S.fq, &fc->qn, S.act, &fc->nact);
-      SYNC();
-      if (lead()) flip_next(fc);
+      if (lead()) {
+        fc->nact = fc->nact_next;
+        fc->nact_next = 0;
+        flip_next(fc);
+      }
       SYNC();
     }
     return GQM_OK;  // errors raised on the device are read by the round loop

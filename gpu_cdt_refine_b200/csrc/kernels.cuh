@@ -852,6 +852,7 @@ struct FlipCtl {
   int gen;          // generation of the stamps of the current step
   unsigned epoch;   // launch epoch of the subseg2tri stores (all kernels share it)
   int nact;         // |A|
+  int nact_next;    // |A| of the next step, counted by k_flip_reset_filter
   int winn;         // |W|
   int qn;           // length of the next queue
   int tn;           // number of claimed triangles
@@ -920,6 +921,7 @@ typedef int cudaGraphConditionalHandle;
 GQM_KERNEL void k_flip_prep(FlipCtl *c, cudaGraphConditionalHandle h, int use_graph) {
   if (GQM_BLOCK0 && threadIdx.x == 0) {
     c->entry_steps = c->steps;
+    c->nact_next = 0;
     int cond = flip_next(c);
 #ifndef GQM_HOST_EMU
     if (use_graph) cudaGraphSetConditional(h, cond);
@@ -931,6 +933,8 @@ GQM_KERNEL void k_flip_prep(FlipCtl *c, cudaGraphConditionalHandle h, int use_gr
 }
 GQM_KERNEL void k_flip_cond(FlipCtl *c, cudaGraphConditionalHandle h, int use_graph) {
   if (GQM_BLOCK0 && threadIdx.x == 0) {
+    c->nact = c->nact_next;  // the filtered queue of this step is the next step's A
+    c->nact_next = 0;
     int cond = flip_next(c);
 #ifndef GQM_HOST_EMU
     if (use_graph) cudaGraphSetConditional(h, cond);
@@ -982,6 +986,18 @@ GQM_KERNEL void k_flip_reset_touched(Mesh M, const int *tl, const int *tn, int *
   int n = *tn;
   GS_LOOP(k, n) M.tmark[tl[k]] = kMaxInt;
   if (GQM_BLOCK0 && threadIdx.x == 0) *nact = 0;
+}
+// k_flip_reset_touched and k_flip_filter in one launch: the claims of this
+// step are cleared and the next A is built (counted in *nextn, which
+// k_flip_cond moves to |A|); the two loops touch disjoint fields.
+GQM_KERNEL void k_flip_reset_filter(Mesh M, const int *tl, const int *tn, const int *q, const int *qn, int *act,
+                                    int *nextn) {
+  const int nt = *tn, nq = *qn;
+  GS_LOOP(k, nt) M.tmark[tl[k]] = kMaxInt;
+  GS_LOOP(k, nq) {
+    const int t = q[k];
+    if (M.tflip[t] && (M.tst[t] & TS_NOTNULL)) act[atomicAdd(nextn, 1)] = t;
+  }
 }
 
 // kernelCheckFlipping (refine.cu:778-1070) on A.  No flag is cleared here

@@ -608,8 +608,7 @@ struct Refiner {
     KL(k_phase2, kStepGrid, 256)(M, win, &fc->winn, ll, sl);
     KL(k_phase3q, kStepGrid, 256)(M, win, &fc->winn, sl, Q);
     KL(k_mark_red_steiner_q, kStepGrid, 256)(M, tl, &fc->tn, Q);
-    KL(k_flip_reset_touched, kStepGrid, 256)(M, tl, &fc->tn, &fc->nact);
-    KL(k_flip_filter, kStepGrid, 256)(M, fq, &fc->qn, act, &fc->nact);
+    KL(k_flip_reset_filter, kStepGrid, 256)(M, tl, &fc->tn, fq, &fc->qn, act, &fc->nact_next);
     KL(k_flip_cond, 1, 32)(fc, h, graph);
   }
   int build_flip_graph() {
@@ -721,7 +720,7 @@ struct Refiner {
       stats.host_syncs++;
       if (!hcount[C_MISC]) break;
       flip_body(h, 0);
-      stats.kernel_launches += 9;
+      stats.kernel_launches += 8;
     }
     return GQM_OK;
   }
@@ -1006,8 +1005,16 @@ struct Refiner {
     while (rc == 0) {
       LAUNCH(k_mark_bad, last_triangle, M, last_triangle);
       compact(PBad{M.tst}, Ident{}, 0, last_triangle, bad, C_LIST2);
-      int nbad = fetch(C_LIST2);
-      int derr = check_device_error();
+      // the bad count and the device error word in one round trip
+      cudaMemcpyAsync(hcount + C_LIST2, dcount + C_LIST2, sizeof(int), cudaMemcpyDeviceToHost, st);
+      cudaMemcpyAsync(hcount + C_MISC, M.err, sizeof(int), cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) {
+        rc = GQM_ERR_CUDA;
+        break;
+      }
+      stats.host_syncs++;
+      const int nbad = hcount[C_LIST2];
+      const int derr = hcount[C_MISC];
       if (derr) {
         rc = derr;
         break;
@@ -1046,9 +1053,9 @@ struct Refiner {
     FlipCtl hf;
     cudaMemcpy(&hf, fc, sizeof(hf), cudaMemcpyDeviceToHost);
     stats.flip_steps = hf.steps;
-    // each graph launch counted one kernel (its loop-entry kernel); the nine
+    // each graph launch counted one kernel (its loop-entry kernel); the eight
     // kernels of every flip step it ran are added here
-    if (use_graph) stats.kernel_launches += 9LL * hf.steps;
+    if (use_graph) stats.kernel_launches += 8LL * hf.steps;
     for (int b = 0; b < kFlipProfileBins; ++b) {
       flip_prof_steps[b] = (long long)hf.prof_steps[b];
       flip_prof_items[b] = (long long)hf.prof_items[b];
