@@ -132,7 +132,7 @@ struct Job {
   int np, nt, ns;
   int offcenter, offconstant, mode, pred, placement;
   MlpDev mlp;  // GQM_PLACE_LEARNED: the network on the device
-  double theta;
+  double theta, max_area;
   long long max_rounds;
   // outputs: each finished domain takes its space from one shared region
   // (bump allocation), so the region holds exactly the batch's results
@@ -592,6 +592,7 @@ struct Cta {
     if (lead()) {
       S.M.gc2 = sh.gc[0];
       S.M.mode = J.mode;
+      S.M.max_area = J.max_area;
       J.goodcos2 = sh.gc[0];
     }
     SYNC();
@@ -805,6 +806,7 @@ int check_domain(const gqm_cdt_in *in, const gqm_options *opt) {
   if (in->numberofsegments > 0 && !in->segmentlist) return GQM_ERR_ARGUMENT;
   if (!(opt->theta > 0.0 && opt->theta < 60.0)) return GQM_ERR_ARGUMENT;
   if (opt->placement != GQM_PLACE_PLAIN && (opt->placement != GQM_PLACE_LEARNED || !opt->mlp)) return GQM_ERR_ARGUMENT;
+  if (!(opt->max_area >= 0.0)) return GQM_ERR_ARGUMENT;
   return GQM_OK;
 }
 
@@ -898,6 +900,7 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
     J.ns = D.numberofsegments;
     const gqm_options &o = opt[d];
     J.theta = o.theta;
+    J.max_area = o.max_area > 0.0 ? o.max_area : 0.0;
     J.mode = o.mode ? 1 : 0;
     J.pred = o.predicates ? 1 : 0;
     J.max_rounds = o.max_rounds > 0 ? o.max_rounds : 1000000;

@@ -101,23 +101,40 @@ int gqm_certify(int np, const double *pts, int nt, const int *tri, const int *nb
     }
   }
   c->min_angle_deg = nt ? minang : 0.0;
-  // Euler: V - E + F = 1 for a triangulated disk (F excludes the outer face)
+  // Euler: V - E + F = 2 - L for a connected triangulated domain with L
+  // boundary loops (1 for a disk, 1 + h with h holes; F excludes the outer face)
   {
     long long E = 0, B = 0;
+    std::vector<int> parent(np > 0 ? np : 1);
+    for (int i = 0; i < np; ++i) parent[i] = i;
+    auto find = [&](int x) {
+      while (parent[x] != x) x = parent[x] = parent[parent[x]];
+      return x;
+    };
+    std::vector<char> onb(np > 0 ? np : 1, 0);
     for (int t = 0; t < nt; ++t)
       for (int i = 0; i < 3; ++i) {
-        if (nbr[3 * t + i] < 0)
+        if (nbr[3 * t + i] < 0) {
           B++;
-        else
+          const int u = tri[3 * t + (i + 1) % 3], w = tri[3 * t + (i + 2) % 3];
+          if (u >= 0 && u < np && w >= 0 && w < np) {
+            onb[u] = onb[w] = 1;
+            parent[find(u)] = find(w);
+          }
+        } else {
           E++;
+        }
       }
     E = E / 2 + B;
     std::vector<char> used(np, 0);
     for (int t = 0; t < 3 * nt; ++t)
       if (tri[t] >= 0 && tri[t] < np) used[tri[t]] = 1;
-    long long V = 0;
+    long long V = 0, L = 0;
     for (char u : used) V += u;
-    c->euler_defect = V - E + nt - 1;
+    for (int i = 0; i < np; ++i)
+      if (onb[i] && find(i) == i) L++;
+    if (L == 0) L = 1;
+    c->euler_defect = V - E + nt - (2 - L);
   }
   // input points preserved
   for (int i = 0; i < nin && i < np; ++i)

@@ -53,6 +53,7 @@ struct Mesh {
   const int2 *segs;
   int *err;  // first error code raised on the device
   double gc2;  // cos^2(theta), computed on the device as the reference does
+  double max_area;  // area bound (0: none): larger triangles are bad whatever their angles
   int mode;    // 1 Ruppert, 0 Chew
 };
 

@@ -297,6 +297,10 @@ GQM_KERNEL void k_mark_bad(Mesh M, int ntri) {
         }
       }
     }
+    // area bound (no counterpart in the reference; Triangle's `a` switch)
+    if (!bad && M.max_area > 0.0 &&
+        0.5 * fabs((b.x - a.x) * (c.y - a.y) - (b.y - a.y) * (c.x - a.x)) > M.max_area)
+      bad = true;
     M.tst[t] = bad ? (uint8_t)(st | TS_BAD) : (uint8_t)(st & ~TS_BAD);
   }
 }

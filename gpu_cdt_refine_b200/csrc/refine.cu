@@ -970,6 +970,7 @@ struct Refiner {
     cudaStreamSynchronize(st);
     M.gc2 = hgc[0];
     M.mode = mode;
+    M.max_area = opt->max_area > 0.0 ? opt->max_area : 0.0;
     stats.goodcos2 = hgc[0];
     LAUNCH(k_init_points, pphys, M, (const double2 *)dpts, np, (int)pphys);
     LAUNCH(k_init_tris, tphys, M, dtri_in, dnbr_in, nt, (int)tphys);
@@ -1131,6 +1132,7 @@ void gqm_default_options(gqm_options *o) {
   o->max_rounds = 0;
   o->placement = GQM_PLACE_PLAIN;
   o->mlp = nullptr;
+  o->max_area = 0.0;
 }
 
 static int validate(const gqm_cdt_in *in, const gqm_options *opt) {
@@ -1140,6 +1142,7 @@ static int validate(const gqm_cdt_in *in, const gqm_options *opt) {
   if (in->numberofsegments > 0 && !in->segmentlist) return GQM_ERR_ARGUMENT;
   if (!(opt->theta > 0.0 && opt->theta < 60.0)) return GQM_ERR_ARGUMENT;
   if (opt->placement != GQM_PLACE_PLAIN && (opt->placement != GQM_PLACE_LEARNED || !opt->mlp)) return GQM_ERR_ARGUMENT;
+  if (!(opt->max_area >= 0.0)) return GQM_ERR_ARGUMENT;
   return GQM_OK;
 }
 

@@ -137,3 +137,72 @@ def batch_domains(count: int = 4096, seed: int = 20261207, nmin: int = 200, nmax
     with ThreadPoolExecutor(nthreads) as ex:
         res = list(ex.map(lambda k: batch_domain(seed + 2 * k, nmin, nmax), range(count)))
     return [r[0] for r in res], [r[1] for r in res]
+
+
+def remove_holes(cdt: CDT, holes) -> CDT:
+    """The CDT with every triangle reachable from a hole point without crossing
+    a segment removed (Triangle's holes; the reference ignores holes), and with
+    the vertices and segments that no remaining triangle uses dropped and the
+    rest renumbered.  Hole boundaries must be segments; the result is a valid
+    input of the refiner (every boundary edge a segment)."""
+    from scipy.sparse import coo_matrix
+    from scipy.sparse.csgraph import connected_components
+
+    tri, nbr, seg, pts = cdt.trianglelist, cdt.neighborlist, cdt.segmentlist, cdt.pointlist
+    nt, npt = tri.shape[0], pts.shape[0]
+    if nt == 0 or len(holes) == 0:
+        return cdt
+    # edge j of a triangle joins vertices j+1 and j+2; covered edges are segments
+    a = tri[:, [1, 2, 0]].astype(np.int64)
+    b = tri[:, [2, 0, 1]].astype(np.int64)
+    ekey = np.minimum(a, b) * npt + np.maximum(a, b)
+    sg = seg.astype(np.int64)
+    skey = np.minimum(sg[:, 0], sg[:, 1]) * npt + np.maximum(sg[:, 0], sg[:, 1])
+    covered = np.isin(ekey, skey)
+    t_idx = np.repeat(np.arange(nt), 3).reshape(nt, 3)
+    link = (nbr >= 0) & ~covered
+    g = coo_matrix((np.ones(int(link.sum()), np.int8), (t_idx[link], nbr[link])), shape=(nt, nt))
+    _, comp = connected_components(g, directed=False)
+    # the triangle that contains each hole point
+    p0, p1, p2 = pts[tri[:, 0]], pts[tri[:, 1]], pts[tri[:, 2]]
+    drop = np.zeros(comp.max() + 1, bool)
+    for hx, hy in np.asarray(holes, np.float64).reshape(-1, 2):
+        def side(u, v):
+            return (v[:, 0] - u[:, 0]) * (hy - u[:, 1]) - (v[:, 1] - u[:, 1]) * (hx - u[:, 0])
+        inside = np.nonzero((side(p0, p1) >= 0) & (side(p1, p2) >= 0) & (side(p2, p0) >= 0))[0]
+        if inside.size:
+            drop[comp[inside[0]]] = True
+    keep = ~drop[comp]
+    newt = -np.ones(nt, np.int64)
+    newt[keep] = np.arange(int(keep.sum()))
+    tri2, nbr2 = tri[keep], nbr[keep]
+    nbr2 = np.where(nbr2 >= 0, newt[np.maximum(nbr2, 0)], -1)
+    used = np.zeros(npt, bool)
+    used[tri2.ravel()] = True
+    newp = -np.ones(npt, np.int64)
+    newp[used] = np.arange(int(used.sum()))
+    # segments still on an edge of a remaining triangle
+    kept_edges = ekey[keep].ravel()
+    seg2 = seg[np.isin(skey, kept_edges)]
+    return CDT(pts[used], newp[tri2].astype(np.int32), nbr2.astype(np.int32), newp[seg2].astype(np.int32))
+
+
+def square_with_hole(seed: int = 20261210, n: int = 4000, hole=(0.35, 0.65)) -> CDT:
+    """A domain with a hole: n uniform points in the unit square outside the
+    square hole [hole[0], hole[1]]^2, the hole's boundary as four segments
+    (with points along them), the CDT built and the hole removed."""
+    rng = np.random.default_rng(seed)
+    lo, hi = hole
+    p = rng.uniform(0.0, 1.0, (2 * n, 2))
+    p = p[~((p[:, 0] > lo - 0.01) & (p[:, 0] < hi + 0.01) & (p[:, 1] > lo - 0.01) & (p[:, 1] < hi + 0.01))][:n]
+    k = 16
+    t = np.linspace(lo, hi, k + 1)[:-1]
+    ring = np.concatenate([np.stack([t, np.full(k, lo)], 1), np.stack([np.full(k, hi), t], 1),
+                           np.stack([t[::-1] + (hi - lo) / k, np.full(k, hi)], 1),
+                           np.stack([np.full(k, lo), t[::-1] + (hi - lo) / k], 1)])
+    pts = np.concatenate([p, ring])
+    r0 = p.shape[0]
+    m = ring.shape[0]
+    seg = np.stack([r0 + np.arange(m), r0 + (np.arange(m) + 1) % m], 1).astype(np.int32)
+    cdt = build_cdt(pts, seg)
+    return remove_holes(cdt, [(0.5 * (lo + hi), 0.5 * (lo + hi))])

@@ -39,7 +39,7 @@ class CdtOut(ctypes.Structure):
 class Options(ctypes.Structure):
     _fields_ = [("theta", ctypes.c_double), ("insert_policy", ctypes.c_int), ("mode", ctypes.c_int),
                 ("predicates", ctypes.c_int), ("device", ctypes.c_int), ("max_rounds", ctypes.c_longlong),
-                ("placement", ctypes.c_int), ("mlp", ctypes.c_void_p)]
+                ("placement", ctypes.c_int), ("mlp", ctypes.c_void_p), ("max_area", ctypes.c_double)]
 
 
 class Stats(ctypes.Structure):
@@ -159,7 +159,7 @@ MLP_FEATURES, MLP_PARAMS = 32, 6337
 
 
 def make_options(theta=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0,
-                 max_rounds=0, mlp=None) -> Options:
+                 max_rounds=0, mlp=None, max_area=0.0) -> Options:
     """Options of one refinement.  mlp: a float32 array of MLP_PARAMS network
     parameters selects the learned Steiner placement (the caller keeps the
     array alive while the options are in use)."""
@@ -171,6 +171,7 @@ def make_options(theta=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REF
     o.predicates = int(predicates)
     o.device = int(device)
     o.max_rounds = int(max_rounds)
+    o.max_area = float(max_area)
     if mlp is not None:
         if mlp.dtype != np.float32 or mlp.shape != (MLP_PARAMS,) or not mlp.flags.c_contiguous:
             raise ValueError("mlp must be a contiguous float32 array of MLP_PARAMS values")
@@ -236,14 +237,15 @@ def _take(out: CdtOut, with_status=False, L=None):
 
 
 def refine(cdt: CDT, theta=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0,
-           max_rounds=0, with_status=False, mlp=None):
-    """Refine a CDT on the GPU; returns (CDT, stats dict) or (CDT, ps, ts, stats)."""
+           max_rounds=0, with_status=False, mlp=None, max_area=0.0):
+    """Refine a CDT on the GPU; returns (CDT, stats dict) or (CDT, ps, ts, stats).
+    max_area > 0 also refines every triangle larger than max_area."""
     L = lib()
     keep = []
     cin = _cdt_in(cdt, keep)
     out = CdtOut()
     st = Stats()
-    opt = make_options(theta, insertpolicy, mode, predicates, device, max_rounds, mlp)
+    opt = make_options(theta, insertpolicy, mode, predicates, device, max_rounds, mlp, max_area)
     rc = L.gqm_refine(ctypes.byref(cin), ctypes.byref(out), ctypes.byref(opt), ctypes.byref(st))
     if rc != 0:
         raise RefineError(rc, L.gqm_status_string(rc).decode())
@@ -276,27 +278,28 @@ def refine_batch(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, predicates=P
     return res, [sts[i].as_dict() for i in range(n)]
 
 
-def _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds, keep, mlp=None):
+def _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds, keep, mlp=None, max_area=0.0):
     n = len(cdts)
     if np.isscalar(thetas):
         thetas = [float(thetas)] * n
     if np.isscalar(predicates):
         predicates = [int(predicates)] * n
     ins = (CdtIn * n)(*[_cdt_in(c, keep) for c in cdts])
-    opts = (Options * n)(*[make_options(t, insertpolicy, mode, p, device, max_rounds, mlp)
+    opts = (Options * n)(*[make_options(t, insertpolicy, mode, p, device, max_rounds, mlp, max_area)
                            for t, p in zip(thetas, predicates)])
     return ins, opts
 
 
 def refine_batch_persistent(cdts, thetas=20.0, insertpolicy=Offcenter, mode=1, predicates=PRED_REFERENCE, device=0,
-                            threads_per_block=0, blocks_per_sm=0, max_rounds=0, with_report=False, mlp=None):
+                            threads_per_block=0, blocks_per_sm=0, max_rounds=0, with_report=False, mlp=None,
+                            max_area=0.0):
     """Refine independent CDTs in one persistent launch
     (gqm_refine_batch_persistent); returns (list of CDT, list of stats dicts)
     and, with with_report, the call's report as a third item."""
     L = lib()
     n = len(cdts)
     keep = []
-    ins, opts = _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds, keep, mlp)
+    ins, opts = _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds, keep, mlp, max_area)
     outs = (CdtOut * n)()
     sts = (Stats * n)()
     bo = BatchOptions(int(threads_per_block), int(blocks_per_sm), 0.0)

@@ -85,6 +85,8 @@ typedef struct {
   long long max_rounds; /* bound on every refinement loop; 0 = default (1e6) */
   int placement;        /* GQM_PLACE_PLAIN (the reference's rule) / GQM_PLACE_LEARNED */
   const float *mlp;     /* GQM_PLACE_LEARNED: host array of GQM_MLP_PARAMS network parameters */
+  double max_area;      /* area bound (no counterpart in the reference; Triangle's `a` switch):
+                           triangles larger than this are refined whatever their angles; 0 = none */
 } gqm_options;
 
 typedef struct {

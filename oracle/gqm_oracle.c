@@ -406,6 +406,7 @@ typedef struct {
   int nempty_p, nempty_t;
   IV emptyp, emptyt;
   double theta, gc2;
+  double max_area;  /* area bound (0: none), the counterpart of Triangle's `a` switch */
   int mode;
   long long max_rounds;
   int err;
@@ -1576,9 +1577,23 @@ static void split_encsegs(St *S) {
 }
 
 /* ---------------- bad triangles (refine.cu:376-570) ---------------- */
+/* twice the area of triangle (a, b, c), as the CUDA kernels compute it */
+static double area2(P2 a, P2 b, P2 c) { return fabs((b.x - a.x) * (c.y - a.y) - (b.y - a.y) * (c.x - a.x)); }
+
+/* kernelMarkBadTriangles with an optional area bound (no counterpart in the
+ * reference): a triangle larger than max_area is bad whatever its angles. */
+static void mark_bad_angle(St *S, int index);
 static void mark_bad(St *S, int index) {
   unsigned char *ts = &S->ts[index];
   if (!(*ts & TS_CHECK)) return;
+  mark_bad_angle(S, index);
+  if (S->max_area > 0.0 && !(*ts & TS_BAD)) {
+    const int *p = &S->tri[3 * index];
+    if (0.5 * area2(S->pts[p[0]], S->pts[p[1]], S->pts[p[2]]) > S->max_area) ts_set(ts, TS_BAD, 1);
+  }
+}
+static void mark_bad_angle(St *S, int index) {
+  unsigned char *ts = &S->ts[index];
   ts_set(ts, TS_CHECK, 0);
   ts_set(ts, TS_NOTNULL, 1);
   int p[3] = {S->tri[3 * index], S->tri[3 * index + 1], S->tri[3 * index + 2]};
@@ -2139,6 +2154,9 @@ int gqm_oracle_refine(int np, const double *pts, int nt, const int *tri, const i
   return gqm_oracle_refine_gc(np, pts, nt, tri, nbr, ns, segs, theta, 0.0, policy, mode, max_rounds, out);
 }
 
+static double g_max_area = 0.0;
+void gqm_oracle_set_max_area(double a) { g_max_area = a > 0.0 ? a : 0.0; }
+
 int gqm_oracle_refine_gc(int np, const double *pts, int nt, const int *tri, const int *nbr, int ns,
                          const int *segs, double theta, double goodcos2, int policy, int mode, long long max_rounds,
                          gqm_oracle_out *out) {
@@ -2146,6 +2164,7 @@ int gqm_oracle_refine_gc(int np, const double *pts, int nt, const int *tri, cons
   St Sv;
   St *S = &Sv;
   memset(S, 0, sizeof(*S));
+  S->max_area = g_max_area;
   S->theta = theta;
   S->mode = mode;
   S->max_rounds = max_rounds;

@@ -43,6 +43,10 @@ int gqm_oracle_refine_gc(int np, const double *pts, int nt, const int *tri, cons
                          gqm_oracle_out *out);
 void gqm_oracle_free(gqm_oracle_out *out);
 
+/* Area bound of the following refinements (0: none): a triangle larger than
+ * `a` is refined whatever its angles (Triangle's `a` switch). */
+void gqm_oracle_set_max_area(double a);
+
 /* Debugging aid: write one digest line per flip step to `path` (NULL: off). */
 void gqm_oracle_trace(const char *path);
 void gqm_oracle_trace_dump(long step, const char *path);

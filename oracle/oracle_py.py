@@ -47,6 +47,7 @@ def lib():
                                            ctypes.POINTER(OracleOut)]
         L.gqm_oracle_refine_gc.restype = ctypes.c_int
         L.gqm_oracle_free.argtypes = [ctypes.POINTER(OracleOut)]
+        L.gqm_oracle_set_max_area.argtypes = [ctypes.c_double]
         for f in ("gqm_oracle_orient",):
             getattr(L, f).argtypes = [dp, dp, dp]
             getattr(L, f).restype = ctypes.c_double
@@ -58,7 +59,7 @@ def lib():
     return _lib
 
 
-def refine(cdt, theta=20.0, policy=1, mode=1, max_rounds=100000, goodcos2=None):
+def refine(cdt, theta=20.0, policy=1, mode=1, max_rounds=100000, goodcos2=None, max_area=0.0):
     """Run the oracle on a CDT; returns (CDT, info dict).  goodcos2: cos^2(theta)
     as the device evaluates it (None: the host's cos())."""
     from gpu_cdt_refine_b200.cdtio import CDT
@@ -69,10 +70,14 @@ def refine(cdt, theta=20.0, policy=1, mode=1, max_rounds=100000, goodcos2=None):
     n = np.ascontiguousarray(cdt.neighborlist, np.int32)
     s = np.ascontiguousarray(cdt.segmentlist, np.int32)
     ip = ctypes.POINTER(ctypes.c_int)
-    rc = L.gqm_oracle_refine_gc(p.shape[0], p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), t.shape[0],
-                                t.ctypes.data_as(ip), n.ctypes.data_as(ip), s.shape[0], s.ctypes.data_as(ip),
-                                float(theta), float(goodcos2 or 0.0), int(policy), int(mode), int(max_rounds),
-                                ctypes.byref(out))
+    L.gqm_oracle_set_max_area(float(max_area))
+    try:
+        rc = L.gqm_oracle_refine_gc(p.shape[0], p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), t.shape[0],
+                                    t.ctypes.data_as(ip), n.ctypes.data_as(ip), s.shape[0], s.ctypes.data_as(ip),
+                                    float(theta), float(goodcos2 or 0.0), int(policy), int(mode), int(max_rounds),
+                                    ctypes.byref(out))
+    finally:
+        L.gqm_oracle_set_max_area(0.0)
     info = dict(status=rc, rounds=out.rounds, flip_steps=out.flip_steps, steiner=out.steiner_inserted,
                 midpoints=out.midpoints_inserted, bad_total=out.bad_total)
     if rc != 0:

@@ -88,3 +88,18 @@ def test_duplicate_points_rejected():
     pts = np.array([[0, 0], [1, 0], [0, 1], [1, 0]], float)
     with pytest.raises(ValueError):
         inputs.build_cdt(pts, np.zeros((0, 2), np.int32))
+
+
+def test_remove_holes_leaves_a_valid_cdt():
+    """Hole removal: the triangles inside the hole are gone, every boundary
+    edge is a segment, neighbours stay symmetric, and the mesh is a
+    constrained Delaunay triangulation with one hole (certificate)."""
+    from gpu_cdt_refine_b200.certify import certify
+    c = inputs.square_with_hole(n=3000)
+    cen = c.pointlist[c.trianglelist].mean(axis=1)
+    assert not np.any((cen[:, 0] > 0.35) & (cen[:, 0] < 0.65) & (cen[:, 1] > 0.35) & (cen[:, 1] < 0.65))
+    cert = certify(c, c, 1e-3)
+    assert cert["ok"], cert
+    # without holes the function returns the CDT unchanged
+    d = inputs.plain_small(seed=9, n=300, nseg=10)
+    assert inputs.remove_holes(d, []) is d

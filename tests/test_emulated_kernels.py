@@ -181,3 +181,31 @@ def test_emulated_learn_collect(emulated):
     assert feat.shape == (st["learned_candidates"], refine.MLP_FEATURES)
     assert np.isfinite(feat).all() and np.all(feat[:, -1] == 1.0)
     assert np.all((tgt >= 0) & (tgt <= 1)) and np.allclose(tgt * 8, np.round(tgt * 8))
+
+
+def test_emulated_area_bound_matches_oracle(emulated):
+    """With an area bound (no counterpart in the reference; Triangle's `a`
+    switch) the kernels still agree with the oracle byte for byte."""
+    cdt = inputs.plain_small(seed=351, n=1500, nseg=60)
+    for area in (400.0, 2000.0):
+        got, st = refine.refine(cdt, 20.0, max_area=area)
+        want, info = oracle_py.refine(cdt, 20.0, 1, 1, max_area=area)
+        _same(got, want)
+        tri = got.pointlist[got.trianglelist]
+        a = 0.5 * np.abs((tri[:, 1, 0] - tri[:, 0, 0]) * (tri[:, 2, 1] - tri[:, 0, 1]) -
+                         (tri[:, 1, 1] - tri[:, 0, 1]) * (tri[:, 2, 0] - tri[:, 0, 0]))
+        assert a.max() <= area
+
+
+def test_emulated_domain_with_hole(emulated):
+    """A domain with a hole (its boundary four chains of segments) refines to
+    the oracle's mesh; no triangle enters the hole."""
+    from gpu_cdt_refine_b200.certify import certify
+    cdt = inputs.square_with_hole(n=1500)
+    got, _ = refine.refine(cdt, 20.0)
+    want, _ = oracle_py.refine(cdt, 20.0, 1, 1)
+    _same(got, want)
+    cen = got.pointlist[got.trianglelist].mean(axis=1)
+    assert not np.any((cen[:, 0] > 0.35) & (cen[:, 0] < 0.65) & (cen[:, 1] > 0.35) & (cen[:, 1] < 0.65))
+    cert = certify(got, cdt, 20.0)
+    assert cert["ok"] and cert["triangles_below_theta"] == 0, cert

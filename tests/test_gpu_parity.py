@@ -91,3 +91,28 @@ def test_round_limit_returns_status(gpu, small_inputs):
     with pytest.raises(refine.RefineError) as e:
         refine.refine(small_inputs["u2k"], 20.0, max_rounds=1)
     assert e.value.status == -2
+
+
+@pytest.mark.parametrize("area", [50.0, 400.0])
+def test_area_bound_matches_oracle(gpu, area):
+    """Area bound (Triangle's `a` switch; no counterpart in the reference):
+    CUDA path == oracle byte for byte, every triangle within the bound."""
+    cdt = inputs.plain_small(seed=361, n=5000, nseg=200)
+    got, _ = refine.refine(cdt, 20.0, max_area=area)
+    want, _ = oracle_py.refine(cdt, 20.0, 1, 1, max_area=area)
+    assert_same(got, want)
+    t = got.pointlist[got.trianglelist]
+    a = 0.5 * np.abs((t[:, 1, 0] - t[:, 0, 0]) * (t[:, 2, 1] - t[:, 0, 1]) -
+                     (t[:, 1, 1] - t[:, 0, 1]) * (t[:, 2, 0] - t[:, 0, 0]))
+    assert a.max() <= area
+    gb, _ = refine.refine_batch_persistent([cdt], 20.0, max_area=area)
+    assert_same(gb[0], got)
+
+
+def test_domain_with_hole_matches_oracle(gpu):
+    cdt = inputs.square_with_hole(n=8000)
+    got, _ = refine.refine(cdt, 20.0)
+    want, _ = oracle_py.refine(cdt, 20.0, 1, 1)
+    assert_same(got, want)
+    cert = certify(got, cdt, 20.0)
+    assert cert["ok"] and cert["triangles_below_theta"] == 0, cert
