@@ -127,18 +127,35 @@ __device__ __forceinline__ int win_rank(const Mesh &M, int index) {
     if ((c << 5) + j < w) b += __popc(M.wbits[(c << 5) + j]);
   return r + b + __popc(M.wbits[w] & ((1u << (index & 31)) - 1u));
 }
-// enter / leave the winner bitmap and its counts
-__device__ __forceinline__ void win_mark(const Mesh &M, int index) {
-  atomicOr(M.wbits + (index >> 5), 1u << (index & 31));
-  atomicAdd(M.wcnt + (index >> 10), 1);
-  atomicAdd(M.wsup + (index >> 15), 1);
-  atomicAdd(M.wmeg + (index >> 20), 1);
+// enter / leave the winner bitmap and its counts.  The two coarse counts
+// (2^15 and 2^20 slots) are few and hot, so the lanes of a warp that hit the
+// same one add together (one atomic per distinct counter); `on` says whether
+// this lane takes part (every lane of the warp must call).
+__device__ __forceinline__ void win_count(int *a, int idx, bool on, int d) {
+#ifdef GQM_HOST_EMU
+  if (on) atomicAdd(a + idx, d);
+#else
+  const unsigned act = __ballot_sync(0xffffffffu, on);
+  if (!on) return;
+  const unsigned same = __match_any_sync(act, idx);
+  if ((int)(threadIdx.x & 31u) == __ffs(same) - 1) atomicAdd(a + idx, d * __popc(same));
+#endif
 }
-__device__ __forceinline__ void win_unmark(const Mesh &M, int index) {
-  atomicAnd(M.wbits + (index >> 5), ~(1u << (index & 31)));
-  atomicAdd(M.wcnt + (index >> 10), -1);
-  atomicAdd(M.wsup + (index >> 15), -1);
-  atomicAdd(M.wmeg + (index >> 20), -1);
+__device__ __forceinline__ void win_mark(const Mesh &M, int index, bool on) {
+  if (on) {
+    atomicOr(M.wbits + (index >> 5), 1u << (index & 31));
+    atomicAdd(M.wcnt + (index >> 10), 1);
+  }
+  win_count(M.wsup, on ? index >> 15 : -1, on, 1);
+  win_count(M.wmeg, on ? index >> 20 : -1, on, 1);
+}
+__device__ __forceinline__ void win_unmark(const Mesh &M, int index, bool on) {
+  if (on) {
+    atomicAnd(M.wbits + (index >> 5), ~(1u << (index & 31)));
+    atomicAdd(M.wcnt + (index >> 10), -1);
+  }
+  win_count(M.wsup, on ? index >> 15 : -1, on, -1);
+  win_count(M.wmeg, on ? index >> 20 : -1, on, -1);
 }
 
 __device__ __forceinline__ void raise_err(const Mesh &M, int code) { atomicCAS(M.err, 0, code); }

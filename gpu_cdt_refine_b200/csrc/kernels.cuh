@@ -1144,51 +1144,57 @@ GQM_KERNEL void GQM_WALK_BOUNDS k_check_flip2(Mesh M, const int *act, const int 
 
 // kernelMarkFlipWinner (refine.cu:1072-1170) on A; applies the deferred flag
 // clears, re-queues the triangles that keep their flag, collects winners.
+// Winner test of one entry of A (the body of kernelMarkFlipWinner); true when
+// the triangle's flip won all the triangles it needs.
+__device__ __forceinline__ bool flip_winner(const Mesh &M, const FlipQ &Q, int index, uint8_t clear) {
+  if (clear) {
+    M.tflip[index] = 0;
+    return false;
+  }
+  push_flag(M, Q, index);
+  int ori = M.tfo[index];
+  if (ori == 15) return false;
+  bool w = false;
+  if (M.tmark[index] == index) {
+    if (ori < 3) {
+      int pOppTri = dtri(ld1(M.tn, index, m3(ori + 1)));
+      w = (M.tmark[pOppTri] == index);
+    } else if (ori < 6) {
+      int o = m3(ori - 3 + 1);
+      int t1 = dtri(ld1(M.tn, index, o)), t2 = dtri(ld1(M.tn, index, m3(o + 2)));
+      w = (t1 < 0 || M.tmark[t1] == index) && (t2 < 0 || M.tmark[t2] == index);
+    } else {
+      int o = ori - 6;
+      int pOpp = ld1(M.tn, index, o);
+      int pOppTri = dtri(pOpp), pOppOri = dori(pOpp);
+      int pOrg = ld1(M.tv, index, m3(o + 1)), pDest = ld1(M.tv, index, m3(o + 2));
+      int t1, t2;
+      if (is_red(M, pOrg) && (!is_red(M, pDest) || pOrg < pDest)) {
+        t1 = ld1(M.tn, index, m3(o + 2));
+        t2 = ld1(M.tn, pOppTri, m3(pOppOri + 1));
+      } else {
+        t1 = ld1(M.tn, index, m3(o + 1));
+        t2 = ld1(M.tn, pOppTri, m3(pOppOri + 2));
+      }
+      t1 = dtri(t1);
+      t2 = dtri(t2);
+      w = (M.tmark[pOppTri] == index && M.tmark[t1] == index && M.tmark[t2] == index);
+    }
+  }
+  if (!w) M.tfo[index] = 15;
+  return w;
+}
+// The loop keeps whole warps together (the winner counts are added per warp).
 GQM_KERNEL void k_flip_winner2(Mesh M, const int *act, const int *dn, const uint8_t *clr, FlipQ Q, int *win,
                                int *winn) {
-  int n = *dn;
-  GS_LOOP(k, n) {
-    int index = act[k];
-    if (clr[k]) {
-      M.tflip[index] = 0;
-      continue;
-    }
-    push_flag(M, Q, index);
-    int ori = M.tfo[index];
-    if (ori == 15) continue;
-    bool w = false;
-    if (M.tmark[index] == index) {
-      if (ori < 3) {
-        int pOppTri = dtri(ld1(M.tn, index, m3(ori + 1)));
-        w = (M.tmark[pOppTri] == index);
-      } else if (ori < 6) {
-        int o = m3(ori - 3 + 1);
-        int t1 = dtri(ld1(M.tn, index, o)), t2 = dtri(ld1(M.tn, index, m3(o + 2)));
-        w = (t1 < 0 || M.tmark[t1] == index) && (t2 < 0 || M.tmark[t2] == index);
-      } else {
-        int o = ori - 6;
-        int pOpp = ld1(M.tn, index, o);
-        int pOppTri = dtri(pOpp), pOppOri = dori(pOpp);
-        int pOrg = ld1(M.tv, index, m3(o + 1)), pDest = ld1(M.tv, index, m3(o + 2));
-        int t1, t2;
-        if (is_red(M, pOrg) && (!is_red(M, pDest) || pOrg < pDest)) {
-          t1 = ld1(M.tn, index, m3(o + 2));
-          t2 = ld1(M.tn, pOppTri, m3(pOppOri + 1));
-        } else {
-          t1 = ld1(M.tn, index, m3(o + 1));
-          t2 = ld1(M.tn, pOppTri, m3(pOppOri + 2));
-        }
-        t1 = dtri(t1);
-        t2 = dtri(t2);
-        w = (M.tmark[pOppTri] == index && M.tmark[t1] == index && M.tmark[t2] == index);
-      }
-    }
-    if (w) {
-      win[atomicAdd(winn, 1)] = index;
-      win_mark(M, index);
-    } else {
-      M.tfo[index] = 15;
-    }
+  const int n = *dn;
+  const int lane = (int)(threadIdx.x & 31u);
+  for (int base = GQM_GTID - lane; base < n; base += GQM_GSIZE) {
+    const int k = base + lane;
+    const int index = k < n ? act[k] : -1;
+    const bool w = k < n && flip_winner(M, Q, index, clr[k]);
+    if (w) win[atomicAdd(winn, 1)] = index;
+    win_mark(M, index, w);
   }
 }
 
@@ -1220,10 +1226,12 @@ struct QueueFlag {
 GQM_KERNEL void k_phase3q(Mesh M, const int *win, const int *dn, const int *sl, FlipQ Q) {
   int n = *dn;
   QueueFlag f{&M, &Q};
-  GS_LOOP(pos, n) {
-    const int index = win[pos];
-    phase3_body(M, pos, index, sl, f);
-    win_unmark(M, index);  // phase 1 has read the bitmap
+  const int lane = (int)(threadIdx.x & 31u);
+  for (int base = GQM_GTID - lane; base < n; base += GQM_GSIZE) {  // whole warps (see win_unmark)
+    const int pos = base + lane;
+    const int index = pos < n ? win[pos] : -1;
+    if (pos < n) phase3_body(M, pos, index, sl, f);
+    win_unmark(M, index, pos < n);  // phase 1 has read the bitmap
   }
 }
 

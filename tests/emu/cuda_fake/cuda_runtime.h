@@ -115,6 +115,7 @@ inline int __popc(unsigned v) { return __builtin_popcount(v); }
 inline int __shfl_up_sync(unsigned, int v, int) { return v; }
 inline int __shfl_sync(unsigned, int v, int) { return v; }
 inline int __ffs(unsigned v) { return __builtin_ffs(v); }
+inline unsigned __match_any_sync(unsigned, int) { return 1u; }
 inline int __clz(int v) { return v == 0 ? 32 : __builtin_clz((unsigned)v); }
 
 typedef int cudaError_t;
