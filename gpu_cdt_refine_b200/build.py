@@ -4,7 +4,8 @@
 
 libgqm_b200.so : refine.cu (kernels, driver, C ABI) + batch.cu (persistent
                  batched engine) + learned.cu (placement network training and
-                 inference) + legacy.cpp (C++ drop-in)
+                 inference) + cdt_gpu.cu (CDT construction on the GPU) +
+                 legacy.cpp (C++ drop-in)
 libgqm_host.so : cdt_build.cpp + synth.cpp + certify.cpp
 
 Every floating-point operation of the refiner is rounded on its own:
@@ -39,7 +40,7 @@ def _stale(out, srcs):
 def build_host(force=False):
     out = os.path.join(HERE, "libgqm_host.so")
     srcs = [os.path.join(CSRC, f) for f in ("cdt_build.cpp", "synth.cpp", "certify.cpp")]
-    deps = srcs + [os.path.join(CSRC, "predicates.h")]
+    deps = srcs + [os.path.join(CSRC, "predicates.h"), os.path.join(INC, "gqm_cdt.h")]
     if force or _stale(out, deps):
         _run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-ffp-contract=off", "-I" + INC, "-o", out] + srcs)
     return out
@@ -47,26 +48,34 @@ def build_host(force=False):
 
 def build_cuda(force=False, extra=None):
     out = os.path.join(HERE, "libgqm_b200.so")
-    srcs = [os.path.join(CSRC, f) for f in ("refine.cu", "batch.cu", "learned.cu", "legacy.cpp")]
-    deps = srcs + [os.path.join(CSRC, f) for f in ("kernels.cuh", "gqm_device.cuh", "predicates.h", "learned.cuh")] + [
-        os.path.join(INC, "gqm_refine.h"), os.path.join(INC, "gqm_triangulateio.h")]
-    if not (force or _stale(out, deps)):
-        return out
+    hdr = [os.path.join(INC, "gqm_refine.h"), os.path.join(INC, "gqm_triangulateio.h"),
+           os.path.join(CSRC, "predicates.h")]
+    refiner = [os.path.join(CSRC, f) for f in ("kernels.cuh", "gqm_device.cuh", "learned.cuh")]
+    units = {  # translation unit -> the headers it includes
+        "refine.cu": hdr + refiner,
+        "batch.cu": hdr + refiner,
+        "learned.cu": hdr + [os.path.join(CSRC, "learned.cuh")],
+        "cdt_gpu.cu": [os.path.join(INC, "gqm_cdt.h"), os.path.join(CSRC, "predicates.h")],
+        "legacy.cpp": hdr,
+    }
     flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler",
                     "-ffp-contract=off", "-I" + INC] + list(extra or [])
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    # the translation units compile in parallel, then one link
+    # stale translation units compile in parallel, then one link
     procs, objs = [], []
-    for src in srcs:
-        obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = [NVCC] + flags + ["-c", src, "-o", obj]
-        print(" ".join(cmd), flush=True)
-        procs.append(subprocess.Popen(cmd))
+    for name, deps in units.items():
+        src = os.path.join(CSRC, name)
+        obj = os.path.join(objdir, name + ".o")
         objs.append(obj)
+        if force or extra or _stale(obj, [src] + deps):
+            cmd = [NVCC] + flags + ["-c", src, "-o", obj]
+            print(" ".join(cmd), flush=True)
+            procs.append(subprocess.Popen(cmd))
     if any(p.wait() != 0 for p in procs):
         raise RuntimeError("nvcc failed")
-    _run([NVCC] + ARCH + ["-shared", "-o", out] + objs)
+    if procs or _stale(out, objs):
+        _run([NVCC] + ARCH + ["-shared", "-o", out] + objs)
     return out
 
 

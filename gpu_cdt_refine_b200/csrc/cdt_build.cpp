@@ -26,6 +26,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "gqm_cdt.h"
 #include "predicates.h"
 
 namespace {
@@ -421,11 +422,6 @@ struct Builder {
 }  // namespace
 
 extern "C" {
-
-struct gqm_cdt_result {
-  int numberofpoints, numberoftriangles, numberofsegments, status;
-  int *trianglelist, *neighborlist, *segmentlist;
-};
 
 // Constrained Delaunay triangulation with the convex hull enclosed by
 // segments (the contract of Triangle's "pzQnc", GPU_Refine/mesh.cpp:397).
