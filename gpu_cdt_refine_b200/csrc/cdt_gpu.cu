@@ -40,6 +40,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #ifndef GQM_HOST_EMU
@@ -47,6 +48,7 @@
 #endif
 
 #include "gqm_cdt.h"
+#include "host_copy.h"
 #include "predicates.h"
 
 namespace gqm_cdt {
@@ -1183,6 +1185,9 @@ struct Builder {
     free_all();
     if (hc) cudaFreeHost(hc);
     hc = nullptr;
+    if (stage) cudaFreeHost(stage);
+    stage = nullptr;
+    stage_cap = 0;
     if (st) cudaStreamDestroy(st);
     st = nullptr;
     dev = -1;
@@ -1202,7 +1207,7 @@ struct Builder {
     rc |= dalloc(&ptype, n) | dalloc(&D, T) | dalloc(&D2, T) | dalloc(&C, 3 * T) | dalloc(&wf, std::max(3 * T, s));
     rc |= dalloc(&ctr, kNctr) | dalloc(&cand, n) | dalloc(&hull, n) | dalloc(&bv, 8 * nb) | dalloc(&bi, 8 * nb);
     rc |= dalloc(&ext, 8);
-    rc |= dalloc(&S, s) | dalloc(&Sout, s) | dalloc(&miss, s) | dalloc(&miss2, s) | dalloc(&mlen, s);
+    rc |= dalloc(&S, s) | dalloc(&Sout, s + n) | dalloc(&miss, s) | dalloc(&miss2, s) | dalloc(&mlen, s);
     rc |= dalloc(&msz, s) | dalloc(&moff, s) | dalloc(&keep, s);
     if (rc) return GQM_CDT_ERR_MEMORY;
 #ifndef GQM_HOST_EMU
@@ -1295,7 +1300,14 @@ struct Builder {
     return 0;
   }
 
-  int run(int np, const double *pts, int ns, const int *segs, gqm_cdt_result *res, gqm_cdt_gpu_stats *sts);
+  // results of the last build (device arrays above)
+  int n_pts = 0, n_tri = 0, n_seg = 0, last_status = 0;
+  char *stage = nullptr;
+  size_t stage_cap = 0;
+
+  int build(int np, const double *pts, int ns, const int *segs, gqm_cdt_gpu_stats *sts);
+  int download(gqm_cdt_result *res, gqm_cdt_gpu_stats *sts);
+  int prepare(int device, int np, const double *pts, int ns, const int *segs, gqm_cdt_gpu_stats *sts);
 };
 
 #ifdef GQM_HOST_EMU
@@ -1309,8 +1321,7 @@ static double ms_since(clk::time_point t0) {
   return std::chrono::duration<double, std::milli>(clk::now() - t0).count();
 }
 
-int Builder::run(int np, const double *pts, int ns, const int *segs, gqm_cdt_result *res,
-                 gqm_cdt_gpu_stats *sts) {
+int Builder::build(int np, const double *pts, int ns, const int *segs, gqm_cdt_gpu_stats *sts) {
   auto t_all = clk::now();
   if (np < 3) return GQM_CDT_ERR_FEW_POINTS;
   if (np > (1 << 28) || ns < 0 || ns > (1 << 29) || (ns > 0 && !segs)) return GQM_CDT_ERR_SEGMENT;
@@ -1513,7 +1524,8 @@ int Builder::run(int np, const double *pts, int ns, const int *segs, gqm_cdt_res
   }
   if (sts) sts->ms_segments = ms_since(t0);
 
-  // 4. output: triangles, neighbours, kept segments, then hull edges without one
+  // 4. output on the device: triangles, neighbours (plain indices), the kept
+  // input segments, then the hull edges that carry none
   t0 = clk::now();
   long need = 6L * ntri;
   if (need > out_cap) {
@@ -1541,33 +1553,78 @@ int Builder::run(int np, const double *pts, int ns, const int *segs, gqm_cdt_res
   std::vector<int> hflag(H);
   cudaMemcpyAsync(hflag.data(), flag, sizeof(int) * H, cudaMemcpyDeviceToHost, st);
   if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_CDT_ERR_CUDA;
-  int nhull = 0;
-  for (int f : hflag) nhull += f;
-  if (sts) sts->ms_output = ms_since(t0);
-  t0 = clk::now();
-  res->numberofpoints = np;
-  res->numberoftriangles = ntri;
-  res->numberofsegments = nkeep + nhull;
-  res->trianglelist = (int *)malloc(sizeof(int) * 3 * (size_t)ntri);
-  res->neighborlist = (int *)malloc(sizeof(int) * 3 * (size_t)ntri);
-  res->segmentlist = (int *)malloc(sizeof(int) * 2 * (size_t)(nkeep + nhull) + 8);
-  if (!res->trianglelist || !res->neighborlist || !res->segmentlist) return GQM_CDT_ERR_MEMORY;
-  cudaMemcpyAsync(res->trianglelist, out, sizeof(int) * 3 * (size_t)ntri, cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(res->neighborlist, out + 3L * ntri, sizeof(int) * 3 * (size_t)ntri, cudaMemcpyDeviceToHost, st);
-  if (nkeep) cudaMemcpyAsync(res->segmentlist, Sout, sizeof(int) * 2 * (size_t)nkeep, cudaMemcpyDeviceToHost, st);
-  if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_CDT_ERR_CUDA;
-  int w = 2 * nkeep;
+  std::vector<int2> hseg;
   for (int i = 0; i < H; ++i)
     if (hflag[i]) {
-      res->segmentlist[w++] = hl[i];
-      res->segmentlist[w++] = hl[(i + 1) % H];
+      int2 e;
+      e.x = hl[i];
+      e.y = hl[(i + 1) % H];
+      hseg.push_back(e);
     }
+  if (!hseg.empty())
+    cudaMemcpyAsync(Sout + nkeep, hseg.data(), sizeof(int2) * hseg.size(), cudaMemcpyHostToDevice, st);
+  if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_CDT_ERR_CUDA;
+  n_pts = np;
+  n_tri = ntri;
+  n_seg = nkeep + (int)hseg.size();
   if (sts) {
-    sts->ms_d2h = ms_since(t0);
+    sts->ms_output = ms_since(t0);
     sts->kernel_launches = launches;
     sts->ms_total = ms_since(t_all);
   }
   return 0;
+}
+
+// The result of the last build, from the device into malloc'ed arrays: one
+// copy into pinned staging, then the host's cores split it up.
+int Builder::download(gqm_cdt_result *res, gqm_cdt_gpu_stats *sts) {
+  auto t0 = clk::now();
+  size_t bt = sizeof(int) * 3 * (size_t)n_tri, bs = sizeof(int) * 2 * (size_t)n_seg;
+  size_t bytes = 2 * bt + bs;
+  if (bytes > stage_cap) {
+    if (stage) cudaFreeHost(stage);
+    stage = nullptr;
+    stage_cap = 0;
+    if (cudaMallocHost((void **)&stage, bytes) != cudaSuccess) return GQM_CDT_ERR_MEMORY;
+    stage_cap = bytes;
+  }
+  cudaMemcpyAsync(stage, out, 2 * bt, cudaMemcpyDeviceToHost, st);
+  if (bs) cudaMemcpyAsync(stage + 2 * bt, Sout, bs, cudaMemcpyDeviceToHost, st);
+  res->numberofpoints = n_pts;
+  res->numberoftriangles = n_tri;
+  res->numberofsegments = n_seg;
+  res->trianglelist = (int *)malloc(bt + 8);
+  res->neighborlist = (int *)malloc(bt + 8);
+  res->segmentlist = (int *)malloc(bs + 8);
+  if (!res->trianglelist || !res->neighborlist || !res->segmentlist) return GQM_CDT_ERR_MEMORY;
+  if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_CDT_ERR_CUDA;
+  host_copy({{res->trianglelist, stage, bt}, {res->neighborlist, stage + bt, bt}, {res->segmentlist, stage + 2 * bt, bs}});
+  if (sts) {
+    sts->ms_d2h = ms_since(t0);
+    sts->ms_total += sts->ms_d2h;
+  }
+  return 0;
+}
+
+// Points and segments in; the refiner's device input out (arrays owned by the builder).
+int Builder::prepare(int device, int np, const double *pts, int ns, const int *segs, gqm_cdt_gpu_stats *stats) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return last_status = GQM_CDT_ERR_NO_DEVICE;
+  if (dev != device) {
+    release();
+    if (cudaSetDevice(device) != cudaSuccess) return GQM_CDT_ERR_NO_DEVICE;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return GQM_CDT_ERR_CUDA;
+    if (cudaMallocHost((void **)&hc, sizeof(int) * kNctr) != cudaSuccess) return GQM_CDT_ERR_MEMORY;
+    dev = device;
+  } else if (cudaSetDevice(device) != cudaSuccess) {
+    return GQM_CDT_ERR_NO_DEVICE;
+  }
+  if (!pts && np > 0) return last_status = GQM_CDT_ERR_FEW_POINTS;
+  int rc = build(np, pts, ns, segs, stats);
+  last_status = rc;
+  if (rc && (rc == GQM_CDT_ERR_CUDA || cudaGetLastError() != cudaSuccess)) release();
+  return rc;
 }
 
 }  // namespace gqm_cdt
@@ -1580,31 +1637,47 @@ int gqm_cdt_build_gpu(int np, const double *pts, int ns, const int *segs, int de
   if (!out) return GQM_CDT_ERR_INTERNAL;
   memset(out, 0, sizeof(*out));
   if (stats) memset(stats, 0, sizeof(*stats));
-  if (!pts && np > 0) return out->status = GQM_CDT_ERR_FEW_POINTS;
   Builder &B = g_builder;
-  int ndev = 0;
-  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
-    return out->status = GQM_CDT_ERR_NO_DEVICE;
-  if (B.dev != device) {
-    B.release();
-    if (cudaSetDevice(device) != cudaSuccess) return out->status = GQM_CDT_ERR_NO_DEVICE;
-    if (cudaStreamCreateWithFlags(&B.st, cudaStreamNonBlocking) != cudaSuccess) return out->status = GQM_CDT_ERR_CUDA;
-    if (cudaMallocHost((void **)&B.hc, sizeof(int) * Builder::kNctr) != cudaSuccess)
-      return out->status = GQM_CDT_ERR_MEMORY;
-    B.dev = device;
-  } else {
-    cudaSetDevice(device);
-  }
-  int rc = B.run(np, pts, ns, segs, out, stats);
+  int rc = B.prepare(device, np, pts, ns, segs, stats);
+  if (rc == 0) rc = B.download(out, stats);
   if (rc) {
     free(out->trianglelist);
     free(out->neighborlist);
     free(out->segmentlist);
     memset(out, 0, sizeof(*out));
-    if (rc == GQM_CDT_ERR_CUDA || cudaGetLastError() != cudaSuccess) B.release();
   }
   return out->status = rc;
 }
+
+int gqm_triangulate_refine(int np, const double *pts, int ns, const int *segs, const gqm_options *opt,
+                           gqm_cdt_out *out, gqm_stats *stats, gqm_cdt_gpu_stats *cdt_stats) {
+  using namespace gqm_cdt;
+  if (!out || !opt) return GQM_ERR_ARGUMENT;
+  memset(out, 0, sizeof(*out));
+  if (cdt_stats) memset(cdt_stats, 0, sizeof(*cdt_stats));
+  if (opt->device < 0 || opt->device >= 64) return GQM_ERR_NO_DEVICE;
+  Builder &B = g_builder;
+  int rc = B.prepare(opt->device, np, pts, ns, segs, cdt_stats);
+  if (rc) return GQM_ERR_INPUT_CDT;
+  // one refiner context per device, kept between calls
+  static std::mutex m;
+  static gqm_context *ctx[64] = {};
+  std::lock_guard<std::mutex> lock(m);
+  if (!ctx[opt->device] && (rc = gqm_context_create(opt->device, &ctx[opt->device]))) return rc;
+  gqm_cdt_in in;
+  in.numberofpoints = B.n_pts;
+  in.pointlist = reinterpret_cast<const double *>(B.P);
+  in.numberoftriangles = B.n_tri;
+  in.trianglelist = B.out;
+  in.neighborlist = B.out + 3L * B.n_tri;
+  in.numberofsegments = B.n_seg;
+  in.segmentlist = reinterpret_cast<const int *>(B.Sout);
+  rc = gqm_context_run(ctx[opt->device], &in, 1, opt, stats);
+  if (rc == GQM_OK) rc = gqm_context_result(ctx[opt->device], out);
+  return rc;
+}
+
+int gqm_cdt_gpu_last_status(void) { return gqm_cdt::g_builder.last_status; }
 
 void gqm_cdt_gpu_free(gqm_cdt_result *r) {
   if (!r) return;

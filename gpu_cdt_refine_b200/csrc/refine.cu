@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "../../include/gqm_refine.h"
+#include "host_copy.h"
 #include "kernels.cuh"
 
 namespace gqm {
@@ -174,32 +175,6 @@ __global__ void k_copy(int *dst, const int *src, const int *dn) {
 }
 __global__ void k_set_count(int *dst, int v) {
   if (threadIdx.x == 0 && blockIdx.x == 0) *dst = v;
-}
-
-// Host memcpy of a few large arrays on the host's cores (staging to and from
-// pinned memory): every copy is cut into pieces of 8 MB shared by the threads.
-struct HostCopy {
-  void *dst;
-  const void *src;
-  size_t bytes;
-};
-static void host_copy(std::initializer_list<HostCopy> list) {
-  constexpr size_t kPiece = 8u << 20;
-  std::vector<HostCopy> pieces;
-  for (const HostCopy &c : list)
-    for (size_t o = 0; o < c.bytes; o += kPiece)
-      pieces.push_back({(char *)c.dst + o, (const char *)c.src + o, std::min(kPiece, c.bytes - o)});
-  int nt = (int)std::min<size_t>(pieces.size(), std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
-  if (nt <= 1) {
-    for (const HostCopy &c : pieces) memcpy(c.dst, c.src, c.bytes);
-    return;
-  }
-  std::vector<std::thread> pool;
-  for (int t = 0; t < nt; ++t)
-    pool.emplace_back([&, t] {
-      for (size_t k = t; k < pieces.size(); k += nt) memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
-    });
-  for (auto &th : pool) th.join();
 }
 
 // ============================================================================
@@ -1354,6 +1329,7 @@ const char *gqm_status_string(int s) {
     case GQM_ERR_CUDA: return "CUDA runtime error";
     case GQM_ERR_NO_DEVICE: return "no CUDA device";
     case GQM_ERR_MEMORY: return "device allocation failed";
+    case GQM_ERR_INPUT_CDT: return "the CDT of the points and segments could not be built";
     case GQM_ERR_ARENA: return "a batched domain outgrew its scratch arena";
     case GQM_ERR_TOO_LARGE: return "result larger than the no-allocation staging array";
     default: return "unknown status";

@@ -51,6 +51,11 @@ def _bind():
         L.gqm_cdt_build_gpu.restype = ctypes.c_int
         L.gqm_cdt_gpu_free.argtypes = [ctypes.POINTER(_native.CdtResult)]
         L.gqm_cdt_gpu_release.argtypes = []
+        L.gqm_cdt_gpu_last_status.restype = ctypes.c_int
+        L.gqm_triangulate_refine.argtypes = [ctypes.c_int, dp, ctypes.c_int, ip, ctypes.POINTER(refine.Options),
+                                             ctypes.POINTER(refine.CdtOut), ctypes.POINTER(refine.Stats),
+                                             ctypes.POINTER(CdtGpuStats)]
+        L.gqm_triangulate_refine.restype = ctypes.c_int
         L._cdt_bound = True
     return L
 
@@ -65,15 +70,45 @@ def build_cdt_gpu(points: np.ndarray, segments: np.ndarray, device: int = 0, wit
     rc = L.gqm_cdt_build_gpu(pts.shape[0], _native.dptr(pts), seg.shape[0], _native.iptr(seg), device, res, st)
     if rc != 0:
         raise CdtBuildError(rc)
-    try:
-        t, s = res.numberoftriangles, res.numberofsegments
-        tri = np.ctypeslib.as_array(res.trianglelist, shape=(t * 3,)).copy()
-        nbr = np.ctypeslib.as_array(res.neighborlist, shape=(t * 3,)).copy()
-        sg = np.ctypeslib.as_array(res.segmentlist, shape=(s * 2,)).copy() if s else np.zeros(0, np.int32)
-    finally:
-        L.gqm_cdt_gpu_free(res)
-    cdt = CDT(pts.copy(), tri, nbr, sg)
+    own = _Owner(L, res)  # the arrays below view the library's memory and free it when gone
+    t, s = res.numberoftriangles, res.numberofsegments
+    cdt = CDT(pts.copy(), refine._view(own, res.trianglelist, 3 * t, ctypes.c_int, np.int32),
+              refine._view(own, res.neighborlist, 3 * t, ctypes.c_int, np.int32),
+              refine._view(own, res.segmentlist, 2 * s, ctypes.c_int, np.int32))
     return (cdt, st.as_dict()) if with_stats else cdt
+
+
+class _Owner:
+    def __init__(self, L, res):
+        self._L, self._res = L, res
+
+    def __del__(self):
+        try:
+            self._L.gqm_cdt_gpu_free(ctypes.byref(self._res))
+        except Exception:
+            pass
+
+
+def triangulate_refine(points: np.ndarray, segments: np.ndarray, theta=20.0, insertpolicy=refine.Offcenter,
+                       mode=1, predicates=refine.PRED_REFERENCE, device=0, max_rounds=0, mlp=None,
+                       max_area=0.0):
+    """Points and segments in, refined mesh out, with the CDT built and refined
+    on the device (no host round trip between the two).  Returns (CDT, refine
+    stats, CDT-construction stats)."""
+    L = _bind()
+    pts = np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 2)
+    seg = np.ascontiguousarray(segments, dtype=np.int32).reshape(-1, 2)
+    out = refine.CdtOut()
+    st = refine.Stats()
+    cst = CdtGpuStats()
+    opt = refine.make_options(theta, insertpolicy, mode, predicates, device, max_rounds, mlp, max_area)
+    rc = L.gqm_triangulate_refine(pts.shape[0], _native.dptr(pts), seg.shape[0], _native.iptr(seg),
+                                  ctypes.byref(opt), ctypes.byref(out), ctypes.byref(st), ctypes.byref(cst))
+    if rc == -15:
+        raise CdtBuildError(L.gqm_cdt_gpu_last_status())
+    if rc != 0:
+        raise refine.RefineError(rc, L.gqm_status_string(rc).decode())
+    return refine._take(out, False, L), st.as_dict(), cst.as_dict()
 
 
 def release() -> None:

@@ -22,6 +22,8 @@
 #ifndef GQM_CDT_H
 #define GQM_CDT_H
 
+#include "gqm_refine.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -67,8 +69,19 @@ void gqm_cdt_free(gqm_cdt_result *r);
 int gqm_cdt_build_gpu(int np, const double *pts, int ns, const int *segs, int device, gqm_cdt_result *out,
                       gqm_cdt_gpu_stats *stats);
 void gqm_cdt_gpu_free(gqm_cdt_result *r);
+/* Status of this host thread's last device build (GQM_CDT_*). */
+int gqm_cdt_gpu_last_status(void);
 /* Frees the device buffers kept between calls on this host thread. */
 void gqm_cdt_gpu_release(void);
+
+/* The reference's whole flow in one call: Triangle "pzQnc" on the host
+ * (GPU_Refine/mesh.cpp:397), then GPU_Refine_Quality (GPU_Refine/main.cpp:1862).  Here the CDT is built
+ * on the device and refined there with no round trip through the host.
+ * Returns a GQM_* status of gqm_refine; GQM_ERR_INPUT_CDT when the CDT could
+ * not be built (gqm_cdt_gpu_last_status() then holds the builder's status).
+ * The refined mesh is released with gqm_free_result; cdt_stats may be NULL. */
+int gqm_triangulate_refine(int np, const double *pts, int ns, const int *segs, const gqm_options *opt,
+                           gqm_cdt_out *out, gqm_stats *stats, gqm_cdt_gpu_stats *cdt_stats);
 
 #ifdef __cplusplus
 }

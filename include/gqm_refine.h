@@ -33,6 +33,7 @@ extern "C" {
 #define GQM_ERR_NO_DEVICE (-11)   /* no CUDA device */
 #define GQM_ERR_MEMORY (-12)      /* device allocation failed */
 #define GQM_ERR_ARENA (-14)       /* a batched domain outgrew its block's scratch arena */
+#define GQM_ERR_INPUT_CDT (-15)   /* gqm_triangulate_refine: the CDT could not be built (gqm_cdt_gpu_last_status) */
 
 /* InsertPolicy (GPU_Refine/refine.h:32) */
 #define GQM_CIRCUMCENTER 0

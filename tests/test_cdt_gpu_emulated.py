@@ -164,3 +164,21 @@ def test_errors(emulated, case, status):
     # the builder stays usable after an error
     ok = triangulate.build_cdt_gpu(rng.uniform(0.0, 1.0, (50, 2)), np.zeros((0, 2), np.int32))
     assert ok.numberoftriangles > 0
+
+
+def test_triangulate_refine_equals_two_calls(emulated):
+    """The fused call (CDT built and refined on the device) gives the bytes of
+    building the CDT and then refining it."""
+    pts = inputs.uniform_points(3000, 0.0, 1000.0, 41)
+    seg = inputs.pick_segments(pts, 150, 42)
+    cdt = triangulate.build_cdt_gpu(pts, seg)
+    two, _ = refine.refine(cdt, theta=20.0)
+    one, st, cst = triangulate.triangulate_refine(pts, seg, theta=20.0)
+    for f in ("pointlist", "trianglelist", "neighborlist", "segmentlist"):
+        assert np.array_equal(getattr(one, f), getattr(two, f)), f
+    assert cst["hull_vertices"] > 2 and st["rounds"] > 0
+    cert = certify(one, cdt, 20.0)
+    assert cert["ok"] and cert["triangles_below_theta"] == 0, cert
+    with pytest.raises(triangulate.CdtBuildError) as e:
+        triangulate.triangulate_refine(np.concatenate([pts, pts[:1]]), seg)
+    assert e.value.status == -8

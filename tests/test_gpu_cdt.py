@@ -102,3 +102,27 @@ def test_refine_a_gpu_built_input():
     cert = certify(out, cdt, 20.0)
     assert cert["ok"], cert
     assert cert["triangles_below_theta"] <= 1
+
+
+def test_triangulate_refine_2m():
+    """Points and segments to refined mesh on the device: the same bytes as
+    the two calls, and the time of the whole flow against the CPU builder
+    followed by the refiner."""
+    pts = inputs.cluster_points(2_000_000, 64, 1.0e4, 5.0, 200.0, 0.10, 20261205)
+    seg = inputs.pick_segments(pts, 100_000, 20261206)
+    triangulate.triangulate_refine(pts, seg)  # warm-up
+    t0 = time.perf_counter()
+    one, st, cst = triangulate.triangulate_refine(pts, seg)
+    t1 = time.perf_counter()
+    cdt = inputs.build_cdt(pts, seg)
+    two, _ = refine.refine(cdt, theta=20.0)
+    t2 = time.perf_counter()
+    same = cdtio.same_mesh(cdt, triangulate.build_cdt_gpu(pts, seg))
+    print(f"\npoints to refined mesh, 2M: fused GPU call {(t1 - t0) * 1e3:.1f} ms, CPU builder + refiner "
+          f"{(t2 - t1) * 1e3:.1f} ms; CDT {cst['ms_total']:.1f} ms, output triangles {one.numberoftriangles}")
+    assert same
+    ref_cdt = triangulate.build_cdt_gpu(pts, seg)
+    three, _ = refine.refine(ref_cdt, theta=20.0)
+    for f in ("pointlist", "trianglelist", "neighborlist", "segmentlist"):
+        assert np.array_equal(getattr(one, f), getattr(three, f)), f
+    assert abs(one.numberoftriangles - two.numberoftriangles) < 0.005 * two.numberoftriangles
