@@ -76,10 +76,13 @@ def parse():
 
 
 def workload(args):
+    """The clustered input of inputs.clustered, keeping its points and segments."""
     from gpu_cdt_refine_b200 import inputs
     t0 = time.time()
-    cdt = inputs.clustered(seed=args.seed, n=args.points, nseg=args.segments)
-    return cdt, time.time() - t0
+    pts = inputs.cluster_points(args.points, 64, 1.0e4, 5.0, 200.0, 0.10, args.seed)
+    seg = inputs.pick_segments(pts, args.segments, args.seed + 1)
+    cdt = inputs.build_cdt(pts, seg)
+    return cdt, time.time() - t0, pts, seg
 
 
 def config(args, cdt):
@@ -251,6 +254,51 @@ def run_learned(cdt, args, local_rank):
     return res
 
 
+def run_construction(pts, seg, e2e_ms, local_rank):
+    """CDT construction, the step in front of the refiner: the GPU builder
+    against the reference's own input builder (Triangle "pzQnc",
+    GPU_Refine/mesh.cpp:397, one host core) and this repository's exact CPU
+    builder on the same points and segments; then the whole flow from points
+    and segments to the refined mesh in one device-resident call."""
+    from gpu_cdt_refine_b200 import cdtio, inputs, triangulate
+    res = {"workload": f"{pts.shape[0]} clustered points, {seg.shape[0]} segments (the input of the main workload)"}
+    walls, st, g = [], None, None
+    for i in range(4):
+        t0 = time.perf_counter()
+        g, st = triangulate.build_cdt_gpu(pts, seg, device=local_rank, with_stats=True)
+        if i:
+            walls.append((time.perf_counter() - t0) * 1e3)
+    res["gpu_ms"] = float(np.median(walls))
+    res["gpu_phases_ms"] = {k: st[k] for k in ("ms_h2d", "ms_hull", "ms_insert", "ms_segments", "ms_output", "ms_d2h")}
+    res["gpu_counts"] = {k: st[k] for k in ("insert_rounds", "flip_rounds", "recover_rounds", "segments_missing",
+                                            "flips", "recover_flips", "kernel_launches", "hull_vertices")}
+    t0 = time.perf_counter()
+    mine = inputs.build_cdt(pts, seg)
+    res["cpu_builder_ms"] = (time.perf_counter() - t0) * 1e3
+    res["same_as_cpu_builder"] = bool(cdtio.same_mesh(mine, g))
+    try:
+        from oracle import tri_ref
+        tri, tri_ms = tri_ref.cdt(pts, seg, with_ms=True)
+        res["triangle_ms"] = tri_ms
+        res["triangle_cores"] = 1
+        res["same_as_triangle"] = bool(cdtio.same_mesh(tri, g))
+        res["speedup_vs_triangle"] = tri_ms / res["gpu_ms"]
+    except Exception as e:  # the reference build is test infrastructure; report, do not fail
+        res["triangle_ms"] = None
+        res["triangle_unavailable"] = str(e)
+    walls = []
+    for i in range(3):
+        t0 = time.perf_counter()
+        out, _, _ = triangulate.triangulate_refine(pts, seg, device=local_rank)
+        if i:
+            walls.append((time.perf_counter() - t0) * 1e3)
+    res["points_to_refined_mesh_ms"] = float(np.median(walls))
+    res["points_to_refined_mesh_triangles"] = out.numberoftriangles
+    if res.get("triangle_ms") is not None:
+        res["triangle_cdt_then_refine_ms"] = res["triangle_ms"] + e2e_ms
+    return res
+
+
 def time_triangle(cdt, reps, theta=20.0, mode=1):
     """Triangle -q (reference CPU quality refinement) on the CDT; returns (tri/s, ms list, out tris)."""
     from oracle import tri_ref
@@ -264,7 +312,7 @@ def time_triangle(cdt, reps, theta=20.0, mode=1):
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    full, _ = workload(args)
+    full = workload(args)[0]
     cdt = cpu_sample(args)
     from oracle import tri_ref
     for _ in range(min(args.warmup, 1)):
@@ -295,7 +343,7 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
-    cdt, gen_s = workload(args)
+    cdt, gen_s, raw_pts, raw_seg = workload(args)
     # inputs resident in HBM
     d_pts = torch.from_numpy(cdt.pointlist).to(dev)
     d_tri = torch.from_numpy(cdt.trianglelist).to(dev)
@@ -389,6 +437,7 @@ def run_ours(args, rank, world, local_rank):
         if args.batch_domains > 0 and world == 1:
             line["batch"] = run_batch_workload(args, local_rank)
         if args.extras and world == 1:
+            line["construction"] = run_construction(raw_pts, raw_seg, e2e_max, local_rank)
             line["learned"] = run_learned(cdt, args, local_rank)
             line["adversarial"] = run_adversarial(local_rank)
         if args.cpu_baseline and world == 1:

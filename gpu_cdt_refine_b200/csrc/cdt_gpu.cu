@@ -58,6 +58,10 @@ constexpr int kNoSeg = 0x7fffffff;      // edge carries no segment
 constexpr int kStampMax = 0x3fffffff;   // round stamps count up to this
 constexpr int kThreads = 256;
 constexpr int kMaxBlocks = 148 * 16;
+// Kernels whose item count is only known on the device (flip rounds, pending
+// points): one wave of four blocks per SM covers the grid-stride loop; idle
+// rounds then cost one short wave instead of many.
+constexpr int kWaveBlocks = 148 * 4;
 
 #define CDEV __device__ __forceinline__
 #define GRID_LOOP(i, n) \
@@ -141,8 +145,22 @@ struct Dm {
 };
 
 CDEV void set_err(int *err, int code) { atomicCAS(err, 0, code); }
-CDEV void dirty(const Dm &M, int t, int tag, int *list, int *cnt) {
-  if (atomicExch(&M.dst[t], tag) != tag) list[atomicAdd(cnt, 1)] = t;
+// Slot in a list of length *len for every lane that wants one: one atomic
+// per group of converged lanes, slots in lane order.  Every lane of the
+// group calls it (want may be false).
+CDEV int warp_slot(int *len, bool want) {
+  unsigned m = __activemask();
+  unsigned b = __ballot_sync(m, want);
+  int lane = threadIdx.x & 31, leader = __ffs(m) - 1, base = 0;
+  if (lane == leader && b) base = atomicAdd(len, __popc(b));
+  base = __shfl_sync(m, base, leader);
+  return base + __popc(b & ((1u << lane) - 1));
+}
+// Appends t to a dirty list unless it is there already (all lanes call it).
+CDEV void dirty(const Dm &M, int t, bool want, int tag, int *list, int *cnt) {
+  want = want && atomicExch(&M.dst[t], tag) != tag;
+  int pos = warp_slot(cnt, want);
+  if (want) list[pos] = t;
 }
 // back pointer of a neighbour that no operation of this round rewrites
 CDEV void link_out(const Dm &M, int s, int e, int nb, int stamp) {
@@ -333,7 +351,8 @@ __global__ void k_pick(Dm M, const int *pend, const int *pn, int stamp) {
   u64 hi = stamp_hi(stamp);
   GRID_LOOP(i, n) {
     int q = pend[i];
-    atomicMin(&M.pick[M.loc[q]], hi | (u64)q);
+    u64 key = hi | (u64)q, *pk = &M.pick[M.loc[q]];
+    if (*pk > key) atomicMin(pk, key);  // most points of a crowded triangle see a smaller index already
   }
 }
 
@@ -403,7 +422,7 @@ __global__ void k_win_insert(Dm M, const int *pend, const int *pn, int stamp, co
   }
 }
 
-CDEV void split13(const Dm &M, int t, int q, int s1, int s2, int stamp, int tag, int *D, int *dcnt) {
+CDEV void split13(const Dm &M, int t, int q, int s1, int s2, int stamp) {
   int4 v = M.tv[t], n = M.tn[t], c = M.tc[t];
   M.tv[t] = i4(q, v.y, v.z, 0);
   M.tv[s1] = i4(v.x, q, v.z, 0);
@@ -419,14 +438,11 @@ CDEV void split13(const Dm &M, int t, int q, int s1, int s2, int stamp, int tag,
   link_out(M, t, 0, n.x, stamp);
   link_out(M, s1, 1, n.y, stamp);
   link_out(M, s2, 2, n.z, stamp);
-  dirty(M, t, tag, D, dcnt);
-  dirty(M, s1, tag, D, dcnt);
-  dirty(M, s2, tag, D, dcnt);
 }
 
 // q on edge i of t, shared with u (edge j).  t keeps v_{i+1} -> q, s1 takes
 // v_{i+2} -> q; u keeps w_{j+1} -> q, s2 takes w_{j+2} -> q.
-CDEV void split24(const Dm &M, int t, int i, int q, int s1, int s2, int stamp, int tag, int *D, int *dcnt) {
+CDEV int split24(const Dm &M, int t, int i, int q, int s1, int s2, int stamp) {
   int4 v = M.tv[t], n = M.tn[t], c = M.tc[t];
   int nbr = comp(n, i), u = nbr >> 2, j = nbr & 3;
   int4 w = M.tv[u], m = M.tn[u], d = M.tc[u];
@@ -488,24 +504,39 @@ CDEV void split24(const Dm &M, int t, int i, int q, int s1, int s2, int stamp, i
   link_out(M, s1, i2, comp(n, i2), stamp);
   link_out(M, u, j1, comp(m, j1), stamp);
   link_out(M, s2, j2, comp(m, j2), stamp);
-  dirty(M, t, tag, D, dcnt);
-  dirty(M, s1, tag, D, dcnt);
-  dirty(M, u, tag, D, dcnt);
-  dirty(M, s2, tag, D, dcnt);
+  return u;
 }
 
 __global__ void k_split(Dm M, const int *pend, const int *pn, const int *ptype, const int *wflag, const int *wrank,
                         const int *ntri, int stamp, int tag, int *D, int *dcnt) {
   int n = *pn, nt0 = *ntri;
   GRID_LOOP(i, n) {
-    if (!wflag[i]) continue;
-    int q = pend[i], t = M.loc[q], ty = ptype[i];
-    int s1 = nt0 + 2 * wrank[i], s2 = s1 + 1;
-    M.loc[q] = -1;
-    if (ty == 3)
-      split13(M, t, q, s1, s2, stamp, tag, D, dcnt);
-    else
-      split24(M, t, ty, q, s1, s2, stamp, tag, D, dcnt);
+    bool win = wflag[i];
+    int t = -1, u = -1, s1 = -1, s2 = -1;
+    if (win) {
+      int q = pend[i], ty = ptype[i];
+      t = M.loc[q];
+      s1 = nt0 + 2 * wrank[i];
+      s2 = s1 + 1;
+      M.loc[q] = -1;
+      if (ty == 3)
+        split13(M, t, q, s1, s2, stamp);
+      else
+        u = split24(M, t, ty, q, s1, s2, stamp);
+    }
+    // the children join the next flip round's list (no slot is in it yet)
+    int pos = warp_slot(dcnt, win), pu = warp_slot(dcnt, u >= 0), p1 = warp_slot(dcnt, win),
+        p2 = warp_slot(dcnt, win);
+    if (win) {
+      D[pos] = t;
+      D[p1] = s1;
+      D[p2] = s2;
+      M.dst[t] = M.dst[s1] = M.dst[s2] = tag;
+    }
+    if (u >= 0) {
+      D[pu] = u;
+      M.dst[u] = tag;
+    }
   }
 }
 
@@ -534,32 +565,32 @@ __global__ void k_fix_insert(Dm M, const int *pend, const int *pn, const int *pt
   }
 }
 
-// Pending points of rewritten triangles move to the child that contains them.
-__global__ void k_relocate(Dm M, const int *pend, const int *pn, int stamp) {
+// Pending points find their triangle again once the flips of a round have
+// converged: a visibility walk from the slot that held them (slots are reused
+// in place, so it is nearby).  The triangulation is Delaunay at that point, so
+// the walk cannot cycle; the step bound only guards the invariant.
+__global__ void k_walk(Dm M, const int *pend, const int *pn) {
   int n = *pn;
   GRID_LOOP(i, n) {
     int q = pend[i], t = M.loc[q];
-    if (t < 0 || M.mst[t] != stamp) continue;
-    int4 r = M.rmap[t], g = M.rgeo[t];
     double2 pq = M.P[q];
-    int to;
-    if (r.w == 3) {
-      double2 p = M.P[g.w];
-      double d1 = orient(p, M.P[g.y], pq), d2 = orient(p, M.P[g.z], pq);
-      if (d1 >= 0 && d2 <= 0) {
-        to = r.x >> 2;
-      } else {
-        double d0 = orient(p, M.P[g.x], pq);
-        to = (d2 >= 0 && d0 <= 0) ? (r.y >> 2) : (r.z >> 2);
+    for (int step = 0;; ++step) {
+      if (step > (1 << 20)) {
+        set_err(M.err, GQM_CDT_ERR_INTERNAL);
+        break;
       }
-    } else if (r.w < 8) {
-      int e = r.w - 4;
-      double o = orient(M.P[g.w], M.P[comp(g, e)], pq);
-      to = o >= 0 ? (comp(r, nx(nx(e))) >> 2) : (comp(r, nx(e)) >> 2);
-    } else {
-      to = orient(M.P[g.x], M.P[g.y], pq) <= 0 ? g.z : g.w;
+      int4 v = M.tv[t];
+      double2 a = M.P[v.x], b = M.P[v.y], c = M.P[v.z];
+      int k = orient(b, c, pq) < 0 ? 0 : (orient(c, a, pq) < 0 ? 1 : (orient(a, b, pq) < 0 ? 2 : -1));
+      if (k < 0) break;
+      int nb = get(M.tn, t, k);
+      if (nb < 0) {
+        set_err(M.err, GQM_CDT_ERR_INTERNAL);
+        break;
+      }
+      t = nb >> 2;
     }
-    M.loc[q] = to;
+    M.loc[q] = t;
   }
 }
 
@@ -603,33 +634,45 @@ CDEV int flip(const Dm &M, int t, int k, int stamp, bool link) {
 
 // Each edge of a dirty triangle that is not a segment and fails the incircle
 // test claims its two triangles with key (stamp, t, k).  An edge between two
-// dirty triangles is tested from the smaller one.
-__global__ void k_flip_check(Dm M, const int *D, const int *pn, int tag, int stamp, int *C, int *ccnt) {
-  int n = *pn;
+// dirty triangles is tested from the smaller one.  A triangle flipped in the
+// previous round first fixes its outer pointers to neighbours that flipped in
+// that round too (their edge maps are complete by now; the check of a
+// triangle reads no other triangle's neighbour words).  Counters: dcur is
+// this round's dirty count, dnext the next round's (cleared here for the
+// apply launch).
+__global__ void k_flip_check(Dm M, const int *D, const int *dcur, int *dnext, int tag, int stamp, int *C,
+                             int *ccur) {
+  int n = *dcur;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *dnext = 0;
   u64 hi = stamp_hi(stamp);
   GRID_LOOP(i, n) {
     int t = D[i];
+    if (M.mst[t] == stamp - 1 && M.rmap[t].w == 8) {
+      fix_edge(M, t, 0, stamp - 1);
+      fix_edge(M, t, 2, stamp - 1);
+    }
     int4 v = M.tv[t], nb = M.tn[t], c = M.tc[t];
-    double2 a = M.P[v.x], b = M.P[v.y], cc = M.P[v.z];
+    double2 a = M.P[v.x], b = M.P[v.y], cc3 = M.P[v.z];
     for (int k = 0; k < 3; ++k) {
-      int e = comp(nb, k);
-      if (e < 0 || comp(c, k) != kNoSeg) continue;
-      int u = e >> 2;
-      if (u < t && M.dst[u] == tag) continue;
-      int w = get(M.tv, u, e & 3);
-      if (incircle(a, b, cc, M.P[w]) > 0) {
-        int code = (t << 2) | k;
+      int e = comp(nb, k), u = e >> 2;
+      bool bad = e >= 0 && comp(c, k) == kNoSeg && !(u < t && M.dst[u] == tag) &&
+                 incircle(a, b, cc3, M.P[get(M.tv, u, e & 3)]) > 0;
+      int code = (t << 2) | k;
+      if (bad) {
         u64 key = hi | (u64)(unsigned)code;
         atomicMin(&M.claim[t], key);
         atomicMin(&M.claim[u], key);
-        C[atomicAdd(ccnt, 1)] = code;
       }
+      int pos = warp_slot(ccur, bad);
+      if (bad) C[pos] = code;
     }
   }
 }
 
-__global__ void k_flip_win(Dm M, const int *C, const int *pn, int stamp, int *wf) {
-  int n = *pn;
+// ccur: this round's candidates; cnext: the next round's (cleared here)
+__global__ void k_flip_win(Dm M, const int *C, const int *ccur, int *cnext, int stamp, int *wf) {
+  int n = *ccur;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *cnext = 0;
   u64 hi = stamp_hi(stamp);
   GRID_LOOP(i, n) {
     int code = C[i], t = code >> 2, u = get(M.tn, t, code & 3) >> 2;
@@ -640,36 +683,21 @@ __global__ void k_flip_win(Dm M, const int *C, const int *pn, int stamp, int *wf
   }
 }
 
-__global__ void k_flip_apply(Dm M, const int *C, const int *pn, const int *wf, int stamp, int tag, int *D,
+__global__ void k_flip_apply(Dm M, const int *C, const int *ccur, const int *wf, int stamp, int tag, int *D,
                              int *dcnt, int *nflips) {
-  int n = *pn;
+  int n = *ccur;
   GRID_LOOP(i, n) {
-    int code = C[i], t = code >> 2;
-    if (!wf[i]) {
-      dirty(M, t, tag, D, dcnt);  // retried next round
-      continue;
-    }
-    int u = flip(M, t, code & 3, stamp, true);
-    atomicAdd(nflips, 1);
-    dirty(M, t, tag, D, dcnt);
-    dirty(M, u, tag, D, dcnt);
-  }
-}
-
-__global__ void k_flip_fix(Dm M, const int *C, const int *pn, const int *wf, int stamp) {
-  int n = *pn;
-  GRID_LOOP(i, n) {
-    if (!wf[i]) continue;
-    int t = C[i] >> 2, u = get(M.tn, t, 1) >> 2;
-    fix_edge(M, t, 0, stamp);
-    fix_edge(M, t, 2, stamp);
-    fix_edge(M, u, 0, stamp);
-    fix_edge(M, u, 2, stamp);
+    int code = C[i], t = code >> 2, u = -1;
+    bool win = wf[i];
+    if (win) u = flip(M, t, code & 3, stamp, true);
+    dirty(M, t, true, tag, D, dcnt);  // a loser is retried next round
+    dirty(M, u, win, tag, D, dcnt);
+    warp_slot(nflips, win);  // counts the flips
   }
 }
 
 __global__ void k_all_dirty(Dm M, int nt, int tag, int *D, int *dcnt) {
-  GRID_LOOP(t, nt) dirty(M, (int)t, tag, D, dcnt);
+  GRID_LOOP(t, nt) dirty(M, (int)t, true, tag, D, dcnt);
 }
 
 // ---------------------------------------------------------------------------
@@ -957,7 +985,8 @@ __global__ void k_chan_sloan(Dm M, const int2 *S, const int *miss, int nm, const
       put(M.rmap, e.x, e.y, (rt << 2) | rk);
       link_out(M, rt, rk, get(M.tn, rt, rk), stamp);
     }
-    for (int r = 0; r < nR; ++r) dirty(M, reg[r], tag, D, dcnt);
+    for (int r = 0; r < nR; ++r)
+      if (atomicExch(&M.dst[reg[r]], tag) != tag) D[atomicAdd(dcnt, 1)] = reg[r];
     atomicAdd(nflips, flips);
   }
 }
@@ -1148,7 +1177,9 @@ struct Builder {
   long long launches = 0;
 
   // device counters in ctr[]
-  enum { kErr = 0, kNtri, kNpend, kNd, kNd2, kNc, kFlips, kTot, kMiss, kHcnt, kRecFlips, kNctr = 16 };
+  // kNd and kNc hold two counters each (dirty list and candidates of
+  // alternating flip rounds)
+  enum { kErr = 0, kNtri, kNpend, kNd, kNc = kNd + 2, kFlips = kNc + 2, kTot, kMiss, kHcnt, kRecFlips, kNctr = 16 };
 
   template <class T>
   int dalloc(T **p, long n) {
@@ -1272,31 +1303,35 @@ struct Builder {
   }
 
   // Lawson flips over the dirty list D (count in ctr[kNd], tag `tag`) until
-  // no edge is illegal.  Pending points follow the flips.
-  int lawson(int npend_bound, gqm_cdt_gpu_stats *sts, long long *flips_total) {
+  // no edge is illegal; three launches a round, one synchronisation every four
+  // rounds.  Pending points then walk to their triangles.
+  int lawson(int npend, gqm_cdt_gpu_stats *sts) {
     Dm M = dm();
+    int *dbuf[2] = {D, D2};
+    KL(k_set, 1, 1)(ctr + kNc, 0);
+    launches++;
+    int r = 0;
     for (int iter = 0;; ++iter) {
-      for (int r = 0; r < 4; ++r) {
+      for (int k = 0; k < 4; ++k, ++r) {
         ++stamp;
-        int t2 = ++tag;
-        KL(k_set, 1, 1)(ctr + kNc, 0);
-        KL(k_flip_check, kMaxBlocks, kThreads)(M, D, ctr + kNd, tag - 1, stamp, C, ctr + kNc);
-        KL(k_flip_win, kMaxBlocks, kThreads)(M, C, ctr + kNc, stamp, wf);
-        KL(k_set, 1, 1)(ctr + kNd2, 0);
-        KL(k_flip_apply, kMaxBlocks, kThreads)(M, C, ctr + kNc, wf, stamp, t2, D2, ctr + kNd2, ctr + kFlips);
-        KL(k_flip_fix, kMaxBlocks, kThreads)(M, C, ctr + kNc, wf, stamp);
-        if (npend_bound > 0) KL(k_relocate, kMaxBlocks, kThreads)(M, pend, ctr + kNpend, stamp);
-        std::swap(D, D2);
-        cudaMemcpyAsync(ctr + kNd, ctr + kNd2, sizeof(int), cudaMemcpyDeviceToDevice, st);
-        launches += 8 + (npend_bound > 0);
+        int t2 = ++tag, p = r & 1, q = p ^ 1;
+        KL(k_flip_check, kWaveBlocks, kThreads)(M, dbuf[p], ctr + kNd + p, ctr + kNd + q, tag - 1, stamp, C,
+                                               ctr + kNc + p);
+        KL(k_flip_win, kWaveBlocks, kThreads)(M, C, ctr + kNc + p, ctr + kNc + q, stamp, wf);
+        KL(k_flip_apply, kWaveBlocks, kThreads)(M, C, ctr + kNc + p, wf, stamp, t2, dbuf[q], ctr + kNd + q,
+                                               ctr + kFlips);
+        launches += 3;
         if (sts) sts->flip_rounds++;
       }
       int e = sync_ctr();
       if (e) return e;
-      if (hc[kNd] == 0) break;
+      if (hc[kNd + (r & 1)] == 0) break;
       if (iter > (1 << 20)) return GQM_CDT_ERR_INTERNAL;
     }
-    if (flips_total) *flips_total = hc[kFlips];
+    if (npend > 0) {
+      KL(k_walk, kWaveBlocks, kThreads)(M, pend, ctr + kNpend);
+      launches++;
+    }
     return 0;
   }
 
@@ -1327,7 +1362,9 @@ int Builder::build(int np, const double *pts, int ns, const int *segs, gqm_cdt_g
   if (np > (1 << 28) || ns < 0 || ns > (1 << 29) || (ns > 0 && !segs)) return GQM_CDT_ERR_SEGMENT;
   int rc = reserve(np, ns);
   if (rc) return rc;
-  stamp = 0;
+  // mst starts at 0 for every slot, so no stamp - 1 seen by a flip check may be
+  // 0: stamps start at 1 (edge maps left by an earlier build are never read)
+  stamp = 1;
   tag = 0;
   launches = 0;
   long T = 2L * np + 8;
@@ -1348,7 +1385,7 @@ int Builder::build(int np, const double *pts, int ns, const int *segs, gqm_cdt_g
 #ifdef GQM_HOST_EMU
   int nb = 1;  // one emulated block covers the grid
 #else
-  int nb = grid_for(np);
+  int nb = std::min(grid_for(np), 2 * 148);  // the final reduction runs on one thread
 #endif
   KL(k_ext_partial, nb, kThreads)(P, np, bv, bi);
   KL(k_ext_final, 1, 1)(nb, bv, bi, ext);
@@ -1436,7 +1473,7 @@ int Builder::build(int np, const double *pts, int ns, const int *segs, gqm_cdt_g
   KL(k_set, 1, 1)(ctr + kNd, 0);
   KL(k_all_dirty, grid_for(ntri), kThreads)(M, ntri, tag, D, ctr + kNd);
   launches += 3;
-  if ((rc = lawson(npend, sts, nullptr))) return rc;
+  if ((rc = lawson(npend, sts))) return rc;
   if (sts) sts->ms_hull = ms_since(t0);
 
   // 2. insertion rounds
@@ -1452,7 +1489,6 @@ int Builder::build(int np, const double *pts, int ns, const int *segs, gqm_cdt_g
     KL(k_split, kMaxBlocks, kThreads)(M, pend, ctr + kNpend, ptype, flag, rank, ctr + kNtri, stamp, t2, D,
                                       ctr + kNd);
     KL(k_fix_insert, kMaxBlocks, kThreads)(M, pend, ctr + kNpend, ptype, flag, rank, ctr + kNtri, stamp);
-    KL(k_relocate, kMaxBlocks, kThreads)(M, pend, ctr + kNpend, stamp);
     KL(k_total, 1, 1)(flag, rank, npend, ctr + kTot);
     KL(k_add, 1, 1)(ctr + kNtri, ctr + kTot, 2);
     // drop inserted points from the pending list (order kept)
@@ -1461,12 +1497,12 @@ int Builder::build(int np, const double *pts, int ns, const int *segs, gqm_cdt_g
     KL(k_scatter, grid_for(npend), kThreads)(pend, npend, flag, rank, pend2);
     KL(k_total, 1, 1)(flag, rank, npend, ctr + kNpend);
     std::swap(pend, pend2);
-    launches += 12;
+    launches += 11;
     if (sts) sts->insert_rounds++;
     if ((rc = sync_ctr())) return rc;
     if (hc[kTot] == 0) return GQM_CDT_ERR_INTERNAL;  // no progress
     npend = hc[kNpend];
-    if ((rc = lawson(npend, sts, nullptr))) return rc;
+    if ((rc = lawson(npend, sts))) return rc;
   }
   if ((rc = sync_ctr())) return rc;
   ntri = hc[kNtri];
@@ -1519,7 +1555,8 @@ int Builder::build(int np, const double *pts, int ns, const int *segs, gqm_cdt_g
       sts->recover_flips = hc[kRecFlips];
     }
     long long before = hc[kFlips];
-    if ((rc = lawson(0, sts, nullptr))) return rc;
+    ++stamp;  // channel slots carry flip maps of this phase; the first check must not read them
+    if ((rc = lawson(0, sts))) return rc;
     if (sts) sts->flips += hc[kFlips] - before;
   }
   if (sts) sts->ms_segments = ms_since(t0);

@@ -114,3 +114,32 @@ def triangulate_refine(points: np.ndarray, segments: np.ndarray, theta=20.0, ins
 def release() -> None:
     """Frees the device buffers the builder keeps between calls."""
     _bind().gqm_cdt_gpu_release()
+
+
+def main(argv=None):
+    """Builds the CDT of the clustered benchmark input on the GPU and prints
+    the builder's statistics (one JSON line per build)."""
+    import argparse
+    import json
+    import time
+
+    from . import inputs
+    p = argparse.ArgumentParser(description=main.__doc__)
+    p.add_argument("--points", type=int, default=2_000_000)
+    p.add_argument("--segments", type=int, default=100_000)
+    p.add_argument("--seed", type=int, default=20261205)
+    p.add_argument("--repeat", type=int, default=1)
+    p.add_argument("--device", type=int, default=0)
+    a = p.parse_args(argv)
+    pts = inputs.cluster_points(a.points, 64, 1.0e4, 5.0, 200.0, 0.10, a.seed)
+    seg = inputs.pick_segments(pts, a.segments, a.seed + 1)
+    for _ in range(a.repeat):
+        t0 = time.perf_counter()
+        cdt, st = build_cdt_gpu(pts, seg, device=a.device, with_stats=True)
+        st["wall_ms"] = (time.perf_counter() - t0) * 1e3
+        st["triangles"] = cdt.numberoftriangles
+        print(json.dumps(st), flush=True)
+
+
+if __name__ == "__main__":
+    main()

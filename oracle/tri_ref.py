@@ -42,7 +42,8 @@ def _take(r):
                np.ctypeslib.as_array(r.sl, shape=(2 * r.ns,)).copy())
 
 
-def cdt(points, segments):
+def cdt(points, segments, with_ms=False):
+    """Triangle "pzQnc" CDT; with_ms also returns the time of the triangulate() call."""
     L = lib()
     r = TriResult()
     p = np.ascontiguousarray(points, np.float64)
@@ -50,7 +51,7 @@ def cdt(points, segments):
     L.tri_ref_cdt(p.shape[0], p.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), s.shape[0],
                   s.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ctypes.byref(r))
     try:
-        return _take(r)
+        return (_take(r), r.ms) if with_ms else _take(r)
     finally:
         L.tri_ref_free(ctypes.byref(r))
 

@@ -111,6 +111,7 @@ inline void __syncthreads() {}
 inline void __syncwarp(unsigned = 0xffffffffu) {}
 inline int __shfl_down_sync(unsigned, int v, int) { return v; }
 inline unsigned __ballot_sync(unsigned, bool p) { return p ? 1u : 0u; }
+inline unsigned __activemask() { return 1u; }
 inline int __popc(unsigned v) { return __builtin_popcount(v); }
 inline int __shfl_up_sync(unsigned, int v, int) { return v; }
 inline int __shfl_sync(unsigned, int v, int) { return v; }
