@@ -11,7 +11,7 @@
 // walks, link updates): ask for at least this many resident 256-thread blocks
 // per SM, so enough warps are in flight to cover their dependent loads.
 #ifndef GQM_WALK_MIN_BLOCKS
-#define GQM_WALK_MIN_BLOCKS 3
+#define GQM_WALK_MIN_BLOCKS 2
 #endif
 
 // Two compilations of the same kernels:
@@ -1019,20 +1019,44 @@ GQM_KERNEL void GQM_WALK_BOUNDS k_check_flip2(Mesh M, const int *act, const int 
     int4 nb = M.tn[index];
     int4 sg = M.tsg[index];
     int pp[3] = {p.x, p.y, p.z};
+    const bool red[3] = {is_red(M, p.x), is_red(M, p.y), is_red(M, p.z)};
+    double2 v[3] = {M.pts[p.x], M.pts[p.y], M.pts[p.z]};
+    // The gathers of all three edges are issued before any decision below:
+    // nothing they read changes during the launch (flags are the ones the
+    // step started with), so the edges are still decided in the reference's
+    // order, but an item waits for two dependent levels of loads instead of
+    // two per edge in turn.
+    int eTri[3], eOri[3], eOpp[3];
+    uint8_t eFlip[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int tri = comp(nb, i);
+      eTri[i] = dtri(tri);
+      eOri[i] = dori(tri);
+      const bool use = comp(sg, i) == -1 && eTri[i] >= 0;
+      eFlip[i] = (use && eTri[i] < index) ? M.tflip[eTri[i]] : 0;
+      eOpp[i] = use ? ld1(M.tv, eTri[i], eOri[i]) : -1;
+    }
+    bool eRed[3];
+    double2 eV[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      eRed[i] = eOpp[i] >= 0 && is_red(M, eOpp[i]);
+      eV[i] = eOpp[i] >= 0 ? M.pts[eOpp[i]] : v[i];
+    }
     int mn = kMaxInt;
     for (int i = 0; i < 3; ++i)
-      if (is_red(M, pp[i]) && pp[i] < mn) mn = pp[i];
-    double2 v[3] = {M.pts[p.x], M.pts[p.y], M.pts[p.z]};
+      if (red[i] && pp[i] < mn) mn = pp[i];
     bool done = false;
+#pragma unroll
     for (int i = 0; i < 3 && !done; i++) {
       if (mn == pp[i]) continue;
       if (comp(sg, i) != -1) continue;
-      int tri = comp(nb, i);
-      int pTri = dtri(tri), pOri = dori(tri);
-      if (!(index < pTri || (pTri >= 0 && !M.tflip[pTri]))) continue;
-      int pOpp = ld1(M.tv, pTri, pOri);
-      if (is_red(M, pOpp) && pOpp < mn) continue;
-      double2 vOpp = M.pts[pOpp];
+      int pTri = eTri[i], pOri = eOri[i];
+      if (!(index < pTri || (pTri >= 0 && !eFlip[i]))) continue;
+      int pOpp = eOpp[i];
+      if (eRed[i] && pOpp < mn) continue;
+      double2 vOpp = eV[i];
       int org = m3(i + 1), dest = m3(i + 2), apex = i;
       if (mn != kMaxInt) {
         int deleteOri, n1, n2;
