@@ -715,7 +715,85 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(Job *jobs, const int *order,
     batch_body<0>(jobs, order, njobs, next, arenas, arena_stride, sh);
 }
 
+// ---------------------------------------------------------------------------
+// Small flip steps of the single-domain engine
+// ---------------------------------------------------------------------------
+// The single-domain flip-flop loop (refine.cu's flip graph: one launch per
+// step phase) spends most of its steps on small active sets: on the 2M-point
+// input three quarters of the steps have fewer than 2,048 triangles, where the
+// eight launches of a step cost more than the work.  This kernel runs in the
+// loop body after the step's condition kernel: while the next step's active
+// set has at most `limit` triangles, one block runs whole steps (the same
+// phases, compiled in block mode, separated by barriers), then it re-sets the
+// loop condition.  The steps and their results are the ones the grid kernels
+// would produce (every phase is decided by the reference's rules, not by the
+// thread layout).
+constexpr int kSmallThreads = 512;
+template <int PRED>
+__global__ void __launch_bounds__(kSmallThreads, 1)
+    k_flip_small(Mesh M, FlipCtl *fc, int *act, uint8_t *clr, int *win, int *ll, int *sl, int *fq, int *tl,
+                 int limit, cudaGraphConditionalHandle h, int graph) {
+  __shared__ int go;
+  for (;;) {
+    if (threadIdx.x == 0) go = fc->cond && fc->nact <= limit;
+    SYNC();
+    if (!go) break;
+    FlipQ Q{fq, &fc->qn, &fc->gen};
+    TouchL T{tl, &fc->tn, &fc->gen};
+    k_check_flip2<PRED>(M, act, &fc->nact, clr, T, &g_ktimer_off);
+    SYNC();
+    k_flip_winner2(M, act, &fc->nact, clr, Q, win, &fc->winn);
+    SYNC();
+    k_link_phase1(M, win, &fc->winn, ll, sl, &fc->epoch);
+    SYNC();
+    k_phase2(M, win, &fc->winn, ll, sl);
+    SYNC();
+    k_phase3q(M, win, &fc->winn, sl, Q);
+    SYNC();
+    k_mark_red_steiner_q(M, tl, &fc->tn, Q);
+    SYNC();
+    k_flip_reset_filter(M, tl, &fc->tn, fq, &fc->qn, act, &fc->nact_next);
+    SYNC();
+    if (threadIdx.x == 0) {
+      fc->nact = fc->nact_next;
+      fc->nact_next = 0;
+      fc->small_steps++;
+      flip_next(fc);
+    }
+    SYNC();
+  }
+#ifndef GQM_HOST_EMU
+  if (graph && threadIdx.x == 0) cudaGraphSetConditional(h, fc->cond);
+#endif
+  (void)h;
+  (void)graph;
+}
+
 }  // namespace gqm
+
+// Launch of k_flip_small on the single-domain engine's buffers (refine.cu).
+// mesh points at the caller's Mesh (the same layout in both compilations).
+int gqm_flip_small_launch(const void *mesh, size_t mesh_bytes, void *fc, int pred, int *act, uint8_t *clr, int *win,
+                          int *ll, int *sl, int *fq, int *tl, int limit, cudaStream_t st,
+                          cudaGraphConditionalHandle h, int graph) {
+  if (mesh_bytes != sizeof(gqm::Mesh)) return GQM_ERR_ARGUMENT;
+  gqm::Mesh M;
+  memcpy(&M, mesh, sizeof(M));
+  gqm::FlipCtl *c = static_cast<gqm::FlipCtl *>(fc);
+#ifdef GQM_HOST_EMU
+  (void)st;
+  if (pred)
+    gqm::k_flip_small<1>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph);
+  else
+    gqm::k_flip_small<0>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph);
+#else
+  if (pred)
+    gqm::k_flip_small<1><<<1, gqm::kSmallThreads, 0, st>>>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph);
+  else
+    gqm::k_flip_small<0><<<1, gqm::kSmallThreads, 0, st>>>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph);
+#endif
+  return GQM_OK;
+}
 
 // ===========================================================================
 // Host side

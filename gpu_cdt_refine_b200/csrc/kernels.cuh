@@ -861,6 +861,7 @@ struct FlipCtl {
   int qn;           // length of the next queue
   int tn;           // number of claimed triangles
   int steps;        // flip steps executed (all loops)
+  int small_steps;  // of which steps run by the single-block kernel (k_flip_small)
   int entry_steps;  // steps at entry of the current loop
   int cap_hit;      // the step bound stopped a loop
   int cond;         // loop condition of the last step
@@ -919,9 +920,6 @@ __device__ __forceinline__ int flip_next(FlipCtl *c) {
   c->cond = cond;
   return cond;
 }
-#ifdef GQM_HOST_EMU
-typedef int cudaGraphConditionalHandle;
-#endif
 GQM_KERNEL void k_flip_prep(FlipCtl *c, cudaGraphConditionalHandle h, int use_graph) {
   if (GQM_BLOCK0 && threadIdx.x == 0) {
     c->entry_steps = c->steps;
@@ -960,6 +958,7 @@ GQM_KERNEL void k_ctl_reset(FlipCtl *c, long long cap, int *errp) {
   }
   if (GQM_BLOCK0 && threadIdx.x == 0) {
     c->steps = 0;
+    c->small_steps = 0;
     c->entry_steps = 0;
     c->cap_hit = 0;
     c->cond = 0;

@@ -25,6 +25,11 @@
 #include "host_copy.h"
 #include "kernels.cuh"
 
+// batch.cu: the flip steps of small active sets in one block
+int gqm_flip_small_launch(const void *mesh, size_t mesh_bytes, void *fc, int pred, int *act, uint8_t *clr, int *win,
+                          int *ll, int *sl, int *fq, int *tl, int limit, cudaStream_t st,
+                          cudaGraphConditionalHandle h, int graph);
+
 namespace gqm {
 
 // ============================================================================
@@ -571,6 +576,11 @@ struct Refiner {
 #endif
   // grid of the flip-step kernels, whose item counts live on the device
   static constexpr int kStepGrid = GQM_STEP_GRID;
+  // steps whose active set has at most this many triangles run in one block
+#ifndef GQM_SMALL_STEP
+#define GQM_SMALL_STEP 2048
+#endif
+  static constexpr int kSmallStep = GQM_SMALL_STEP;
   void flip_body(cudaGraphConditionalHandle h, int graph) {
     FlipQ Q{fq, &fc->qn, &fc->gen};
     TouchL T{tl, &fc->tn, &fc->gen};
@@ -585,6 +595,8 @@ struct Refiner {
     KL(k_mark_red_steiner_q, kStepGrid, 256)(M, tl, &fc->tn, Q);
     KL(k_flip_reset_filter, kStepGrid, 256)(M, tl, &fc->tn, fq, &fc->qn, act, &fc->nact_next);
     KL(k_flip_cond, 1, 32)(fc, h, graph);
+    // the following small steps in one block (batch.cu), which re-sets the condition
+    gqm_flip_small_launch(&M, sizeof(M), fc, pred_mode, act, clr, win, ll, sl, fq, tl, kSmallStep, st, h, graph);
   }
   int build_flip_graph() {
 #ifdef GQM_HOST_EMU
@@ -695,7 +707,7 @@ struct Refiner {
       stats.host_syncs++;
       if (!hcount[C_MISC]) break;
       flip_body(h, 0);
-      stats.kernel_launches += 8;
+      stats.kernel_launches += 9;
     }
     return GQM_OK;
   }
@@ -1029,9 +1041,10 @@ struct Refiner {
     FlipCtl hf;
     cudaMemcpy(&hf, fc, sizeof(hf), cudaMemcpyDeviceToHost);
     stats.flip_steps = hf.steps;
-    // each graph launch counted one kernel (its loop-entry kernel); the eight
-    // kernels of every flip step it ran are added here
-    if (use_graph) stats.kernel_launches += 8LL * hf.steps;
+    // each graph launch counted one kernel (its loop-entry kernel); the nine
+    // kernels of every loop iteration it ran (a grid step, its condition and
+    // the single-block kernel that runs the small steps after it) are added here
+    if (use_graph) stats.kernel_launches += 9LL * (hf.steps - hf.small_steps);
     for (int b = 0; b < kFlipProfileBins; ++b) {
       flip_prof_steps[b] = (long long)hf.prof_steps[b];
       flip_prof_items[b] = (long long)hf.prof_items[b];

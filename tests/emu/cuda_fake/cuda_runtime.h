@@ -195,5 +195,6 @@ inline cudaError_t cudaGetSymbolAddress(void **p, T &sym) {
   return cudaSuccess;
 }
 typedef void *cudaGraph_t;
+typedef int cudaGraphConditionalHandle;
 typedef void *cudaGraphExec_t;
 inline cudaError_t cudaGraphLaunch(cudaGraphExec_t, cudaStream_t) { return 1; }
