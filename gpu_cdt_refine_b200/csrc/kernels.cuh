@@ -1685,30 +1685,30 @@ GQM_KERNEL void k_remove_losers(Mesh M, const int *bad, const int *dn, const int
 // the markers change, never the mesh or the centres, so its walk visits exactly
 // the triangles stored here (up to the first failure): checking the stored
 // list gives the same verdict without a second walk or any predicate.
+//
+// The reference rescans a triangle's three edges from the first every time the
+// walk comes back to it; the edges before the one it descended through were
+// then rejected (circumcircle test false, a subsegment or the boundary) or lead
+// to a triangle already in the region, and neither changes while the walk runs.
+// So each stack frame keeps the edge to resume at: the same triangles are
+// visited and claimed in the same order, each neighbour tested once.
 template <int PRED>
 __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, int badIndex, int *out,
                            int stride) {
-  int region[kCavityCap], loop[kCavityCap];
+  int region[kCavityCap], loop[kCavityCap];  // loop: (triangle << 2) | edge to resume at
   int rsize = 0, lsize = 0;
-  int cur = sink;
+  int cur = sink, start = 0;
   for (int guard = 0; guard < 4 * kCavityCap * 3 + 16; ++guard) {
-    bool found = false;
-    for (int i = 0; i < rsize; ++i)
-      if (region[i] == cur) {
-        found = true;
-        break;
-      }
-    if (!found) {
+    if (start == 0) {  // first visit (a return always resumes past the edge it left by)
       if (rsize == kCavityCap || lsize == kCavityCap) return -1;
       region[rsize++] = cur;
-      loop[lsize++] = cur;
+      loop[lsize++] = cur << 2;
       atomicMin(M.tmark + cur, badIndex);
     }
-    bool recursive = false;
-    int nIdx = -1;
+    int nIdx = -1, taken = -1;
     int4 sg = M.tsg[cur];
     int4 nb = M.tn[cur];
-    for (int i = 0; i < 3; i++) {
+    for (int i = start; i < 3; i++) {
       int si = comp(sg, i);
       if (cur == sink) {
         if (direction == 3 && si != -1) continue;
@@ -1717,30 +1717,34 @@ __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, i
         continue;
       int neighbor = comp(nb, i);
       if (neighbor == -1) continue;
-      nIdx = dtri(neighbor);
+      int t = dtri(neighbor);
       bool seen = false;
       for (int r = 0; r < rsize; ++r)
-        if (region[r] == nIdx) {
+        if (region[r] == t) {
           seen = true;
           break;
         }
       if (seen) continue;
-      int4 q = M.tv[nIdx];
+      int4 q = M.tv[t];
       double r = incircle<PRED>(M.pts[q.x], M.pts[q.y], M.pts[q.z], cc);
       if (r > 0) {
-        recursive = true;
+        nIdx = t;
+        taken = i;
         break;
       }
     }
-    if (recursive)
+    if (taken >= 0) {
+      loop[lsize - 1] = (cur << 2) | (taken + 1);
       cur = nIdx;
-    else {
+      start = 0;
+    } else {
       if (lsize > 0) lsize--;
       if (lsize == 0) {
         for (int j = 0; j < rsize; ++j) out[(long)j * stride] = region[j];
         return rsize;
       }
-      cur = loop[lsize - 1];
+      cur = loop[lsize - 1] >> 2;
+      start = loop[lsize - 1] & 3;
     }
   }
   raise_err(M, -6);

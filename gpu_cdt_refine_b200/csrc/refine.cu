@@ -87,10 +87,12 @@ __global__ void k_scan(int *bc, int nb, int *total) {
   if (threadIdx.x == 0) *total = carry;
 }
 // ordered emit: each thread takes 16 consecutive elements of a 4096-element
-// tile, a block-wide exclusive scan of the per-thread counts gives the slots
+// tile, a block-wide exclusive scan of the per-thread counts gives the slots.
+// With total set (a one-block compaction, bc pointing at a zero), the block
+// also writes the count, so a range of one block needs no count or scan launch.
 template <class F, class Mp>
 __global__ void __launch_bounds__(kCompactThreads) k_emit(F f, Mp m, int lo, int hi, int chunk, const int *bc,
-                                                          int *out) {
+                                                          int *out, int *total) {
   __shared__ int wsum[kCompactThreads / 32];
   int b0 = lo + blockIdx.x * chunk, b1 = min(hi, b0 + chunk);
   int base = bc[blockIdx.x];
@@ -126,6 +128,7 @@ __global__ void __launch_bounds__(kCompactThreads) k_emit(F f, Mp m, int lo, int
     base += tot;
     __syncthreads();
   }
+  if (total && threadIdx.x == 0) *total = base;
 }
 
 // predicates and maps for the compactions
@@ -371,6 +374,7 @@ struct Refiner {
         return GQM_ERR_MEMORY;
       cudaMemsetAsync(fc, 0, sizeof(FlipCtl), st);
       cudaMemsetAsync(ktm, 0, sizeof(KTimer), st);  // off until gqm_context_probe
+      cudaMemsetAsync(bc + kMaxCompactBlocks, 0, sizeof(int), st);  // the zero base of one-block compactions
 #ifdef GQM_HOST_EMU
       use_graph = false;
 #else
@@ -423,9 +427,14 @@ struct Refiner {
     int chunk = std::max(kCompactTile, (n + kMaxCompactBlocks - 1) / kMaxCompactBlocks);
     chunk = (chunk + kCompactTile - 1) / kCompactTile * kCompactTile;
     int nb = (n + chunk - 1) / chunk;
+    if (nb == 1) {  // one block: emit and count in one launch (bc[kMaxCompactBlocks] stays 0)
+      KL(k_emit, 1, kCompactThreads)(f, m, lo, hi, chunk, bc + kMaxCompactBlocks, out, dcnt);
+      stats.kernel_launches++;
+      return;
+    }
     KL(k_cnt, nb, kCompactThreads)(f, lo, hi, chunk, bc);
     KL(k_scan, 1, 1024)(bc, nb, dcnt);
-    KL(k_emit, nb, kCompactThreads)(f, m, lo, hi, chunk, bc, out);
+    KL(k_emit, nb, kCompactThreads)(f, m, lo, hi, chunk, bc, out, nullptr);
     stats.kernel_launches += 3;
   }
   int fetch(int slot) {

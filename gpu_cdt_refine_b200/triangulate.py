@@ -118,7 +118,8 @@ def release() -> None:
 
 def main(argv=None):
     """Builds the CDT of the clustered benchmark input on the GPU and prints
-    the builder's statistics (one JSON line per build)."""
+    the builder's statistics (one JSON line per build); with --theta, also
+    refines it in the same call (gqm_triangulate_refine) and prints both."""
     import argparse
     import json
     import time
@@ -130,14 +131,20 @@ def main(argv=None):
     p.add_argument("--seed", type=int, default=20261205)
     p.add_argument("--repeat", type=int, default=1)
     p.add_argument("--device", type=int, default=0)
+    p.add_argument("--theta", type=float, default=0.0, help="also refine at this angle (degrees)")
     a = p.parse_args(argv)
     pts = inputs.cluster_points(a.points, 64, 1.0e4, 5.0, 200.0, 0.10, a.seed)
     seg = inputs.pick_segments(pts, a.segments, a.seed + 1)
     for _ in range(a.repeat):
         t0 = time.perf_counter()
-        cdt, st = build_cdt_gpu(pts, seg, device=a.device, with_stats=True)
+        if a.theta > 0:
+            out, rst, st = triangulate_refine(pts, seg, theta=a.theta, device=a.device)
+            st["refine"] = rst
+            st["triangles"] = out.numberoftriangles
+        else:
+            cdt, st = build_cdt_gpu(pts, seg, device=a.device, with_stats=True)
+            st["triangles"] = cdt.numberoftriangles
         st["wall_ms"] = (time.perf_counter() - t0) * 1e3
-        st["triangles"] = cdt.numberoftriangles
         print(json.dumps(st), flush=True)
 
 
