@@ -53,6 +53,8 @@ CHECK_BYTES_PER_ITEM = 4 + 36 + 3 + 48 + 66 + 1
 # `ncu --set full` on its first launch of the 1,000,000-point clustered case
 # (profiles/k_check_flip2_clustered1M.md: 74.59 MB for 162,684 triangles).
 CHECK_DRAM_BYTES_PER_ITEM = 74.59e6 / 162684
+# timed Triangle runs of the CPU baseline (about 2 s each on the 1/4 sample)
+CPU_RUNS = 6
 
 
 def parse():
@@ -154,10 +156,10 @@ def measured_peak():
 
 def cpu_sample(args):
     """Bounded sample of the workload for the CPU legs: the same generator at
-    1/8 of the points and segments (Triangle needs ~40 s for the full 2M-point
-    input on one core)."""
+    1/4 of the points and segments, about 2 s per Triangle run on one core
+    (Triangle needs ~40 s for the full 2M-point input)."""
     from gpu_cdt_refine_b200 import inputs
-    return inputs.clustered(seed=args.seed + 7, n=max(args.points // 8, 1000), nseg=max(args.segments // 8, 50))
+    return inputs.clustered(seed=args.seed + 7, n=max(args.points // 4, 1000), nseg=max(args.segments // 4, 50))
 
 
 def run_batch_workload(args, local_rank):
@@ -325,7 +327,7 @@ def run_reference(args, rank, world):
             "config": config(args, full),
             "cpu_baseline": {"value": tps, "unit": "triangles/s", "cores": 1, "kind": "reference",
                              "sample": f"Triangle 1.6 pzDQnrq20 (single-threaded, as vendored by the reference) on "
-                                       f"a 1/8 sample of the workload ({cdt.numberofpoints} points, "
+                                       f"a 1/4 sample of the workload ({cdt.numberofpoints} points, "
                                        f"{cdt.numberofsegments} segments) per step"},
             "e2e": {"value": tps, "unit": "triangles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "output_triangles": nt}
@@ -442,11 +444,14 @@ def run_ours(args, rank, world, local_rank):
             line["adversarial"] = run_adversarial(local_rank)
         if args.cpu_baseline and world == 1:
             try:
+                from oracle import tri_ref
                 smp = cpu_sample(args)
-                tps, times, ntc = time_triangle(smp, 2)
+                tri_ref.quality(smp, 20.0, 1)  # warm-up run, untimed
+                tps, times, ntc = time_triangle(smp, CPU_RUNS)
                 line["cpu_baseline"] = {"value": tps, "unit": "triangles/s", "cores": 1, "kind": "reference",
-                                        "sample": f"Triangle 1.6 pzDQnrq20 on a 1/8 sample of the workload "
-                                                  f"({smp.numberofpoints} points), 2 runs",
+                                        "sample": f"Triangle 1.6 pzDQnrq20 on a 1/4 sample of the workload "
+                                                  f"({smp.numberofpoints} points), {CPU_RUNS} timed runs, "
+                                                  f"{sum(times) / 1e3:.1f} s of CPU work",
                                         "output_triangles": ntc}
             except Exception as e:  # the reference build is test infrastructure; report, do not fail
                 line["cpu_baseline"] = {"value": None, "unit": "triangles/s", "cores": 1, "kind": "reference",
