@@ -186,6 +186,10 @@ def run_batch_workload(args, local_rank):
     for i in samp:
         refine.refine(doms[i], thetas[i], device=local_rank)
     single_ms = (time.perf_counter() - t0) * 1e3 * n / len(samp)
+    try:
+        cpu = batch_cpu_baseline(doms, thetas) if args.cpu_baseline else None
+    except Exception as e:  # the reference build is test infrastructure; report, do not fail
+        cpu = {"value": None, "unit": "triangles/s", "kind": "reference", "sample": f"unavailable: {e}"}
     return {"workload": f"{n} independent domains, N log-uniform [200, 50000], uniform or 1-8 Gaussian clusters, "
                         f"segments 5% of N, theta in {{15, 18, 20}}, Ruppert, Offcenter",
             "domains": n, "points_in": int(sum(d.numberofpoints for d in doms)), "output_triangles": int(tris),
@@ -195,7 +199,51 @@ def run_batch_workload(args, local_rank):
             "per_domain_calls_ms": single_ms,
             "per_domain_sample": f"{len(samp)} seeded domains, one gqm_refine call each (host arrays in and out), "
                                  f"time scaled by {n}/{len(samp)}",
-            "generation_s": gen_s}
+            "cpu_baseline": cpu, "generation_s": gen_s}
+
+
+def _triangle_worker(ids, seed, barrier, out):
+    """One host core of the batch's CPU baseline: builds its domains (untimed),
+    waits for the other workers, then refines its domains one after another
+    with Triangle -q and reports (output triangles, seconds).  Triangle keeps
+    its state in globals, so each core is a process of its own."""
+    from gpu_cdt_refine_b200 import inputs
+    from oracle import tri_ref
+    work = [inputs.batch_domain(seed + 2 * k) for k in ids]
+    barrier.wait()
+    t0 = time.perf_counter()
+    tris = 0
+    for cdt, theta in work:
+        tris += tri_ref.quality(cdt, theta, 1)[1]
+    out.put((tris, time.perf_counter() - t0, sum(c.numberofpoints for c, _ in work)))
+
+
+def batch_cpu_baseline(doms, thetas, seed=20261207):
+    """Triangle's quality refinement (pzDQnrq<theta>, the reference's CPU path)
+    of every domain of the batch on all host cores: one spawned process per
+    core (no CUDA state is inherited), domains assigned by the same
+    cost-balanced partition as the multi-GPU batch, all workers released
+    together; triangles/s = output triangles / the slowest worker's time."""
+    import multiprocessing as mp
+    from gpu_cdt_refine_b200 import replicas
+    cores = max(1, min(os.cpu_count() or 1, len(doms)))
+    parts, _ = replicas.partition_domains([replicas.domain_cost(d.numberofpoints, t) for d, t in zip(doms, thetas)],
+                                          cores)
+    ctx = mp.get_context("spawn")
+    barrier, out = ctx.Barrier(cores), ctx.Queue()
+    procs = [ctx.Process(target=_triangle_worker, args=(p, seed, barrier, out)) for p in parts]
+    for p in procs:
+        p.start()
+    res = [out.get(timeout=900) for _ in procs]
+    for p in procs:
+        p.join()
+    tris, wall = sum(r[0] for r in res), max(r[1] for r in res)
+    if sum(r[2] for r in res) != sum(d.numberofpoints for d in doms):
+        raise RuntimeError("the workers' domains differ from the batch")
+    return {"value": tris / wall, "unit": "triangles/s", "cores": cores, "kind": "reference",
+            "sample": f"Triangle 1.6 pzDQnrq<theta> on all {len(doms)} domains of the batch, one process per core, "
+                      f"{wall:.1f} s wall (slowest core), {sum(r[1] for r in res):.1f} s of CPU work",
+            "output_triangles": int(tris), "wall_ms": wall * 1e3}
 
 
 def run_adversarial(local_rank):
