@@ -210,7 +210,7 @@ def _triangle_worker(ids, seed, barrier, out):
     from gpu_cdt_refine_b200 import inputs
     from oracle import tri_ref
     work = [inputs.batch_domain(seed + 2 * k) for k in ids]
-    barrier.wait()
+    barrier.wait(timeout=300)
     t0 = time.perf_counter()
     tris = 0
     for cdt, theta in work:
@@ -231,12 +231,16 @@ def batch_cpu_baseline(doms, thetas, seed=20261207):
                                           cores)
     ctx = mp.get_context("spawn")
     barrier, out = ctx.Barrier(cores), ctx.Queue()
-    procs = [ctx.Process(target=_triangle_worker, args=(p, seed, barrier, out)) for p in parts]
+    procs = [ctx.Process(target=_triangle_worker, args=(p, seed, barrier, out), daemon=True) for p in parts]
     for p in procs:
         p.start()
-    res = [out.get(timeout=900) for _ in procs]
-    for p in procs:
-        p.join()
+    try:
+        res = [out.get(timeout=600) for _ in procs]
+    finally:  # a worker that failed leaves no process behind
+        for p in procs:
+            p.join(timeout=10)
+            if p.is_alive():
+                p.terminate()
     tris, wall = sum(r[0] for r in res), max(r[1] for r in res)
     if sum(r[2] for r in res) != sum(d.numberofpoints for d in doms):
         raise RuntimeError("the workers' domains differ from the batch")
