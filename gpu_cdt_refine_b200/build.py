@@ -49,13 +49,14 @@ def build_host(force=False):
 def build_cuda(force=False, extra=None):
     out = os.path.join(HERE, "libgqm_b200.so")
     hdr = [os.path.join(INC, "gqm_refine.h"), os.path.join(INC, "gqm_triangulateio.h"),
-           os.path.join(CSRC, "predicates.h")]
+           os.path.join(CSRC, "predicates.h"), os.path.join(CSRC, "host_copy.h")]
     refiner = [os.path.join(CSRC, f) for f in ("kernels.cuh", "gqm_device.cuh", "learned.cuh")]
     units = {  # translation unit -> the headers it includes
         "refine.cu": hdr + refiner,
         "batch.cu": hdr + refiner,
         "learned.cu": hdr + [os.path.join(CSRC, "learned.cuh")],
-        "cdt_gpu.cu": [os.path.join(INC, "gqm_cdt.h"), os.path.join(CSRC, "predicates.h")],
+        "cdt_gpu.cu": [os.path.join(INC, "gqm_cdt.h"), os.path.join(CSRC, "predicates.h"),
+                       os.path.join(CSRC, "host_copy.h")],
         "legacy.cpp": hdr,
     }
     flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler",

@@ -1634,6 +1634,8 @@ int Builder::download(gqm_cdt_result *res, gqm_cdt_gpu_stats *sts) {
   res->neighborlist = (int *)malloc(bt + 8);
   res->segmentlist = (int *)malloc(bs + 8);
   if (!res->trianglelist || !res->neighborlist || !res->segmentlist) return GQM_CDT_ERR_MEMORY;
+  advise_huge(res->trianglelist, bt);
+  advise_huge(res->neighborlist, bt);
   if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_CDT_ERR_CUDA;
   host_copy({{res->trianglelist, stage, bt}, {res->neighborlist, stage + bt, bt}, {res->segmentlist, stage + 2 * bt, bs}});
   if (sts) {

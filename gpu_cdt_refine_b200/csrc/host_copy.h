@@ -1,7 +1,10 @@
 // Host memcpy of a few large arrays on the host's cores (staging to and from
 // pinned memory): every copy is cut into pieces of 8 MB shared by the threads.
 #pragma once
+#include <sys/mman.h>
+
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <initializer_list>
 #include <thread>
@@ -30,4 +33,17 @@ static inline void host_copy(std::initializer_list<HostCopy> list) {
       for (size_t k = t; k < pieces.size(); k += nt) memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
     });
   for (auto &th : pool) th.join();
+}
+
+// Transparent huge pages for a large host array that has not been touched yet
+// (a result array just allocated): the first-touch page faults of the copies
+// into it then come in 2 MB steps instead of 4 KB ones, which roughly halves
+// the time of unpacking a result of a few hundred MB.  Only the page-aligned
+// interior is advised; the call is a hint and its failure is harmless.
+static inline void advise_huge(void *p, size_t bytes) {
+  constexpr size_t kMin = 4u << 20;
+  if (!p || bytes < kMin) return;
+  const uintptr_t a = ((uintptr_t)p + 4095) & ~(uintptr_t)4095;
+  const uintptr_t e = ((uintptr_t)p + bytes) & ~(uintptr_t)4095;
+  if (e > a) madvise((void *)a, e - a, MADV_HUGEPAGE);
 }

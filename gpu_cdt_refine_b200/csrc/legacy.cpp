@@ -6,6 +6,7 @@
 
 #include "../../include/gqm_refine.h"
 #include "../../include/gqm_triangulateio.h"
+#include "host_copy.h"
 
 void GPU_Refine_Quality(triangulateio *input, triangulateio *result, double theta, InsertPolicy insertpolicy,
                         DeletePolicy /*deletepolicy*/, int mode, int /*debug_iter*/, PStatus **ps_debug,
@@ -39,24 +40,28 @@ void GPU_Refine_Quality(triangulateio *input, triangulateio *result, double thet
     fprintf(stderr, "GPU_Refine_Quality: %s (status %d)\n", gqm_status_string(rc), rc);
     return;
   }
+  // new[] arrays as the reference hands them out, filled on the host's cores
+  const size_t np = (size_t)out.numberofpoints, nt = (size_t)out.numberoftriangles, ns = (size_t)out.numberofsegments;
   result->numberofpoints = out.numberofpoints;
-  result->pointlist = new double[2 * (size_t)out.numberofpoints];
-  memcpy(result->pointlist, out.pointlist, sizeof(double) * 2 * (size_t)out.numberofpoints);
+  result->pointlist = new double[2 * np];
   result->numberoftriangles = out.numberoftriangles;
-  result->trianglelist = new int[3 * (size_t)out.numberoftriangles];
-  memcpy(result->trianglelist, out.trianglelist, sizeof(int) * 3 * (size_t)out.numberoftriangles);
-  result->neighborlist = new int[3 * (size_t)out.numberoftriangles];
-  memcpy(result->neighborlist, out.neighborlist, sizeof(int) * 3 * (size_t)out.numberoftriangles);
+  result->trianglelist = new int[3 * nt];
+  result->neighborlist = new int[3 * nt];
   result->numberofsegments = out.numberofsegments;
-  result->segmentlist = new int[2 * (size_t)out.numberofsegments];
-  memcpy(result->segmentlist, out.segmentlist, sizeof(int) * 2 * (size_t)out.numberofsegments);
+  result->segmentlist = new int[2 * ns];
+  advise_huge(result->pointlist, 16 * np);
+  advise_huge(result->trianglelist, 12 * nt);
+  advise_huge(result->neighborlist, 12 * nt);
+  host_copy({{result->pointlist, out.pointlist, 16 * np}, {result->trianglelist, out.trianglelist, 12 * nt},
+             {result->neighborlist, out.neighborlist, 12 * nt}, {result->segmentlist, out.segmentlist, 8 * ns}});
+  static_assert(sizeof(PStatus) == 1 && sizeof(TStatus) == 1, "one status byte per point and triangle");
   if (ps_debug) {
-    *ps_debug = new PStatus[out.numberofpoints];
-    for (int i = 0; i < out.numberofpoints; ++i) (*ps_debug)[i]._status = out.pstatus[i];
+    *ps_debug = new PStatus[np];
+    memcpy(*ps_debug, out.pstatus, np);
   }
   if (ts_debug) {
-    *ts_debug = new TStatus[out.numberoftriangles];
-    for (int i = 0; i < out.numberoftriangles; ++i) (*ts_debug)[i]._status = out.tstatus[i];
+    *ts_debug = new TStatus[nt];
+    memcpy(*ts_debug, out.tstatus, nt);
   }
   gqm_free_result(&out);
 }

@@ -1096,6 +1096,10 @@ struct Refiner {
     out->segmentlist = (int *)malloc(sizeof(int) * 2 * (size_t)ns + 16);
     out->pstatus = (unsigned char *)malloc((size_t)np + 16);
     out->tstatus = (unsigned char *)malloc((size_t)nt + 16);
+    advise_huge(out->pointlist, 16 * (size_t)np);
+    advise_huge(out->trianglelist, 12 * (size_t)nt);
+    advise_huge(out->neighborlist, 12 * (size_t)nt);
+    advise_huge(out->tstatus, (size_t)nt);
     const cudaError_t ce = cudaStreamSynchronize(st);
     if (ce != cudaSuccess || !out->pointlist || !out->trianglelist || !out->neighborlist || !out->segmentlist ||
         !out->pstatus || !out->tstatus) {
