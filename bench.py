@@ -51,8 +51,8 @@ METRIC = "output triangles/s at theta=20 deg, 1 B200 (learned vs plain); output 
 CHECK_BYTES_PER_ITEM = 4 + 36 + 3 + 48 + 66 + 1
 # DRAM bytes (read + write) per active triangle of the same kernel, from
 # `ncu --set full` on its first launch of the 1,000,000-point clustered case
-# (profiles/k_check_flip2_clustered1M.md: 74.59 MB for 162,684 triangles).
-CHECK_DRAM_BYTES_PER_ITEM = 74.59e6 / 162684
+# (profiles/k_check_flip2_clustered1M.md: 72.92 MB for 162,684 triangles).
+CHECK_DRAM_BYTES_PER_ITEM = 72.92e6 / 162684
 # timed Triangle runs of the CPU baseline (about 2 s each on the 1/4 sample)
 CPU_RUNS = 6
 
