@@ -53,6 +53,13 @@ CHECK_BYTES_PER_ITEM = 4 + 36 + 3 + 48 + 66 + 1
 # `ncu --set full` on its first launch of the 1,000,000-point clustered case
 # (profiles/k_check_flip2_clustered1M.md: 72.92 MB for 162,684 triangles).
 CHECK_DRAM_BYTES_PER_ITEM = 72.92e6 / 162684
+# FP64-pipe utilisation of the same launch (sm__inst_executed_pipe_fp64, % of
+# peak sustained active): the exact-predicate filters are a small part of its work.
+CHECK_FP64_PIPE_PCT = 4.36
+# Shares of the device time of one refinement of the 2M-point input in the ncu
+# launch list (profiles/launches_clustered2M.md): the check kernel and the
+# single-block kernel that runs the flip steps of at most 2,048 triangles.
+LAUNCH_LIST_SHARES = {"k_flip_small": 0.230, "k_check_flip2": 0.209, "k_cavity_mark": 0.084, "k_phase3q": 0.082}
 # timed Triangle runs of the CPU baseline (about 2 s each on the 1/4 sample)
 CPU_RUNS = 6
 
@@ -486,7 +493,13 @@ def run_ours(args, rank, world, local_rank):
                              "first_launch_items": probe["first_items"],
                              "timing": "per-launch device timer (%globaltimer, first block start to last block "
                                        "end) in one extra probed step after the timed region",
-                             "path_achieved_gbs": path_gbs, "path_frac": path_gbs / peak},
+                             "path_achieved_gbs": path_gbs, "path_frac": path_gbs / peak,
+                             "fp64_pipe_pct_ncu": CHECK_FP64_PIPE_PCT,
+                             "launch_list_shares_ncu": LAUNCH_LIST_SHARES,
+                             "note": "k_flip_small (one thread block running whole flip steps of at most 2,048 "
+                                     "triangles) holds a slightly larger share than k_check_flip2; as a "
+                                     "single block it is latency bound by construction, so the roofline is "
+                                     "reported for the dominant grid-wide kernel"},
                 "clocks": clk.summary(), "input_generation_s": gen_s}
         if args.batch_domains > 0 and world == 1:
             line["batch"] = run_batch_workload(args, local_rank)
