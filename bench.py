@@ -153,6 +153,19 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def cpu_model():
+    """The host CPU's model name and logical core count, reported beside every CPU baseline."""
+    name = "unknown"
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                name = line.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{name}, {os.cpu_count()} logical cores"
+
+
 def measured_peak():
     try:
         d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -251,7 +264,7 @@ def batch_cpu_baseline(doms, thetas, seed=20261207):
     tris, wall = sum(r[0] for r in res), max(r[1] for r in res)
     if sum(r[2] for r in res) != sum(d.numberofpoints for d in doms):
         raise RuntimeError("the workers' domains differ from the batch")
-    return {"value": tris / wall, "unit": "triangles/s", "cores": cores, "kind": "reference",
+    return {"value": tris / wall, "unit": "triangles/s", "cores": cores, "kind": "reference", "host": cpu_model(),
             "sample": f"Triangle 1.6 pzDQnrq<theta> on all {len(doms)} domains of the batch, one process per core, "
                       f"{wall:.1f} s wall (slowest core), {sum(r[1] for r in res):.1f} s of CPU work",
             "output_triangles": int(tris), "wall_ms": wall * 1e3}
@@ -384,7 +397,7 @@ def run_reference(args, rank, world):
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)", "impl": "reference",
             "config": config(args, full),
-            "cpu_baseline": {"value": tps, "unit": "triangles/s", "cores": 1, "kind": "reference",
+            "cpu_baseline": {"value": tps, "unit": "triangles/s", "cores": 1, "kind": "reference", "host": cpu_model(),
                              "sample": f"Triangle 1.6 pzDQnrq20 (single-threaded, as vendored by the reference) on "
                                        f"a 1/4 sample of the workload ({cdt.numberofpoints} points, "
                                        f"{cdt.numberofsegments} segments) per step"},
@@ -514,7 +527,7 @@ def run_ours(args, rank, world, local_rank):
                 tri_ref.quality(smp, 20.0, 1)  # warm-up run, untimed
                 tps, times, ntc = time_triangle(smp, CPU_RUNS)
                 line["cpu_baseline"] = {"value": tps, "unit": "triangles/s", "cores": 1, "kind": "reference",
-                                        "sample": f"Triangle 1.6 pzDQnrq20 on a 1/4 sample of the workload "
+                                        "host": cpu_model(), "sample": f"Triangle 1.6 pzDQnrq20 on a 1/4 sample of the workload "
                                                   f"({smp.numberofpoints} points), {CPU_RUNS} timed runs, "
                                                   f"{sum(times) / 1e3:.1f} s of CPU work",
                                         "output_triangles": ntc}
