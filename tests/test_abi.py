@@ -3,6 +3,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 from gpu_cdt_refine_b200 import _native
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -34,3 +36,49 @@ def test_status_strings_and_no_device_error():
     L = refine.lib()
     assert L.gqm_status_string(0) == b"ok"
     assert L.gqm_version() >= 100
+
+
+def _bad_call(case):
+    """gqm_refine on a small valid CDT with one argument made invalid."""
+    from gpu_cdt_refine_b200 import inputs, refine
+    L = refine.lib()
+    cdt = inputs.plain_small(seed=11, n=200, nseg=10)
+    keep = []
+    cin = refine._cdt_in(cdt, keep)
+    opt = refine.make_options(20.0, refine.Offcenter, 1)
+    if case == "few_points":
+        cin.numberofpoints = 2
+    elif case == "no_triangles":
+        cin.numberoftriangles = 0
+    elif case == "negative_segments":
+        cin.numberofsegments = -1
+    elif case == "null_points":
+        cin.pointlist = None
+    elif case == "null_neighbours":
+        cin.neighborlist = None
+    elif case == "null_segments":
+        cin.segmentlist = None
+    elif case in ("theta_zero", "theta_60", "theta_nan"):
+        opt.theta = {"theta_zero": 0.0, "theta_60": 60.0, "theta_nan": float("nan")}[case]
+    elif case == "negative_area":
+        opt.max_area = -1.0
+    elif case == "learned_without_network":
+        opt.placement = refine.PLACE_LEARNED
+        opt.mlp = None
+    out = refine.CdtOut()
+    if case == "null_input":
+        return L.gqm_refine(None, ctypes.byref(out), ctypes.byref(opt), None)
+    if case == "null_output":
+        return L.gqm_refine(ctypes.byref(cin), None, ctypes.byref(opt), None)
+    rc = L.gqm_refine(ctypes.byref(cin), ctypes.byref(out), ctypes.byref(opt), None)
+    assert not out.pointlist and not out.trianglelist  # nothing handed out on an error
+    return rc
+
+
+@pytest.mark.parametrize("case", ["null_input", "null_output", "few_points", "no_triangles", "negative_segments",
+                                  "null_points", "null_neighbours", "null_segments", "theta_zero", "theta_60",
+                                  "theta_nan", "negative_area", "learned_without_network"])
+def test_refine_rejects_invalid_arguments_before_touching_a_device(case):
+    """Argument checks run on the host before any CUDA call, so they answer the
+    same on a machine without a GPU: GQM_ERR_ARGUMENT, and no output arrays."""
+    assert _bad_call(case) == -1
