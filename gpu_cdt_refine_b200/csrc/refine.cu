@@ -913,7 +913,11 @@ struct Refiner {
       if (need > dinput_bytes) {
         if (dinput) cudaFree(dinput);
         dinput = nullptr;
-        if (cudaMalloc((void **)&dinput, need) != cudaSuccess) return GQM_ERR_MEMORY;
+        dinput_bytes = 0;
+        if (cudaMalloc((void **)&dinput, need) != cudaSuccess) {
+          dinput = nullptr;
+          return GQM_ERR_MEMORY;
+        }
         dinput_bytes = need;
       }
       char *base = (char *)dinput;
@@ -974,16 +978,16 @@ struct Refiner {
     {
       unsigned hsz = 1;
       while (hsz < 2u * (unsigned)ns + 16) hsz <<= 1;
-      if (hsz > hash_cap) {
-        if (grow_dev(&hkeys, &hash_cap, hsz)) return GQM_ERR_MEMORY;
-        size_t c2 = 0;
+      if (hsz > hash_cap) {  // the three tables share one capacity, set once all three exist
+        hash_cap = 0;
+        size_t c0 = 0, c1 = 0, c2 = 0;
         if (hvals) cudaFree(hvals);
-        hvals = nullptr;
-        if (grow_dev(&hvals, &c2, hsz)) return GQM_ERR_MEMORY;
-        c2 = 0;
         if (s2ti) cudaFree(s2ti);
+        hvals = nullptr;
         s2ti = nullptr;
-        if (grow_dev(&s2ti, &c2, hsz)) return GQM_ERR_MEMORY;
+        if (grow_dev(&hkeys, &c0, hsz) || grow_dev(&hvals, &c1, hsz) || grow_dev(&s2ti, &c2, hsz))
+          return GQM_ERR_MEMORY;
+        hash_cap = hsz;
       }
       cudaMemsetAsync(hkeys, 0xff, sizeof(unsigned long long) * hsz, st);
       cudaMemsetAsync(s2ti, 0xff, sizeof(int) * (ns + 1), st);

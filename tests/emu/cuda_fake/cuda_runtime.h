@@ -126,7 +126,21 @@ enum { cudaSuccess = 0, cudaErrorMemoryAllocation = 2 };
 enum cudaMemcpyKind { cudaMemcpyHostToDevice, cudaMemcpyDeviceToHost, cudaMemcpyDeviceToDevice };
 #define cudaStreamNonBlocking 1
 
+// Fault injection for the CPU tests: allocation number `fail_at` (counted
+// from the last gqm_fake_fail_alloc_at call, device and pinned allocations
+// together) fails as an out-of-memory would; -1 turns it off.
+inline long long g_fake_fail_at = -1;
+inline long long g_fake_allocs = 0;
+extern "C" __attribute__((weak)) void gqm_fake_fail_alloc_at(long long fail_at) {
+  g_fake_fail_at = fail_at;
+  g_fake_allocs = 0;
+}
+extern "C" __attribute__((weak)) long long gqm_fake_alloc_count(void) { return g_fake_allocs; }
 inline cudaError_t cudaMalloc(void **p, size_t n) {
+  if (g_fake_allocs++ == g_fake_fail_at) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
   *p = calloc(1, n ? n : 1);
   return *p ? cudaSuccess : cudaErrorMemoryAllocation;
 }
