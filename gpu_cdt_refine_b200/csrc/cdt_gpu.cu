@@ -1261,6 +1261,7 @@ struct Builder {
     Q = nullptr;
     Bd = nullptr;
     long c = std::max(n, 2 * cap_scratch);
+    cap_scratch = 0;  // set again only once all three exist
     if (dalloc(&R, c) || dalloc(&Q, c) || dalloc(&Bd, c)) return GQM_CDT_ERR_MEMORY;
     cap_scratch = c;
     return 0;
@@ -1568,6 +1569,7 @@ int Builder::build(int np, const double *pts, int ns, const int *segs, gqm_cdt_g
   if (need > out_cap) {
     if (out) cudaFree(out);
     out = nullptr;
+    out_cap = 0;
     if (dalloc(&out, need)) return GQM_CDT_ERR_MEMORY;
     out_cap = need;
   }

@@ -136,3 +136,48 @@ def test_allocation_failure_in_the_persistent_batch(emulated):  # noqa: F811
             for f in FIELDS:
                 assert np.array_equal(getattr(g, f).view(np.uint8), getattr(w, f).view(np.uint8)), (k, f)
     L.gqm_batch_release(0)
+
+
+def test_allocation_failure_in_the_cdt_builder(emulated):  # noqa: F811
+    """The GPU CDT builder's buffers are released and each of its allocations
+    fails in turn (first build, then the growth for a larger input): the call
+    reports GQM_CDT_ERR_MEMORY, and the next call builds the same mesh as
+    before."""
+    from gpu_cdt_refine_b200 import cdtio, triangulate
+    L = refine.lib()
+    L.gqm_fake_fail_alloc_at.argtypes = [ctypes.c_longlong]
+    L.gqm_fake_alloc_count.restype = ctypes.c_longlong
+    cdt_err_memory = -11
+    cases = []
+    for seed, n in ((65, 400), (66, 1500)):
+        pts = inputs.uniform_points(n, 0.0, 1000.0, seed)
+        seg = inputs.pick_segments(pts, n // 25, seed + 1)
+        cases.append((pts, seg, inputs.build_cdt(pts, seg)))
+
+    def build(i):
+        pts, seg, _ = cases[i]
+        return triangulate.build_cdt_gpu(pts, seg)
+
+    for grow in (False, True):
+        triangulate._bind().gqm_cdt_gpu_release()
+        if grow:
+            L.gqm_fake_fail_alloc_at(-1)
+            build(0)
+        L.gqm_fake_fail_alloc_at(-1)
+        build(1)
+        total = L.gqm_fake_alloc_count()
+        assert total >= 3
+        for k in range(total):
+            triangulate._bind().gqm_cdt_gpu_release()
+            if grow:
+                L.gqm_fake_fail_alloc_at(-1)
+                build(0)
+            L.gqm_fake_fail_alloc_at(k)
+            with pytest.raises(triangulate.CdtBuildError) as e:
+                build(1)
+            assert e.value.status == cdt_err_memory, (grow, k, e.value.status)
+            L.gqm_fake_fail_alloc_at(-1)
+            for i in (0, 1):  # the smaller input first: it must not reuse a buffer that was not reallocated
+                assert cdtio.same_mesh(build(i), cases[i][2]), (grow, k, i)
+    triangulate._bind().gqm_cdt_gpu_release()
+    L.gqm_fake_fail_alloc_at(-1)
