@@ -181,3 +181,4 @@ def test_allocation_failure_in_the_cdt_builder(emulated):  # noqa: F811
                 assert cdtio.same_mesh(build(i), cases[i][2]), (grow, k, i)
     triangulate._bind().gqm_cdt_gpu_release()
     L.gqm_fake_fail_alloc_at(-1)
+

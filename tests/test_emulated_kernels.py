@@ -209,3 +209,17 @@ def test_emulated_domain_with_hole(emulated):
     assert not np.any((cen[:, 0] > 0.35) & (cen[:, 0] < 0.65) & (cen[:, 1] > 0.35) & (cen[:, 1] < 0.65))
     cert = certify(got, cdt, 20.0)
     assert cert["ok"] and cert["triangles_below_theta"] == 0, cert
+
+
+def test_sharded_batch_default_engine_single_rank(emulated):
+    """replicas.refine_batch_sharded with its default engine (the persistent
+    batch engine on this rank's device) and no process group: one rank holds
+    every domain, and each result is the oracle's."""
+    from gpu_cdt_refine_b200 import replicas
+    doms = [inputs.plain_small(seed=67 + i, n=n, nseg=max(4, n // 25)) for i, n in enumerate((300, 500))]
+    got, stats, rep = replicas.refine_batch_sharded(doms, [18.0, 20.0])
+    assert rep["domains"] == [2] and len(stats) == 2
+    for d, t, g in zip(doms, (18.0, 20.0), got):
+        want, _ = oracle_py.refine(d, t, 1, 1)
+        for f in FIELDS:
+            assert np.array_equal(getattr(g, f).view(np.uint8), getattr(want, f).view(np.uint8)), f
