@@ -64,7 +64,7 @@ def _shard_domains():
     return doms, [15.0, 20.0, 18.0, 20.0, 15.0, 18.0]
 
 
-def _shard_worker(rank, world, port, out):
+def _shard_worker(rank, world, port, out, count=None):
     import pickle
 
     import torch.distributed as dist
@@ -73,6 +73,7 @@ def _shard_worker(rank, world, port, out):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         doms, thetas = _shard_domains()
+        doms, thetas = doms[:count], thetas[:count]
         res, stats, rep = replicas.refine_batch_sharded(doms, thetas, engine=_oracle_engine)
         ids, own, _, rep2 = replicas.refine_batch_sharded(doms, thetas, engine=_oracle_engine, gather=False)
         out[rank] = pickle.dumps((res, stats, rep, ids, own, rep2))
@@ -111,3 +112,20 @@ def test_batch_sharded_single_process():
     want, _ = _oracle_engine(doms[:3], thetas[:3])
     assert rep["domains"] == [3]
     assert all(a.numberoftriangles == b.numberoftriangles for a, b in zip(res, want))
+
+
+def test_batch_sharded_rank_without_domains():
+    """One domain over two ranks: the rank that receives none takes part in
+    the timing reduction and the gather, and rank 0 returns the one result."""
+    import pickle
+    mgr = mp.Manager()
+    out = mgr.dict()
+    port = 29900 + (os.getpid() % 1000)
+    mp.spawn(_shard_worker, args=(2, port, out, 1), nprocs=2, join=True)
+    doms, thetas = _shard_domains()
+    want, _ = _oracle_engine(doms[:1], thetas[:1])
+    res0, _, rep0, ids0, _, _ = pickle.loads(out[0])
+    res1, _, rep1, ids1, _, _ = pickle.loads(out[1])
+    assert sorted(rep0["domains"]) == [0, 1] and res1 is None
+    assert sorted(ids0 + ids1) == [0]
+    assert len(res0) == 1 and res0[0].numberoftriangles == want[0].numberoftriangles
