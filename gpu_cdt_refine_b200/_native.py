@@ -52,6 +52,13 @@ def host() -> ctypes.CDLL:
         lib.gqm_pick_segments.restype = ctypes.c_int
         lib.gqm_filter_segments.argtypes = [ctypes.c_int, dp, ctypes.c_int, ip, ctypes.c_int, ip]
         lib.gqm_filter_segments.restype = ctypes.c_int
+        lib.gqm_remove_holes.argtypes = [ctypes.c_int, dp, ctypes.c_int, ip, ip, ctypes.c_int, ip, ctypes.c_int, dp,
+                                         ctypes.c_void_p]
+        lib.gqm_remove_holes.restype = ctypes.c_int
+        lib.gqm_region_attributes.argtypes = [ctypes.c_int, dp, ctypes.c_int, ip, ip, ctypes.c_int, ip, ctypes.c_int,
+                                              dp, dp, dp]
+        lib.gqm_region_attributes.restype = ctypes.c_int
+        lib.gqm_mesh_free.argtypes = [ctypes.c_void_p]
         if hasattr(lib, "gqm_certify"):
             lib.gqm_certify.restype = ctypes.c_int
         _host = lib

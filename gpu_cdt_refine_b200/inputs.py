@@ -8,6 +8,8 @@ deterministic for a given seed.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 from . import _native
@@ -139,52 +141,63 @@ def batch_domains(count: int = 4096, seed: int = 20261207, nmin: int = 200, nmax
     return [r[0] for r in res], [r[1] for r in res]
 
 
+class _Mesh(ctypes.Structure):
+    _fields_ = [("numberofpoints", ctypes.c_int), ("pointlist", ctypes.POINTER(ctypes.c_double)),
+                ("numberoftriangles", ctypes.c_int), ("trianglelist", ctypes.POINTER(ctypes.c_int)),
+                ("neighborlist", ctypes.POINTER(ctypes.c_int)), ("numberofsegments", ctypes.c_int),
+                ("segmentlist", ctypes.POINTER(ctypes.c_int))]
+
+
+def _mesh_args(cdt: CDT):
+    p = np.ascontiguousarray(cdt.pointlist, np.float64)
+    t = np.ascontiguousarray(cdt.trianglelist, np.int32)
+    n = np.ascontiguousarray(cdt.neighborlist, np.int32)
+    s = np.ascontiguousarray(cdt.segmentlist, np.int32)
+    keep = (p, t, n, s)
+    return keep, (cdt.numberofpoints, _native.dptr(p), cdt.numberoftriangles, _native.iptr(t), _native.iptr(n),
+                  cdt.numberofsegments, _native.iptr(s))
+
+
 def remove_holes(cdt: CDT, holes) -> CDT:
     """The CDT with every triangle reachable from a hole point without crossing
     a segment removed (Triangle's holes; the reference ignores holes), and with
     the vertices and segments that no remaining triangle uses dropped and the
-    rest renumbered.  Hole boundaries must be segments; the result is a valid
-    input of the refiner (every boundary edge a segment)."""
-    from scipy.sparse import coo_matrix
-    from scipy.sparse.csgraph import connected_components
-
-    tri, nbr, seg, pts = cdt.trianglelist, cdt.neighborlist, cdt.segmentlist, cdt.pointlist
-    nt, npt = tri.shape[0], pts.shape[0]
-    if nt == 0 or len(holes) == 0:
+    rest renumbered (gqm_remove_holes in the host library).  Hole boundaries
+    must be segments; the result is a valid input of the refiner (every
+    boundary edge a segment)."""
+    h = np.ascontiguousarray(np.asarray(holes, np.float64).reshape(-1, 2))
+    if cdt.numberoftriangles == 0 or h.shape[0] == 0:
         return cdt
-    # edge j of a triangle joins vertices j+1 and j+2; covered edges are segments
-    a = tri[:, [1, 2, 0]].astype(np.int64)
-    b = tri[:, [2, 0, 1]].astype(np.int64)
-    ekey = np.minimum(a, b) * npt + np.maximum(a, b)
-    sg = seg.astype(np.int64)
-    skey = np.minimum(sg[:, 0], sg[:, 1]) * npt + np.maximum(sg[:, 0], sg[:, 1])
-    covered = np.isin(ekey, skey)
-    t_idx = np.repeat(np.arange(nt), 3).reshape(nt, 3)
-    link = (nbr >= 0) & ~covered
-    g = coo_matrix((np.ones(int(link.sum()), np.int8), (t_idx[link], nbr[link])), shape=(nt, nt))
-    _, comp = connected_components(g, directed=False)
-    # the triangle that contains each hole point
-    p0, p1, p2 = pts[tri[:, 0]], pts[tri[:, 1]], pts[tri[:, 2]]
-    drop = np.zeros(comp.max() + 1, bool)
-    for hx, hy in np.asarray(holes, np.float64).reshape(-1, 2):
-        def side(u, v):
-            return (v[:, 0] - u[:, 0]) * (hy - u[:, 1]) - (v[:, 1] - u[:, 1]) * (hx - u[:, 0])
-        inside = np.nonzero((side(p0, p1) >= 0) & (side(p1, p2) >= 0) & (side(p2, p0) >= 0))[0]
-        if inside.size:
-            drop[comp[inside[0]]] = True
-    keep = ~drop[comp]
-    newt = -np.ones(nt, np.int64)
-    newt[keep] = np.arange(int(keep.sum()))
-    tri2, nbr2 = tri[keep], nbr[keep]
-    nbr2 = np.where(nbr2 >= 0, newt[np.maximum(nbr2, 0)], -1)
-    used = np.zeros(npt, bool)
-    used[tri2.ravel()] = True
-    newp = -np.ones(npt, np.int64)
-    newp[used] = np.arange(int(used.sum()))
-    # segments still on an edge of a remaining triangle
-    kept_edges = ekey[keep].ravel()
-    seg2 = seg[np.isin(skey, kept_edges)]
-    return CDT(pts[used], newp[tri2].astype(np.int32), nbr2.astype(np.int32), newp[seg2].astype(np.int32))
+    L = _native.host()
+    keep, args = _mesh_args(cdt)
+    m = _Mesh()
+    rc = L.gqm_remove_holes(*args, h.shape[0], _native.dptr(h), ctypes.byref(m))
+    if rc != 0:
+        raise ValueError(f"gqm_remove_holes failed ({rc})")
+    try:
+        return CDT(np.ctypeslib.as_array(m.pointlist, shape=(2 * m.numberofpoints,)).copy(),
+                   np.ctypeslib.as_array(m.trianglelist, shape=(3 * m.numberoftriangles,)).copy(),
+                   np.ctypeslib.as_array(m.neighborlist, shape=(3 * m.numberoftriangles,)).copy(),
+                   np.ctypeslib.as_array(m.segmentlist, shape=(2 * m.numberofsegments,)).copy())
+    finally:
+        L.gqm_mesh_free(ctypes.byref(m))
+
+
+def region_attributes(cdt: CDT, regions):
+    """Per-triangle (attribute, max_area) arrays from regions given as rows
+    (x, y, attribute, max_area), Triangle's regionlist layout
+    (gqm_region_attributes in the host library): each triangle reachable from
+    a region's point without crossing a segment gets that region's values, a
+    later region overwriting an earlier one; unreached triangles get 0."""
+    r = np.ascontiguousarray(np.asarray(regions, np.float64).reshape(-1, 4))
+    attr = np.zeros(cdt.numberoftriangles, np.float64)
+    area = np.zeros(cdt.numberoftriangles, np.float64)
+    keep, args = _mesh_args(cdt)
+    rc = _native.host().gqm_region_attributes(*args, r.shape[0], _native.dptr(r), _native.dptr(attr),
+                                              _native.dptr(area))
+    if rc != 0:
+        raise ValueError(f"gqm_region_attributes failed ({rc})")
+    return attr, area
 
 
 def square_with_hole(seed: int = 20261210, n: int = 4000, hole=(0.35, 0.65)) -> CDT:

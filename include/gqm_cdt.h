@@ -74,6 +74,39 @@ int gqm_cdt_gpu_last_status(void);
 /* Frees the device buffers kept between calls on this host thread. */
 void gqm_cdt_gpu_release(void);
 
+/* Holes and regional attributes (host library; no counterpart in the
+ * reference, which ignores both: Triangle's hole list and its `-A` regional
+ * attributes, GPU_Refine/triangle.cpp).  A mesh whose arrays the library
+ * malloc'ed; release it with gqm_mesh_free. */
+typedef struct gqm_mesh {
+  int numberofpoints;
+  double *pointlist;
+  int numberoftriangles;
+  int *trianglelist;
+  int *neighborlist;
+  int numberofsegments;
+  int *segmentlist;
+} gqm_mesh;
+/* The CDT (np points, nt triangles with neighbours, ns segments) without every
+ * triangle reachable from one of the nholes hole points (x, y pairs) without
+ * crossing a segment; vertices and segments no remaining triangle uses are
+ * dropped, the rest renumbered in order.  Hole boundaries must be segments, so
+ * the result is a valid refiner input.  GQM_OK, GQM_ERR_ARGUMENT (an index out
+ * of range) or GQM_ERR_MEMORY. */
+int gqm_remove_holes(int np, const double *pts, int nt, const int *tri, const int *nbr, int ns, const int *segs,
+                     int nholes, const double *holes, gqm_mesh *out);
+/* Regional attributes: regions holds nregions rows (x, y, attribute,
+ * max_area), Triangle's regionlist layout.  Every triangle reachable from a
+ * region's point without crossing a segment gets the region's attribute
+ * (and max_area, when max_area is not NULL); regions are applied in order, a
+ * later one overwriting an earlier one; unreached triangles get 0.  Regions
+ * are bounded by segments and refinement keeps every segment, so on a refined
+ * mesh this gives each triangle its input region's attribute. */
+int gqm_region_attributes(int np, const double *pts, int nt, const int *tri, const int *nbr, int ns,
+                          const int *segs, int nregions, const double *regions, double *attribute,
+                          double *max_area);
+void gqm_mesh_free(gqm_mesh *m);
+
 /* The reference's whole flow in one call: Triangle "pzQnc" on the host
  * (GPU_Refine/mesh.cpp:397), then GPU_Refine_Quality (GPU_Refine/main.cpp:1862).  Here the CDT is built
  * on the device and refined there with no round trip through the host.

@@ -65,7 +65,7 @@ def test_grid_circles_matches_triangle():
 
 def test_input_is_valid_cdt():
     c = inputs.plain_small(seed=11, n=3000, nseg=150)
-    cert = certify(c, c, 20.0)
+    cert = certify(c, c, 0.0)  # an input CDT: no angle bound
     assert cert["ok"], cert
     # convex hull enclosed by segments: no open boundary edge
     assert cert["open_boundary"] == 0
@@ -98,7 +98,7 @@ def test_remove_holes_leaves_a_valid_cdt():
     c = inputs.square_with_hole(n=3000)
     cen = c.pointlist[c.trianglelist].mean(axis=1)
     assert not np.any((cen[:, 0] > 0.35) & (cen[:, 0] < 0.65) & (cen[:, 1] > 0.35) & (cen[:, 1] < 0.65))
-    cert = certify(c, c, 1e-3)
+    cert = certify(c, c, 0.0)  # an input CDT: no angle bound
     assert cert["ok"], cert
     # without holes the function returns the CDT unchanged
     d = inputs.plain_small(seed=9, n=300, nseg=10)
