@@ -51,7 +51,8 @@ def test_partition_domains_deterministic():
 
 def _oracle_engine(doms, thetas, **kw):
     """Stand-in for the persistent batch engine on CPU ranks: the oracle on each
-    domain (the CUDA engine is held to the same outputs by the GPU tests)."""
+    domain (the CUDA engine is held to the same outputs by the GPU tests).  The
+    emulated-engine tests below run the engine's own code instead."""
     from oracle import oracle_py
     outs = [oracle_py.refine(d, t, 1, 1) for d, t in zip(doms, thetas)]
     return [o[0] for o in outs], [o[1] for o in outs]
@@ -129,3 +130,97 @@ def test_batch_sharded_rank_without_domains():
     assert sorted(rep0["domains"]) == [0, 1] and res1 is None
     assert sorted(ids0 + ids1) == [0]
     assert len(res0) == 1 and res0[0].numberoftriangles == want[0].numberoftriangles
+
+
+# --- the engine's own code on CPU ranks --------------------------------------
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EMU_LIB = os.path.join(ROOT, "tests", "emu", "_build", "libgqm_emu.so")
+
+
+def _emu_worker(rank, world, port, out, fail_rank):
+    """A gloo rank whose engine is the persistent batch engine of this
+    repository (batch.cu and refine.cu compiled as host C++ against the
+    test-only runtime stand-in, tests/emu); with fail_rank set, that rank's
+    engine raises instead."""
+    import pickle
+
+    import torch.distributed as dist
+    from gpu_cdt_refine_b200 import refine
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    refine.use_library(EMU_LIB)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        doms, thetas = _shard_domains()
+        engine = None
+        if fail_rank == rank:
+            def engine(d, t, **kw):
+                raise RuntimeError("injected engine failure")
+        try:
+            res, stats, rep = replicas.refine_batch_sharded(doms, thetas, engine=engine, device=0)
+            out[rank] = pickle.dumps(("ok", res, rep))
+        except replicas.ShardError as e:
+            out[rank] = pickle.dumps(("failed", str(e), None))
+        # the process group still works after a failed call on every rank
+        ms, _ = replicas.reduce_step(1.0 + rank, 0.0)
+        out[f"after{rank}"] = ms
+    finally:
+        dist.destroy_process_group()
+
+
+def _build_emu():
+    import subprocess
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "tests", "emu"), EMU_LIB])
+
+
+def test_batch_sharded_emulated_engine_matches_oracle():
+    """Two gloo ranks run the persistent batch engine's own code (emulated on
+    the host) on their shares; rank 0 gathers the raw arrays through /dev/shm,
+    in input order, equal to the oracle byte for byte."""
+    import pickle
+
+    import numpy as np
+    _build_emu()
+    mgr = mp.Manager()
+    out = mgr.dict()
+    port = 30100 + (os.getpid() % 1000)
+    mp.spawn(_emu_worker, args=(2, port, out, -1), nprocs=2, join=True)
+    doms, thetas = _shard_domains()
+    want, _ = _oracle_engine(doms, thetas)
+    kind0, res0, rep0 = pickle.loads(out[0])
+    kind1, res1, _ = pickle.loads(out[1])
+    assert kind0 == kind1 == "ok" and res1 is None
+    assert sorted(rep0["domains"]) == [3, 3] or sum(rep0["domains"]) == len(doms)
+    for g, w in zip(res0, want):
+        for f in ("pointlist", "trianglelist", "neighborlist", "segmentlist"):
+            assert np.array_equal(getattr(g, f).view(np.uint8), getattr(w, f).view(np.uint8)), f
+    assert out["after0"] == out["after1"] == 2.0
+
+
+@pytest.mark.parametrize("fail_rank", [0, 1])
+def test_batch_sharded_engine_failure_reaches_every_rank(fail_rank):
+    """One rank's engine raises: both ranks raise ShardError after the same
+    collectives (none waits for the process-group timeout), and the group is
+    still usable."""
+    import pickle
+    _build_emu()
+    mgr = mp.Manager()
+    out = mgr.dict()
+    port = 30300 + 10 * fail_rank + (os.getpid() % 1000)
+    mp.spawn(_emu_worker, args=(2, port, out, fail_rank), nprocs=2, join=True)
+    for r in range(2):
+        kind, msg, _ = pickle.loads(out[r])
+        assert kind == "failed" and "1 rank(s)" in msg
+        assert ("injected engine failure" in msg) == (r == fail_rank)
+    assert out["after0"] == out["after1"] == 2.0
+
+
+def test_pack_unpack_roundtrip():
+    import numpy as np
+    doms, _ = _shard_domains()
+    back = replicas._unpack(replicas._pack(doms[:3]))
+    for a, b in zip(back, doms[:3]):
+        for f in ("pointlist", "trianglelist", "neighborlist", "segmentlist"):
+            assert np.array_equal(getattr(a, f), getattr(b, f))
+    assert replicas._unpack(replicas._pack([])) == []
