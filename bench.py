@@ -17,12 +17,18 @@ arrays) exceeds the 126 MB L2, so no explicit flush is done between steps.
 --impl reference times the reference's own CPU quality refinement (Triangle
 1.6 as vendored by the reference, triangulate("pzDQnrq20"),
 GPU_Refine/main.cpp:389-407) compiled from the reference sources into
-oracle/_ref, on the host cores.
+oracle/_ref, on the full workload and on all host cores: Triangle refines one
+mesh on one thread, so every step is one full refinement in a process of its
+own, as many at a time as there are cores; value = output triangles of all
+timed steps / the wall time of the timed steps.
 
 Multi-GPU: the single-domain refinement does not shard (its rounds resolve
 conflicts globally), so --gpus N runs N independent replicas, one per GPU,
 each refining the full workload; value is the sum over ranks of output
-triangles divided by the slowest rank's time ("scaling": "weak").
+triangles divided by the slowest rank's time ("scaling": "weak").  The
+batched workload shards by domain: with N > 1 the line also carries the
+4,096-domain batch distributed over the ranks (replicas.refine_batch_sharded,
+no data-path collective), timed as the slowest rank's engine call.
 """
 from __future__ import annotations
 
@@ -56,12 +62,17 @@ CHECK_DRAM_BYTES_PER_ITEM = 72.92e6 / 162684
 # FP64-pipe utilisation of the same launch (sm__inst_executed_pipe_fp64, % of
 # peak sustained active): the exact-predicate filters are a small part of its work.
 CHECK_FP64_PIPE_PCT = 4.36
-# Shares of the device time of one refinement of the 2M-point input in the ncu
-# launch list (profiles/launches_clustered2M.md): the check kernel and the
-# single-block kernel that runs the flip steps of at most 2,048 triangles.
-LAUNCH_LIST_SHARES = {"k_flip_small": 0.230, "k_check_flip2": 0.209, "k_cavity_mark": 0.084, "k_phase3q": 0.082}
-# timed Triangle runs of the CPU baseline (about 2 s each on the 1/4 sample)
-CPU_RUNS = 6
+# Algorithmic bytes of one whole flip step, for the small-step kernel (it runs
+# every phase of a step in one launch), per active triangle: the check
+# (CHECK_BYTES_PER_ITEM), the winner test (list entry 4, deferred-clear byte
+# 1, flip orientation 1, the claim words of the triangle and its partner 8)
+# and the filter into the next active set (queue entry 4, flip flag 1, status
+# 1, list entry written 4) ...
+STEP_BYTES_PER_ITEM = CHECK_BYTES_PER_ITEM + 14 + 10
+# ... and per flip or flop applied: the vertex, neighbour and subsegment rows
+# (48 B) of its two triangles read and written, and the back pointers of their
+# four outer neighbours read and written (4 x 8).
+STEP_BYTES_PER_WINNER = 2 * 2 * 48 + 4 * 8
 
 
 def parse():
@@ -81,6 +92,8 @@ def parse():
                    help="domains refined one call each to time the per-domain path")
     p.add_argument("--extras", type=int, default=1,
                    help="also measure the adversarial input and the learned placement (0: skip)")
+    p.add_argument("--autotune", type=int, default=1,
+                   help="choose the flip-loop launch shape with the autotuner before timing (0: defaults)")
     return p.parse_args()
 
 
@@ -172,14 +185,6 @@ def measured_peak():
         return float(d["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
-
-
-def cpu_sample(args):
-    """Bounded sample of the workload for the CPU legs: the same generator at
-    1/4 of the points and segments, about 2 s per Triangle run on one core
-    (Triangle needs ~40 s for the full 2M-point input)."""
-    from gpu_cdt_refine_b200 import inputs
-    return inputs.clustered(seed=args.seed + 7, n=max(args.points // 4, 1000), nseg=max(args.segments // 4, 50))
 
 
 def run_batch_workload(args, local_rank):
@@ -373,37 +378,119 @@ def run_construction(pts, seg, e2e_ms, local_rank):
     return res
 
 
-def time_triangle(cdt, reps, theta=20.0, mode=1):
-    """Triangle -q (reference CPU quality refinement) on the CDT; returns (tri/s, ms list, out tris)."""
+def _triangle_step(path, theta, mode):
+    """One step of the reference arm, in a spawned process: Triangle's quality
+    refinement of the CDT stored at `path`; returns (ms, output triangles)."""
+    from gpu_cdt_refine_b200 import cdtio
     from oracle import tri_ref
-    times, nt = [], 0
-    for _ in range(reps):
-        ms, nt = tri_ref.quality(cdt, theta, mode)
-        times.append(ms)
-    return nt / (np.mean(times) / 1e3), times, nt
+    return tri_ref.quality(cdtio.read_cdt(path), theta, mode)
+
+
+def triangle_steps(cdt, count, workers, theta=20.0, mode=1):
+    """`count` full Triangle refinements of `cdt`, `workers` processes at a
+    time (spawned, so no CUDA state is inherited); returns (wall s, list of
+    (ms, triangles))."""
+    import concurrent.futures as cf
+    import multiprocessing as mp
+    import tempfile
+    from gpu_cdt_refine_b200 import cdtio
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "workload.bin")
+        cdtio.write_cdt(path, cdt)
+        with cf.ProcessPoolExecutor(max(1, min(workers, count)), mp_context=mp.get_context("spawn")) as ex:
+            ex.submit(int, 0).result()  # processes up before the clock starts
+            t0 = time.perf_counter()
+            runs = list(ex.map(_triangle_step, [path] * count, [theta] * count, [mode] * count))
+            wall = time.perf_counter() - t0
+    return wall, runs
 
 
 def run_reference(args, rank, world):
+    """The reference's CPU quality refinement on the full workload, every host
+    core used: one Triangle process per step, as many at a time as cores."""
     if rank != 0:
         return
     full = workload(args)[0]
-    cdt = cpu_sample(args)
-    from oracle import tri_ref
-    for _ in range(min(args.warmup, 1)):
-        tri_ref.quality(cdt, 20.0, 1)
-    tps, times, nt = time_triangle(cdt, args.steps)
-    ms = float(np.mean(times))
-    line = {"metric": METRIC, "value": tps, "unit": "triangles/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)", "impl": "reference",
-            "config": config(args, full),
-            "cpu_baseline": {"value": tps, "unit": "triangles/s", "cores": 1, "kind": "reference", "host": cpu_model(),
-                             "sample": f"Triangle 1.6 pzDQnrq20 (single-threaded, as vendored by the reference) on "
-                                       f"a 1/4 sample of the workload ({cdt.numberofpoints} points, "
-                                       f"{cdt.numberofsegments} segments) per step"},
-            "e2e": {"value": tps, "unit": "triangles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "output_triangles": nt}
+    cores = os.cpu_count() or 1
+    triangle_steps(full, args.warmup, cores)  # warm-up steps, untimed
+    wall, runs = triangle_steps(full, args.steps, cores)
+    tris = sum(r[1] for r in runs)
+    value = tris / wall
+    single = float(np.mean([r[1] / (r[0] / 1e3) for r in runs]))
+    line = {"metric": METRIC, "value": value, "unit": "triangles/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "impl": "reference", "config": config(args, full),
+            "cpu_baseline": {"value": value, "unit": "triangles/s", "cores": min(cores, args.steps),
+                             "kind": "reference", "host": cpu_model(),
+                             "sample": f"Triangle 1.6 pzDQnrq20 (as vendored by the reference; one refinement per "
+                                       f"thread) on the full workload ({full.numberofpoints} points, "
+                                       f"{full.numberofsegments} segments), {args.steps} timed refinements, "
+                                       f"{min(cores, args.steps)} at a time in processes of their own; "
+                                       f"{wall:.1f} s wall",
+                             "single_refinement_ms": float(np.mean([r[0] for r in runs])),
+                             "single_core_value": single},
+            "e2e": {"value": value, "unit": "triangles/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "output_triangles": int(runs[0][1])}
     print(json.dumps(line), flush=True)
+
+
+def kernel_rooflines(probe, ms_step, peak, peak_kind):
+    """Roofline entries of the two kernels that take most of the device time,
+    from the per-launch device timers of one probed refinement: the grid-wide
+    flip-step check kernel (CHECK_BYTES_PER_ITEM per active triangle) and the
+    small-step kernel (STEP_BYTES_PER_ITEM per active triangle plus
+    STEP_BYTES_PER_WINNER per flip applied, summed over the steps it ran)."""
+    out = []
+    launches = max(int(probe["check_launches"]), 1)
+    if probe["check_ms"] > 0:
+        items = probe["check_items"] / launches
+        launch_s = probe["check_ms"] / 1e3 / launches
+        ach = CHECK_BYTES_PER_ITEM * items / launch_s / 1e9
+        out.append({"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                    "traffic": CHECK_DRAM_BYTES_PER_ITEM * items, "peak_kind": peak_kind,
+                    "kernel": "k_check_flip2 (grid-wide flip-step check)", "bytes_per_item": CHECK_BYTES_PER_ITEM,
+                    "launches": launches, "items_per_launch": items, "avg_launch_us": launch_s * 1e6,
+                    "share_of_step": probe["check_ms"] / ms_step,
+                    "traffic_note": "ncu DRAM bytes per active triangle of the 1M-point capture "
+                                    "(profiles/k_check_flip2_clustered1M.md) times this launch's items",
+                    "fp64_pipe_pct_ncu": CHECK_FP64_PIPE_PCT})
+    sl = max(int(probe["small_launches"]), 1)
+    if probe["small_ms"] > 0:
+        alg = STEP_BYTES_PER_ITEM * probe["small_items"] + STEP_BYTES_PER_WINNER * probe["small_winners"]
+        launch_s = probe["small_ms"] / 1e3 / sl
+        ach = alg / sl / launch_s / 1e9
+        out.append({"bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+                    "traffic": None, "peak_kind": peak_kind,
+                    "kernel": "small-step kernel (whole flip steps of small active sets in one launch)",
+                    "bytes_per_item": STEP_BYTES_PER_ITEM, "bytes_per_winner": STEP_BYTES_PER_WINNER,
+                    "launches": sl, "items_per_launch": probe["small_items"] / sl,
+                    "winners_per_launch": probe["small_winners"] / sl, "avg_launch_us": launch_s * 1e6,
+                    "share_of_step": probe["small_ms"] / ms_step})
+    out.sort(key=lambda r: -r["share_of_step"])
+    return out
+
+
+def run_sharded_batch(args, world, local_rank, dev):
+    """The batched workload over all ranks: every rank builds the same domain
+    list, replicas.refine_batch_sharded gives each rank its cost-balanced share
+    and times its engine call; the job time is the slowest rank's."""
+    from gpu_cdt_refine_b200 import inputs, refine, replicas
+    doms, thetas = inputs.batch_domains(args.batch_domains)
+    mine = replicas.partition_domains([replicas.domain_cost(d.numberofpoints, t) for d, t in zip(doms, thetas)],
+                                      world)[0]
+    import torch.distributed as dist
+    own = mine[dist.get_rank()]
+    if own:  # warm-up: this rank's buffers grow once
+        refine.refine_batch_persistent([doms[i] for i in own], [thetas[i] for i in own], device=local_rank)
+    dist.barrier()
+    ids, res, _, rep = replicas.refine_batch_sharded(doms, thetas, gather=False, device=local_rank)
+    tris_all = replicas.reduce_step(0.0, float(sum(r.numberoftriangles for r in res)), device=dev)[1]
+    return {"workload": f"{len(doms)} independent domains (the batched workload) sharded over {world} ranks",
+            "domains_per_rank": rep["domains"], "max_ms": rep["max_ms"], "rank0_ms": rep["rank_ms"],
+            "output_triangles": int(tris_all), "value": tris_all / (rep["max_ms"] / 1e3), "unit": "triangles/s",
+            "timing": "each rank's wall time of its engine call (pack, upload, one persistent launch, download, "
+                      "unpack); max over ranks by all-reduce"}
 
 
 def run_ours(args, rank, world, local_rank):
@@ -427,6 +514,11 @@ def run_ours(args, rank, world, local_rank):
     ctx = refine.Context(local_rank)
     opt = refine.make_options(20.0, refine.Offcenter, 1, device=local_rank)
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    # launch shape of the flip-flop loop chosen by the autotuner on this input
+    # (untimed; no shape changes a result)
+    t0 = time.perf_counter()
+    tuned, tuned_ms = ctx.autotune(cdt, opt) if args.autotune else (ctx.tuning(), None)
+    autotune_s = time.perf_counter() - t0
 
     def step():
         return ctx.run_device(cdt.numberofpoints, cdt.numberoftriangles, cdt.numberofsegments, d_pts.data_ptr(),
@@ -451,7 +543,7 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
     torch.cuda.synchronize()
     ms = ms_total / args.steps
-    # one more step with the device-side launch timer of the dominant kernel on
+    # one more step with the device-side launch timers of the two main kernels on
     ctx.probe(True)
     step()
     probe = ctx.probe_read()
@@ -460,8 +552,11 @@ def run_ours(args, rank, world, local_rank):
     ms_max, tris_all = replicas.reduce_step(ms, nt_out, device=dev)
     value = tris_all / (ms_max / 1e3)
 
-    # end to end through the reference-facing call: host arrays in, host arrays out
+    # end to end through the reference-facing call: host arrays in, host arrays
+    # out (the autotuned shape set on the library's cached context of this device)
+    refine.set_default_tuning(local_rank, **{k: v for k, v in tuned.items()})
     e2e_ms, h2d, d2h = [], cdt.nbytes(), 0
+    refine.refine(cdt, 20.0, refine.Offcenter, 1, device=local_rank)  # warm-up of the cached context
     for _ in range(args.e2e_steps):
         t0 = time.perf_counter()
         out, _ = refine.refine(cdt, 20.0, refine.Offcenter, 1, device=local_rank)
@@ -469,25 +564,27 @@ def run_ours(args, rank, world, local_rank):
         d2h = out.nbytes() + out.numberofpoints + out.numberoftriangles
     e2e_max, _ = replicas.reduce_step(float(np.median(e2e_ms)), nt_out, device=dev)
     e2e_value = tris_all / (e2e_max / 1e3)
+    sharded = run_sharded_batch(args, world, local_rank, dev) if (world > 1 and args.batch_domains > 0) else None
 
     if rank == 0:
         peak, peak_kind = measured_peak()
         s = stats[-1]
-        # dominant kernel: the flip-step check, timed on the device per launch
-        launches = max(int(probe["check_launches"]), 1)
-        items_per_launch = probe["check_items"] / launches
-        launch_s = probe["check_ms"] / 1e3 / launches
-        achieved = CHECK_BYTES_PER_ITEM * items_per_launch / launch_s / 1e9
-        traffic = (CHECK_DRAM_BYTES_PER_ITEM * items_per_launch if CHECK_DRAM_BYTES_PER_ITEM else None)
+        roofs = kernel_rooflines(probe, ms, peak, peak_kind)
         # path-level algorithmic bytes (input + output mesh + one quality check of
         # every output triangle): 16 B/point, 24 B/triangle, 8 B/segment, 60 B/tri
         alg = (16 * cdt.numberofpoints + 24 * cdt.numberoftriangles + 8 * cdt.numberofsegments + 16 * np_out +
                24 * nt_out + 8 * ns_out + 60 * nt_out)
         path_gbs = alg / (ms / 1e3) / 1e9
+        top = dict(roofs[0]) if roofs else {}
+        top.update({"timing": "per-launch device timers (%globaltimer, first block start to last block end) in "
+                              "one extra probed step after the timed region, on the context's stream",
+                    "path_achieved_gbs": path_gbs, "path_frac": path_gbs / peak, "kernels": roofs})
+        cfg = config(args, cdt)
+        cfg["launch_shape"] = tuned
         line = {"metric": METRIC, "value": value, "unit": "triangles/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-                "config": config(args, cdt),
+                "config": cfg,
                 "output_vertices": np_out, "output_triangles": nt_out, "output_segments": ns_out,
                 "e2e": {"value": e2e_value, "unit": "triangles/s", "h2d_bytes_per_step": int(h2d),
                         "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_max},
@@ -496,24 +593,13 @@ def run_ours(args, rank, world, local_rank):
                 "gpu_launches": int(sum(x["kernel_launches"] for x in stats)),
                 "gpu_launches_per_refinement": int(s["kernel_launches"]),
                 "host_syncs": int(s["host_syncs"]), "rounds": int(s["rounds"]),
-                "flip_steps": int(s["flip_steps"]),
-                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                             "kernel": "k_check_flip2 (flip-step check)",
-                             "bytes_per_item": CHECK_BYTES_PER_ITEM, "launches": launches,
-                             "items_per_launch": items_per_launch, "avg_launch_us": launch_s * 1e6,
-                             "share_of_step": probe["check_ms"] / ms,
-                             "first_launch_items": probe["first_items"],
-                             "timing": "per-launch device timer (%globaltimer, first block start to last block "
-                                       "end) in one extra probed step after the timed region",
-                             "path_achieved_gbs": path_gbs, "path_frac": path_gbs / peak,
-                             "fp64_pipe_pct_ncu": CHECK_FP64_PIPE_PCT,
-                             "launch_list_shares_ncu": LAUNCH_LIST_SHARES,
-                             "note": "k_flip_small (one thread block running whole flip steps of at most 2,048 "
-                                     "triangles) holds a slightly larger share than k_check_flip2; as a "
-                                     "single block it is latency bound by construction, so the roofline is "
-                                     "reported for the dominant grid-wide kernel"},
-                "clocks": clk.summary(), "input_generation_s": gen_s}
+                "flip_steps": int(s["flip_steps"]), "device_ms_library": s["device_ms"],
+                "autotune": {"chosen": tuned, "best_ms": tuned_ms, "seconds": autotune_s},
+                "roofline": top, "clocks": clk.summary(), "input_generation_s": gen_s}
+        if sharded:
+            line["batch_sharded"] = sharded
+        if world == 1:
+            line["other_modes"] = run_other_modes(ctx, cdt, local_rank)
         if args.batch_domains > 0 and world == 1:
             line["batch"] = run_batch_workload(args, local_rank)
         if args.extras and world == 1:
@@ -522,15 +608,14 @@ def run_ours(args, rank, world, local_rank):
             line["adversarial"] = run_adversarial(local_rank)
         if args.cpu_baseline and world == 1:
             try:
-                from oracle import tri_ref
-                smp = cpu_sample(args)
-                tri_ref.quality(smp, 20.0, 1)  # warm-up run, untimed
-                tps, times, ntc = time_triangle(smp, CPU_RUNS)
-                line["cpu_baseline"] = {"value": tps, "unit": "triangles/s", "cores": 1, "kind": "reference",
-                                        "host": cpu_model(), "sample": f"Triangle 1.6 pzDQnrq20 on a 1/4 sample of the workload "
-                                                  f"({smp.numberofpoints} points), {CPU_RUNS} timed runs, "
-                                                  f"{sum(times) / 1e3:.1f} s of CPU work",
-                                        "output_triangles": ntc}
+                wall, runs = triangle_steps(cdt, 1, 1)
+                ms_cpu, ntc = runs[0]
+                line["cpu_baseline"] = {"value": ntc / (ms_cpu / 1e3), "unit": "triangles/s", "cores": 1,
+                                        "kind": "reference", "host": cpu_model(),
+                                        "sample": f"Triangle 1.6 pzDQnrq20 on the full workload "
+                                                  f"({cdt.numberofpoints} points, {cdt.numberofsegments} "
+                                                  f"segments), one refinement on one core, {ms_cpu / 1e3:.1f} s",
+                                        "output_triangles": int(ntc)}
             except Exception as e:  # the reference build is test infrastructure; report, do not fail
                 line["cpu_baseline"] = {"value": None, "unit": "triangles/s", "cores": 1, "kind": "reference",
                                         "sample": f"unavailable: {e}"}
@@ -538,6 +623,22 @@ def run_ours(args, rank, world, local_rank):
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+def run_other_modes(ctx, cdt, local_rank):
+    """The same input in the other three {mode} x {policy} combinations of the
+    workload's configuration: device time of one refinement after a warm-up."""
+    from gpu_cdt_refine_b200 import refine
+    out = {}
+    for name, policy, mode in (("ruppert_circumcenter", refine.Circumcenter, 1), ("chew_offcenter", refine.Offcenter, 0),
+                               ("chew_circumcenter", refine.Circumcenter, 0)):
+        opt = refine.make_options(20.0, policy, mode, device=local_rank)
+        ctx.run_host(cdt, opt)
+        st = ctx.run_host(cdt, opt)
+        npo, nto, _ = ctx.sizes()
+        out[name] = {"device_ms": st["device_ms"], "output_triangles": nto, "output_vertices": npo,
+                     "triangles_per_s_device": nto / (st["device_ms"] / 1e3), "rounds": st["rounds"]}
+    return out
 
 
 def main():

@@ -3,14 +3,18 @@
     python -m gpu_cdt_refine_b200.build
 
 libgqm_b200.so : refine.cu (kernels, driver, C ABI) + batch.cu (persistent
-                 batched engine) + learned.cu (placement network training and
+                 batched engine, one-block small flip steps) + flipcl.cu
+                 (small flip steps on a thread-block cluster) + learned.cu (placement network training and
                  inference) + cdt_gpu.cu (CDT construction on the GPU) +
                  legacy.cpp (C++ drop-in)
-libgqm_host.so : cdt_build.cpp + synth.cpp + certify.cpp
+libgqm_b200_fma.so : the same with the refiner's kernels compiled under nvcc's
+                 default FMA contraction (-fmad=true), the arithmetic of the
+                 reference as its own project builds it
+libgqm_host.so : cdt_build.cpp + synth.cpp + certify.cpp + regions.cpp
 
-Every floating-point operation of the refiner is rounded on its own:
-nvcc -fmad=false and gcc -ffp-contract=off, the same arithmetic as the
-reference built with -fmad=false.
+In libgqm_b200.so every floating-point operation of the refiner is rounded on
+its own: nvcc -fmad=false and gcc -ffp-contract=off, the same arithmetic as
+the reference built with -fmad=false, which the CPU oracle restates.
 """
 from __future__ import annotations
 
@@ -39,45 +43,80 @@ def _stale(out, srcs):
 
 def build_host(force=False):
     out = os.path.join(HERE, "libgqm_host.so")
-    srcs = [os.path.join(CSRC, f) for f in ("cdt_build.cpp", "synth.cpp", "certify.cpp")]
+    srcs = [os.path.join(CSRC, f) for f in ("cdt_build.cpp", "synth.cpp", "certify.cpp", "regions.cpp")]
     deps = srcs + [os.path.join(CSRC, "predicates.h"), os.path.join(INC, "gqm_cdt.h")]
     if force or _stale(out, deps):
         _run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-ffp-contract=off", "-I" + INC, "-o", out] + srcs)
     return out
 
 
-def build_cuda(force=False, extra=None):
-    out = os.path.join(HERE, "libgqm_b200.so")
+# Refiner translation units: compiled once per arithmetic variant.
+REFINER_UNITS = ("refine.cu", "batch.cu", "flipcl.cu")
+# The arithmetic variants of the refiner:
+#   "separate"   every product and sum rounded on its own (-fmad=false): the
+#                reference built with -fmad=false, which the oracle restates;
+#   "contracted" nvcc's default contraction of a product feeding an add or a
+#                subtract into one fused multiply-add (-fmad=true): the
+#                reference as its project builds it (no -fmad option set).
+VARIANTS = {"separate": ("libgqm_b200.so", "-fmad=false", "_build"),
+            "contracted": ("libgqm_b200_fma.so", "-fmad=true", os.path.join("_build", "fma"))}
+
+
+def _cuda_jobs(force=False, extra=None, variant="separate"):
+    """(library path, object paths, compile commands of the stale objects)."""
+    lib, fmad, objsub = VARIANTS[variant]
+    out = os.path.join(HERE, lib)
     hdr = [os.path.join(INC, "gqm_refine.h"), os.path.join(INC, "gqm_triangulateio.h"),
            os.path.join(CSRC, "predicates.h"), os.path.join(CSRC, "host_copy.h")]
     refiner = [os.path.join(CSRC, f) for f in ("kernels.cuh", "gqm_device.cuh", "learned.cuh")]
-    units = {  # translation unit -> the headers it includes
-        "refine.cu": hdr + refiner,
-        "batch.cu": hdr + refiner,
-        "learned.cu": hdr + [os.path.join(CSRC, "learned.cuh")],
-        "cdt_gpu.cu": [os.path.join(INC, "gqm_cdt.h"), os.path.join(CSRC, "predicates.h"),
-                       os.path.join(CSRC, "host_copy.h")],
-        "legacy.cpp": hdr,
+    units = {  # translation unit -> (the headers it includes, its own flags)
+        "refine.cu": (hdr + refiner, []),
+        "batch.cu": (hdr + refiner, []),
+        # phases on several SMs of a cluster: global loads are cached in L2 only
+        "flipcl.cu": (hdr + refiner, ["-Xptxas", "-dlcm=cg"]),
+        "learned.cu": (hdr + [os.path.join(CSRC, "learned.cuh")], []),
+        "cdt_gpu.cu": ([os.path.join(INC, "gqm_cdt.h"), os.path.join(CSRC, "predicates.h"),
+                        os.path.join(CSRC, "host_copy.h")], []),
+        "legacy.cpp": (hdr, []),
     }
-    flags = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler",
-                    "-ffp-contract=off", "-I" + INC] + list(extra or [])
+    base = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+                   "-I" + INC] + list(extra or [])
     objdir = os.path.join(HERE, "_build")
-    os.makedirs(objdir, exist_ok=True)
-    # stale translation units compile in parallel, then one link
-    procs, objs = [], []
-    for name, deps in units.items():
+    vdir = os.path.join(HERE, objsub)
+    os.makedirs(vdir, exist_ok=True)
+    objs, cmds = [], []
+    for name, (deps, own) in units.items():
         src = os.path.join(CSRC, name)
-        obj = os.path.join(objdir, name + ".o")
+        mine = name in REFINER_UNITS
+        obj = os.path.join(vdir if mine else objdir, name + ".o")
         objs.append(obj)
-        if force or extra or _stale(obj, [src] + deps):
-            cmd = [NVCC] + flags + ["-c", src, "-o", obj]
+        # the units outside the refiner are shared by the variants (always
+        # -fmad=false) and compiled by the "separate" variant's jobs only
+        if (mine or variant == "separate") and (force or extra or _stale(obj, [src] + deps)):
+            flags = base + [fmad if mine else "-fmad=false"] + own
+            if mine and variant == "contracted":
+                flags = flags + ["-DGQM_CONTRACTED=1"]
+            cmds.append([NVCC] + flags + ["-c", src, "-o", obj])
+    return out, objs, cmds
+
+
+def build_cuda(force=False, extra=None, variants=("separate", "contracted")):
+    """Compile the stale objects of every variant in parallel, then link each
+    library whose objects changed."""
+    jobs = [_cuda_jobs(force, extra, v) for v in variants]
+    procs = []
+    for _, _, cmds in jobs:
+        for cmd in cmds:
             print(" ".join(cmd), flush=True)
             procs.append(subprocess.Popen(cmd))
     if any(p.wait() != 0 for p in procs):
         raise RuntimeError("nvcc failed")
-    if procs or _stale(out, objs):
-        _run([NVCC] + ARCH + ["-shared", "-o", out] + objs)
-    return out
+    outs = []
+    for out, objs, _ in jobs:
+        if procs or _stale(out, objs):
+            _run([NVCC] + ARCH + ["-shared", "-o", out] + objs)
+        outs.append(out)
+    return outs[0]
 
 
 def build(force=False):

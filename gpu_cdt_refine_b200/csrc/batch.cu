@@ -732,18 +732,23 @@ constexpr int kSmallThreads = 512;
 template <int PRED>
 __global__ void __launch_bounds__(kSmallThreads, 1)
     k_flip_small(Mesh M, FlipCtl *fc, int *act, uint8_t *clr, int *win, int *ll, int *sl, int *fq, int *tl,
-                 int limit, cudaGraphConditionalHandle h, int graph) {
+                 int limit, cudaGraphConditionalHandle h, int graph, KTimer *tm) {
   __shared__ int go;
+  const int timed = tm->on;
+  const unsigned long long start = timed ? global_ns() : 0;
+  long long items = 0, wins = 0;  // thread 0's count of the launch's work (probe only)
   for (;;) {
     if (threadIdx.x == 0) go = fc->cond && fc->nact <= limit;
     SYNC();
     if (!go) break;
+    if (threadIdx.x == 0) items += fc->nact;
     FlipQ Q{fq, &fc->qn, &fc->gen};
     TouchL T{tl, &fc->tn, &fc->gen};
     k_check_flip2<PRED>(M, act, &fc->nact, clr, T, &g_ktimer_off);
     SYNC();
     k_flip_winner2(M, act, &fc->nact, clr, Q, win, &fc->winn);
     SYNC();
+    if (threadIdx.x == 0) wins += fc->winn;
     k_link_phase1(M, win, &fc->winn, ll, sl, &fc->epoch);
     SYNC();
     k_phase2(M, win, &fc->winn, ll, sl);
@@ -767,31 +772,60 @@ __global__ void __launch_bounds__(kSmallThreads, 1)
 #endif
   (void)h;
   (void)graph;
+  if (timed) ktimer_end(tm, start, items, wins);
 }
 
 }  // namespace gqm
 
 // Launch of k_flip_small on the single-domain engine's buffers (refine.cu).
-// mesh points at the caller's Mesh (the same layout in both compilations).
+// mesh points at the caller's Mesh (the same layout in both compilations);
+// timer is the caller's KTimer (the same layout too).
 int gqm_flip_small_launch(const void *mesh, size_t mesh_bytes, void *fc, int pred, int *act, uint8_t *clr, int *win,
                           int *ll, int *sl, int *fq, int *tl, int limit, cudaStream_t st,
-                          cudaGraphConditionalHandle h, int graph) {
+                          cudaGraphConditionalHandle h, int graph, void *timer) {
   if (mesh_bytes != sizeof(gqm::Mesh)) return GQM_ERR_ARGUMENT;
   gqm::Mesh M;
   memcpy(&M, mesh, sizeof(M));
   gqm::FlipCtl *c = static_cast<gqm::FlipCtl *>(fc);
+  gqm::KTimer *tm = static_cast<gqm::KTimer *>(timer);
 #ifdef GQM_HOST_EMU
   (void)st;
   if (pred)
-    gqm::k_flip_small<1>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph);
+    gqm::k_flip_small<1>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph, tm);
   else
-    gqm::k_flip_small<0>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph);
+    gqm::k_flip_small<0>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph, tm);
 #else
   if (pred)
-    gqm::k_flip_small<1><<<1, gqm::kSmallThreads, 0, st>>>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph);
+    gqm::k_flip_small<1><<<1, gqm::kSmallThreads, 0, st>>>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph, tm);
   else
-    gqm::k_flip_small<0><<<1, gqm::kSmallThreads, 0, st>>>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph);
+    gqm::k_flip_small<0><<<1, gqm::kSmallThreads, 0, st>>>(M, c, act, clr, win, ll, sl, fq, tl, limit, h, graph, tm);
 #endif
+  return GQM_OK;
+}
+
+// The incircle expansion-fallback counter of this translation unit's kernels
+// (a device variable exists once per translation unit): added to *sum, then
+// zeroed when `reset` is set.  Called by the single-domain driver, which
+// reports the counters of all its kernels together.
+int gqm_fallbacks_cta(unsigned long long *sum, int reset, cudaStream_t st) {
+  unsigned long long v = 0;
+#ifdef GQM_HOST_EMU
+  (void)st;
+  v = gqm::g_incircle_fallbacks;
+  if (reset) gqm::g_incircle_fallbacks = 0;
+#else
+  if (cudaMemcpyFromSymbolAsync(&v, gqm::g_incircle_fallbacks, sizeof(v), 0, cudaMemcpyDeviceToHost, st) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return GQM_ERR_CUDA;
+  if (reset) {
+    const unsigned long long zero = 0;
+    if (cudaMemcpyToSymbolAsync(gqm::g_incircle_fallbacks, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, st) !=
+        cudaSuccess)
+      return GQM_ERR_CUDA;
+  }
+#endif
+  if (sum) *sum += v;
   return GQM_OK;
 }
 

@@ -14,21 +14,34 @@
 #define GQM_WALK_MIN_BLOCKS 2
 #endif
 
-// Two compilations of the same kernels:
+// Three compilations of the same kernels:
 //  * grid mode (default): every step below is a __global__ kernel whose
 //    grid-stride loop covers its items across the whole grid;
 //  * CTA mode (GQM_CTA_MODE, batch.cu): every step is a __device__ function
 //    that one thread block runs over one domain's items, the block's threads
-//    striding over them; the caller separates steps with __syncthreads().
-#ifdef GQM_CTA_MODE
+//    striding over them; the caller separates steps with __syncthreads();
+//  * cluster mode (GQM_CLUSTER_MODE, flipcl.cu): every step is a __device__
+//    function that the blocks of one thread-block cluster (the whole grid of
+//    the launch) run together, striding over the items with all their
+//    threads; the caller separates steps with cluster barriers.
+#if defined(GQM_CTA_MODE)
 #define GQM_KERNEL __device__
 #define GQM_WALK_BOUNDS
+#define GQM_BOUNDS(minb)
 #define GQM_GTID ((int)threadIdx.x)
 #define GQM_GSIZE ((int)blockDim.x)
 #define GQM_BLOCK0 true
+#elif defined(GQM_CLUSTER_MODE)
+#define GQM_KERNEL __device__
+#define GQM_WALK_BOUNDS
+#define GQM_BOUNDS(minb)
+#define GQM_GTID ((int)(blockIdx.x * blockDim.x + threadIdx.x))
+#define GQM_GSIZE ((int)(gridDim.x * blockDim.x))
+#define GQM_BLOCK0 (blockIdx.x == 0)
 #else
 #define GQM_KERNEL __global__
 #define GQM_WALK_BOUNDS __launch_bounds__(256, GQM_WALK_MIN_BLOCKS)
+#define GQM_BOUNDS(minb) __launch_bounds__(256, minb)
 #define GQM_GTID ((int)(blockIdx.x * blockDim.x + threadIdx.x))
 #define GQM_GSIZE ((int)(gridDim.x * blockDim.x))
 #define GQM_BLOCK0 (blockIdx.x == 0)
@@ -804,6 +817,7 @@ GQM_KERNEL void k_mark_redundant(Mesh M, int *delmarker, const int *dellist, con
 struct KTimer {
   unsigned long long t0, t1;  // earliest block start / latest block end of the current launch
   unsigned long long total_ns, launches, items;
+  unsigned long long winners;  // flips and flops applied (small-step kernel)
   unsigned long long first_items[4];  // items of the first four launches since the reset
   unsigned blocks_done;
   int on;
@@ -819,8 +833,10 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 #endif
 }
-// called by every thread of the block after its work, with the block's start stamp
-__device__ __forceinline__ void ktimer_end(KTimer *tm, unsigned long long start, int items) {
+// called by every thread of the block after its work, with the block's start
+// stamp; the last block's `items` and `winners` are added for the launch
+__device__ __forceinline__ void ktimer_end(KTimer *tm, unsigned long long start, long long items,
+                                           long long winners = 0) {
   __syncthreads();
   if (threadIdx.x == 0) {
     atomicMin(&tm->t0, start);
@@ -834,6 +850,7 @@ __device__ __forceinline__ void ktimer_end(KTimer *tm, unsigned long long start,
       if (v->launches < 4) v->first_items[v->launches] = (unsigned long long)items;
       v->launches += 1;
       v->items += (unsigned long long)items;
+      v->winners += (unsigned long long)winners;
       v->t0 = ~0ull;
       v->t1 = 0;
       v->blocks_done = 0;
@@ -844,7 +861,7 @@ GQM_KERNEL void k_ktimer_reset(KTimer *tm, int on) {
   if (GQM_BLOCK0 && threadIdx.x == 0) {
     tm->t0 = ~0ull;
     tm->t1 = 0;
-    tm->total_ns = tm->launches = tm->items = 0;
+    tm->total_ns = tm->launches = tm->items = tm->winners = 0;
     for (int i = 0; i < 4; ++i) tm->first_items[i] = 0;
     tm->blocks_done = 0;
     tm->on = on;
@@ -1005,10 +1022,12 @@ GQM_KERNEL void k_flip_reset_filter(Mesh M, const int *tl, const int *tn, const 
 
 // kernelCheckFlipping (refine.cu:778-1070) on A.  No flag is cleared here
 // (the decision is kept in clr[k] and applied by k_flip_winner2), so the
-// neighbour flags read below are the ones the step started with.
-template <int PRED>
-GQM_KERNEL void GQM_WALK_BOUNDS k_check_flip2(Mesh M, const int *act, const int *dn, uint8_t *clr, TouchL T,
-                                              KTimer *tm) {
+// neighbour flags read below are the ones the step started with.  MINB is the
+// grid-mode register budget: at least MINB resident 256-thread blocks per SM
+// (2: at most 128 registers, some spilled; 1: up to 255, none spilled).
+template <int PRED, int MINB = GQM_WALK_MIN_BLOCKS>
+GQM_KERNEL void GQM_BOUNDS(MINB) k_check_flip2(Mesh M, const int *act, const int *dn, uint8_t *clr, TouchL T,
+                                               KTimer *tm) {
   const int timed = tm->on;
   const unsigned long long start = timed ? global_ns() : 0;
   int n = *dn;

@@ -46,7 +46,15 @@ struct NvtxRange {
 // batch.cu: the flip steps of small active sets in one block
 int gqm_flip_small_launch(const void *mesh, size_t mesh_bytes, void *fc, int pred, int *act, uint8_t *clr, int *win,
                           int *ll, int *sl, int *fq, int *tl, int limit, cudaStream_t st,
-                          cudaGraphConditionalHandle h, int graph);
+                          cudaGraphConditionalHandle h, int graph, void *timer);
+// flipcl.cu: the same on one thread-block cluster of csize blocks
+int gqm_flip_small_cl_launch(const void *mesh, size_t mesh_bytes, void *fc, int pred, int *act, uint8_t *clr,
+                             int *win, int *ll, int *sl, int *fq, int *tl, int limit, int csize, cudaStream_t st,
+                             cudaGraphConditionalHandle h, int graph, void *timer);
+int gqm_flip_cluster_ok(int csize);
+// the incircle expansion-fallback counters of batch.cu's and flipcl.cu's kernels
+int gqm_fallbacks_cta(unsigned long long *sum, int reset, cudaStream_t st);
+int gqm_fallbacks_cluster(unsigned long long *sum, int reset, cudaStream_t st);
 
 namespace gqm {
 
@@ -228,6 +236,7 @@ struct Refiner {
   uint8_t *clr = nullptr;            // deferred flag clears of a flip step
   FlipCtl *fc = nullptr;             // flip-loop control block (device)
   KTimer *ktm = nullptr;             // launch timer of the flip-step check kernel
+  KTimer *stm = nullptr;             // launch timer of the small-step kernel
   bool probing = false;              // events around every flip-loop launch
   std::vector<cudaEvent_t> loop_ev;  // pairs, reused every run
   size_t loop_ev_used = 0;
@@ -337,7 +346,7 @@ struct Refiner {
   void release() {
     drop_flip_graph();
     void *ptrs[] = {M.pts, M.ps, M.pred, M.tv, M.tn, M.tsg, M.tst, M.tflip, M.tfo, M.flip0, M.tmark, M.tpos,
-                    M.s2t, M.s2seg, M.enc, M.err, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
+                    M.s2t, M.s2seg, M.enc, M.err, stm, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
                     newidx, tail, center, emptyp, pnew, enclist, encl2, smark, mids, snap, segs, dcount, bc,
                     dctr, dgc, dinput, mlp_w, mlp_b, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wsup, M.wmeg};
     for (void *p : ptrs)
@@ -350,6 +359,7 @@ struct Refiner {
     clr = nullptr;
     fc = nullptr;
     ktm = nullptr;
+    stm = nullptr;
     mlp_w = nullptr;
     mlp_b = nullptr;
     for (cudaEvent_t e : loop_ev) cudaEventDestroy(e);
@@ -388,10 +398,11 @@ struct Refiner {
     if (!ev1) cudaEventCreate(&ev1);
     if (!dcount) {
       if (dalloc(&dcount, 16) || dalloc(&bc, kMaxCompactBlocks + 1) || dalloc(&dctr, 8) || dalloc(&dgc, 2) ||
-          dalloc(&M.err, 1) || dalloc(&fc, 1) || dalloc(&ktm, 1))
+          dalloc(&M.err, 1) || dalloc(&fc, 1) || dalloc(&ktm, 1) || dalloc(&stm, 1))
         return GQM_ERR_MEMORY;
       cudaMemsetAsync(fc, 0, sizeof(FlipCtl), st);
       cudaMemsetAsync(ktm, 0, sizeof(KTimer), st);  // off until gqm_context_probe
+      cudaMemsetAsync(stm, 0, sizeof(KTimer), st);
       cudaMemsetAsync(bc + kMaxCompactBlocks, 0, sizeof(int), st);  // the zero base of one-block compactions
 #ifdef GQM_HOST_EMU
       use_graph = false;
@@ -601,30 +612,55 @@ struct Refiner {
 #ifndef GQM_STEP_GRID
 #define GQM_STEP_GRID (148 * 4)
 #endif
-  // grid of the flip-step kernels, whose item counts live on the device
-  static constexpr int kStepGrid = GQM_STEP_GRID;
-  // steps whose active set has at most this many triangles run in one block
+  // steps whose active set has at most this many triangles run in one launch
 #ifndef GQM_SMALL_STEP
 #define GQM_SMALL_STEP 2048
 #endif
-  static constexpr int kSmallStep = GQM_SMALL_STEP;
+  // Launch shape of the flip-flop loop (gqm_tuning).  None of it changes a
+  // result: every step makes the reference's decisions whatever the grid.
+  struct Tuning {
+    int step_grid = GQM_STEP_GRID;       // blocks of each grid-wide step kernel
+    int small_limit = GQM_SMALL_STEP;    // <= this many active triangles: small-step kernel (0: never)
+    int small_cluster = 1;               // small-step kernel: 1 = one 512-thread block, 8 / 16 = a cluster
+    int check_minb = GQM_WALK_MIN_BLOCKS;  // register budget of the check kernel (blocks per SM)
+    bool operator==(const Tuning &o) const {
+      return step_grid == o.step_grid && small_limit == o.small_limit && small_cluster == o.small_cluster &&
+             check_minb == o.check_minb;
+    }
+  } tune, flip_graph_tune;
+  template <int PRED>
+  void launch_check(const TouchL &T) {
+    void (*check)(Mesh, const int *, const int *, uint8_t *, TouchL, KTimer *) =
+        tune.check_minb == 1 ? k_check_flip2<PRED, 1> : k_check_flip2<PRED, 2>;
+    KL(check, tune.step_grid, 256)(M, act, &fc->nact, clr, T, ktm);
+  }
   void flip_body(cudaGraphConditionalHandle h, int graph) {
     FlipQ Q{fq, &fc->qn, &fc->gen};
     TouchL T{tl, &fc->tn, &fc->gen};
+    const int g = tune.step_grid;
     if (pred_mode)
-      KL(k_check_flip2<1>, kStepGrid, 256)(M, act, &fc->nact, clr, T, ktm);
+      launch_check<1>(T);
     else
-      KL(k_check_flip2<0>, kStepGrid, 256)(M, act, &fc->nact, clr, T, ktm);
-    KL(k_flip_winner2, kStepGrid, 256)(M, act, &fc->nact, clr, Q, win, &fc->winn);
-    KL(k_link_phase1, kStepGrid, 256)(M, win, &fc->winn, ll, sl, &fc->epoch);
-    KL(k_phase2, kStepGrid, 256)(M, win, &fc->winn, ll, sl);
-    KL(k_phase3q, kStepGrid, 256)(M, win, &fc->winn, sl, Q);
-    KL(k_mark_red_steiner_q, kStepGrid, 256)(M, tl, &fc->tn, Q);
-    KL(k_flip_reset_filter, kStepGrid, 256)(M, tl, &fc->tn, fq, &fc->qn, act, &fc->nact_next);
+      launch_check<0>(T);
+    KL(k_flip_winner2, g, 256)(M, act, &fc->nact, clr, Q, win, &fc->winn);
+    KL(k_link_phase1, g, 256)(M, win, &fc->winn, ll, sl, &fc->epoch);
+    KL(k_phase2, g, 256)(M, win, &fc->winn, ll, sl);
+    KL(k_phase3q, g, 256)(M, win, &fc->winn, sl, Q);
+    KL(k_mark_red_steiner_q, g, 256)(M, tl, &fc->tn, Q);
+    KL(k_flip_reset_filter, g, 256)(M, tl, &fc->tn, fq, &fc->qn, act, &fc->nact_next);
     KL(k_flip_cond, 1, 32)(fc, h, graph);
-    // the following small steps in one block (batch.cu), which re-sets the condition
-    gqm_flip_small_launch(&M, sizeof(M), fc, pred_mode, act, clr, win, ll, sl, fq, tl, kSmallStep, st, h, graph);
+    // the following small steps in one block (batch.cu) or one cluster
+    // (flipcl.cu), which re-sets the condition
+    if (tune.small_limit <= 0) return;
+    if (tune.small_cluster > 1)
+      gqm_flip_small_cl_launch(&M, sizeof(M), fc, pred_mode, act, clr, win, ll, sl, fq, tl, tune.small_limit,
+                               tune.small_cluster, st, h, graph, stm);
+    else
+      gqm_flip_small_launch(&M, sizeof(M), fc, pred_mode, act, clr, win, ll, sl, fq, tl, tune.small_limit, st, h,
+                            graph, stm);
   }
+  // kernels one grid step of the loop body launches (with its condition kernel)
+  int step_kernels() const { return tune.small_limit > 0 ? 9 : 8; }
   int build_flip_graph() {
 #ifdef GQM_HOST_EMU
     return GQM_ERR_CUDA;
@@ -685,6 +721,7 @@ struct Refiner {
     flip_graph = g;
     flip_graph_mesh = M;
     flip_graph_pred = pred_mode;
+    flip_graph_tune = tune;
     return GQM_OK;
 #endif
   }
@@ -711,7 +748,8 @@ struct Refiner {
     LAUNCH(k_flip_entry_reset, ntri, M, ntri);
     compact_to(PNotNullFlag{M.tst, M.tflip}, Ident{}, 0, ntri, act, &fc->nact);
     if (use_graph) {
-      if (!flip_exec || memcmp(&flip_graph_mesh, &M, sizeof(Mesh)) != 0 || flip_graph_pred != pred_mode) {
+      if (!flip_exec || memcmp(&flip_graph_mesh, &M, sizeof(Mesh)) != 0 || flip_graph_pred != pred_mode ||
+          !(flip_graph_tune == tune)) {
         if (build_flip_graph() != GQM_OK) {
           use_graph = false;
           cudaGetLastError();
@@ -735,7 +773,7 @@ struct Refiner {
       stats.host_syncs++;
       if (!hcount[C_MISC]) break;
       flip_body(h, 0);
-      stats.kernel_launches += 9;
+      stats.kernel_launches += step_kernels();
     }
     return GQM_OK;
   }
@@ -981,6 +1019,9 @@ struct Refiner {
     {
       const unsigned long long zero = 0;
       cudaMemcpyToSymbolAsync(g_incircle_fallbacks, &zero, sizeof(zero), 0, cudaMemcpyHostToDevice, st);
+      // the small-step kernels' counters (their own translation units)
+      gqm_fallbacks_cta(nullptr, 1, st);
+      gqm_fallbacks_cluster(nullptr, 1, st);
     }
     KL(k_ctl_reset, 1, 32)(fc, 64 * max_rounds, M.err);
     LAUNCH(k_check_input, std::max(np, nt), (const double2 *)dpts, np, dtri_in, dnbr_in, nt, dseg_in, ns, M.err);
@@ -1080,7 +1121,7 @@ struct Refiner {
     // each graph launch counted one kernel (its loop-entry kernel); the nine
     // kernels of every loop iteration it ran (a grid step, its condition and
     // the single-block kernel that runs the small steps after it) are added here
-    if (use_graph) stats.kernel_launches += 9LL * (hf.steps - hf.small_steps);
+    if (use_graph) stats.kernel_launches += (long long)step_kernels() * (hf.steps - hf.small_steps);
     for (int b = 0; b < kFlipProfileBins; ++b) {
       flip_prof_steps[b] = (long long)hf.prof_steps[b];
       flip_prof_items[b] = (long long)hf.prof_items[b];
@@ -1090,6 +1131,8 @@ struct Refiner {
     {
       unsigned long long fb = 0;
       cudaMemcpyFromSymbol(&fb, g_incircle_fallbacks, sizeof(fb));
+      gqm_fallbacks_cta(&fb, 0, st);
+      gqm_fallbacks_cluster(&fb, 0, st);
       stats.exact_fallbacks = (long long)fb;
     }
     have_result = (rc == 0);
@@ -1207,8 +1250,10 @@ int gqm_context_probe(gqm_context *ctx, int enable) {
   if (cudaSetDevice(r.device) != cudaSuccess) return GQM_ERR_CUDA;
 #ifdef GQM_HOST_EMU
   gqm::k_ktimer_reset(r.ktm, enable ? 1 : 0);
+  gqm::k_ktimer_reset(r.stm, enable ? 1 : 0);
 #else
   gqm::k_ktimer_reset<<<1, 32, 0, r.st>>>(r.ktm, enable ? 1 : 0);
+  gqm::k_ktimer_reset<<<1, 32, 0, r.st>>>(r.stm, enable ? 1 : 0);
 #endif
   r.probing = enable != 0;
   r.probe_loop_ms = 0.0;
@@ -1219,16 +1264,109 @@ int gqm_context_probe_read(gqm_context *ctx, gqm_probe *p) {
   if (!ctx || !p || !ctx->r.ktm) return GQM_ERR_ARGUMENT;
   gqm::Refiner &r = ctx->r;
   if (cudaSetDevice(r.device) != cudaSuccess) return GQM_ERR_CUDA;
-  gqm::KTimer h;
+  gqm::KTimer h, hs;
   if (cudaStreamSynchronize(r.st) != cudaSuccess ||
-      cudaMemcpy(&h, r.ktm, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+      cudaMemcpy(&h, r.ktm, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(&hs, r.stm, sizeof(hs), cudaMemcpyDeviceToHost) != cudaSuccess)
     return GQM_ERR_CUDA;
+  p->small_launches = (long long)hs.launches;
+  p->small_items = (long long)hs.items;
+  p->small_winners = (long long)hs.winners;
+  p->small_ms = (double)hs.total_ns * 1e-6;
   p->check_launches = (long long)h.launches;
   p->check_items = (long long)h.items;
   p->check_ms = (double)h.total_ns * 1e-6;
   for (int i = 0; i < 4; ++i) p->first_items[i] = (long long)h.first_items[i];
   p->loop_launches = r.probe_loops;
   p->loop_ms = r.probe_loop_ms;
+  return GQM_OK;
+}
+int gqm_context_set_tuning(gqm_context *ctx, const gqm_tuning *t) {
+  if (!ctx || !t) return GQM_ERR_ARGUMENT;
+  gqm::Refiner::Tuning n;
+  if (t->step_grid < 0 || t->step_grid > 148 * 64) return GQM_ERR_ARGUMENT;
+  if (t->step_grid > 0) n.step_grid = t->step_grid;
+  if (t->small_limit < 0)
+    n.small_limit = 0;
+  else if (t->small_limit > 0)
+    n.small_limit = t->small_limit;
+  if (t->small_cluster != 0 && t->small_cluster != 1 && t->small_cluster != 8 && t->small_cluster != 16)
+    return GQM_ERR_ARGUMENT;
+  if (t->small_cluster > 1) n.small_cluster = t->small_cluster;
+  if (t->check_blocks_per_sm < 0 || t->check_blocks_per_sm > 2) return GQM_ERR_ARGUMENT;
+  if (t->check_blocks_per_sm > 0) n.check_minb = t->check_blocks_per_sm;
+  if (n.small_cluster > 1) {
+    if (cudaSetDevice(ctx->r.device) != cudaSuccess) return GQM_ERR_CUDA;
+    if (!gqm_flip_cluster_ok(n.small_cluster)) return GQM_ERR_CUDA;
+  }
+  ctx->r.tune = n;
+  return GQM_OK;
+}
+int gqm_context_get_tuning(gqm_context *ctx, gqm_tuning *t) {
+  if (!ctx || !t) return GQM_ERR_ARGUMENT;
+  const gqm::Refiner::Tuning &c = ctx->r.tune;
+  t->step_grid = c.step_grid;
+  t->small_limit = c.small_limit > 0 ? c.small_limit : -1;
+  t->small_cluster = c.small_cluster;
+  t->check_blocks_per_sm = c.check_minb;
+  return GQM_OK;
+}
+int gqm_context_autotune(gqm_context *ctx, const gqm_cdt_in *in, int in_on_device, const gqm_options *opt,
+                         int repeats, gqm_tuning *chosen, double *best_ms) {
+  if (!ctx || !chosen) return GQM_ERR_ARGUMENT;
+  int rc = validate(in, opt);
+  if (rc) return rc;
+  if (repeats < 1) repeats = 1;
+  gqm::Refiner &R = ctx->r;
+  auto time_of = [&](double *ms) -> int {
+    double best = 1e300;
+    for (int k = 0; k < repeats; ++k) {
+      int e = R.run(in, in_on_device != 0, opt);
+      if (e) return e;
+      best = std::min(best, (double)R.stats.device_ms);
+    }
+    *ms = best;
+    return GQM_OK;
+  };
+  gqm_tuning cur;
+  gqm_context_get_tuning(ctx, &cur);
+  // one untimed run first: buffers grow and the loop graph is built once
+  rc = R.run(in, in_on_device != 0, opt);
+  if (rc) return rc;
+  double best = 0.0;
+  rc = time_of(&best);
+  if (rc) return rc;
+  // one field at a time, in order of expected effect; each candidate that the
+  // device cannot run (a cluster size it cannot place) is skipped
+  const int checks[] = {2, 1};
+  const int clusters[] = {1, 8, 16};
+  const int limits[] = {1024, 2048, 4096, 8192};
+  const int grids[] = {148 * 2, 148 * 4, 148 * 8};
+  for (int field = 0; field < 4; ++field) {
+    const int *vals = field == 0 ? checks : field == 1 ? clusters : field == 2 ? limits : grids;
+    const int nv = field == 0 ? 2 : field == 1 ? 3 : field == 2 ? 4 : 3;
+    for (int k = 0; k < nv; ++k) {
+      gqm_tuning cand = cur;
+      int *f = field == 0 ? &cand.check_blocks_per_sm
+                          : field == 1 ? &cand.small_cluster : field == 2 ? &cand.small_limit : &cand.step_grid;
+      if (*f == vals[k]) continue;
+      *f = vals[k];
+      if (gqm_context_set_tuning(ctx, &cand) != GQM_OK) continue;
+      double ms = 0.0;
+      rc = time_of(&ms);
+      if (rc) {
+        gqm_context_set_tuning(ctx, &cur);
+        return rc;
+      }
+      if (ms < best) {
+        best = ms;
+        cur = cand;
+      }
+    }
+    gqm_context_set_tuning(ctx, &cur);
+  }
+  gqm_context_get_tuning(ctx, chosen);
+  if (best_ms) *best_ms = best;
   return GQM_OK;
 }
 int gqm_context_flip_profile(gqm_context *ctx, long long *steps, long long *items) {
@@ -1287,6 +1425,21 @@ int gqm_context_result_sizes(gqm_context *ctx, int *np, int *nt, int *ns) {
 }
 void *gqm_context_stream(gqm_context *ctx) { return ctx ? (void *)ctx->r.st : nullptr; }
 
+// One cached context per device for gqm_refine: device buffers and the
+// captured flip-loop graph are reused by later calls instead of being
+// allocated every time.  Callers hold g_cache_mutex.
+static std::mutex g_cache_mutex;
+static gqm_context *g_cache[64] = {};
+static int cached_context(int device, gqm_context **out) {
+  gqm_context *&ctx = g_cache[device];
+  if (!ctx) {
+    int rc = gqm_context_create(device, &ctx);
+    if (rc) return rc;
+  }
+  *out = ctx;
+  return GQM_OK;
+}
+
 int gqm_refine(const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt, gqm_stats *stats) {
   if (!out) return GQM_ERR_ARGUMENT;
   memset(out, 0, sizeof(*out));
@@ -1297,20 +1450,23 @@ int gqm_refine(const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt, g
   }
   int rc = validate(in, opt);
   if (rc) return rc;
-  // One cached context per device: device buffers and the captured flip-loop
-  // graph are reused by later calls instead of being allocated every time.
-  static std::mutex cache_mutex;
-  static gqm_context *cache[64] = {};
   if (opt->device < 0 || opt->device >= 64) return GQM_ERR_NO_DEVICE;
-  std::lock_guard<std::mutex> lock(cache_mutex);
-  gqm_context *&ctx = cache[opt->device];
-  if (!ctx) {
-    rc = gqm_context_create(opt->device, &ctx);
-    if (rc) return rc;
-  }
+  std::lock_guard<std::mutex> lock(g_cache_mutex);
+  gqm_context *ctx = nullptr;
+  rc = cached_context(opt->device, &ctx);
+  if (rc) return rc;
   rc = gqm_context_run(ctx, in, 0, opt, stats);
   if (rc == GQM_OK) rc = gqm_context_result(ctx, out);
   return rc;
+}
+
+int gqm_set_default_tuning(int device, const gqm_tuning *t) {
+  if (!t || device < 0 || device >= 64) return GQM_ERR_ARGUMENT;
+  std::lock_guard<std::mutex> lock(g_cache_mutex);
+  gqm_context *ctx = nullptr;
+  int rc = cached_context(device, &ctx);
+  if (rc) return rc;
+  return gqm_context_set_tuning(ctx, t);
 }
 
 int gqm_refine_batch(int ndomains, const gqm_cdt_in *in, gqm_cdt_out *out, const gqm_options *opt,
@@ -1389,7 +1545,11 @@ const char *gqm_status_string(int s) {
     default: return "unknown status";
   }
 }
-int gqm_version(void) { return 100; }
+int gqm_version(void) { return 101; }
+#ifndef GQM_CONTRACTED
+#define GQM_CONTRACTED 0
+#endif
+int gqm_arithmetic(void) { return GQM_CONTRACTED ? GQM_ARITH_CONTRACTED : GQM_ARITH_SEPARATE; }
 
 }  // extern "C"
 
@@ -1399,10 +1559,11 @@ int gqm_version(void) { return 100; }
 // For callers that cannot allocate at the time they read a result: a service
 // with a device memory budget fixed at start-up that reads many small results
 // in a loop, or code sharing the GPU with work that must not be stalled by the
-// device-wide synchronization cudaFree implies.  The kernel below is the
-// result-emission kernel of gqm_context_result() staging into a statically
-// allocated device array instead of per-call cudaMalloc buffers; the caller
-// provides the host arrays.
+// device-wide synchronization a cudaFree implies.  gqm_context_result() mallocs
+// the host result arrays on every call and grows its device and pinned staging
+// buffers (cudaMalloc / cudaFree) whenever a larger result arrives; the kernel
+// below is its result-emission kernel staging into a statically allocated
+// device array instead, and the caller provides the host arrays.
 // ============================================================================
 namespace gqm {
 
@@ -1492,15 +1653,24 @@ extern "C" int gqm_context_result_noalloc(gqm_context *ctx, gqm_cdt_out *out) {
   int work = std::max(std::max(nt, ns), np);
   KL(gqm::k_emit_output_staged, gqm::Refiner::grid_for(work), 256)(R.M, np, nt, ns, stage);
   if (cudaGetLastError() != cudaSuccess) return GQM_ERR_CUDA;
-  cudaMemcpyAsync(out->pointlist, R.M.pts, sizeof(double) * 2 * (size_t)np, cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(out->trianglelist, stage + gqm::kNoAllocTri, sizeof(int) * 3 * (size_t)nt,
-                  cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(out->neighborlist, stage + gqm::kNoAllocNbr, sizeof(int) * 3 * (size_t)nt,
-                  cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(out->segmentlist, stage + gqm::kNoAllocSeg, sizeof(int) * 2 * (size_t)ns,
-                  cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(out->tstatus, stage + gqm::kNoAllocTs, (size_t)nt, cudaMemcpyDeviceToHost, st);
-  cudaMemcpyAsync(out->pstatus, stage + gqm::kNoAllocPs, (size_t)np, cudaMemcpyDeviceToHost, st);
+  // errors reported when a copy is issued (an invalid host pointer, for one)
+  // are not sticky, so each copy's status is checked here: a failed call
+  // returns before the counts are written
+  const struct {
+    void *dst;
+    const void *src;
+    size_t bytes;
+  } copies[] = {{out->pointlist, R.M.pts, sizeof(double) * 2 * (size_t)np},
+                {out->trianglelist, stage + gqm::kNoAllocTri, sizeof(int) * 3 * (size_t)nt},
+                {out->neighborlist, stage + gqm::kNoAllocNbr, sizeof(int) * 3 * (size_t)nt},
+                {out->segmentlist, stage + gqm::kNoAllocSeg, sizeof(int) * 2 * (size_t)ns},
+                {out->tstatus, stage + gqm::kNoAllocTs, (size_t)nt},
+                {out->pstatus, stage + gqm::kNoAllocPs, (size_t)np}};
+  for (const auto &c : copies)
+    if (cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, st) != cudaSuccess) {
+      cudaStreamSynchronize(st);  // copies already issued finish before the caller reuses its arrays
+      return GQM_ERR_CUDA;
+    }
   if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_ERR_CUDA;
   out->numberofpoints = np;
   out->numberoftriangles = nt;

@@ -57,7 +57,8 @@ class Stats(ctypes.Structure):
 class Probe(ctypes.Structure):
     _fields_ = [("check_launches", ctypes.c_longlong), ("check_items", ctypes.c_longlong),
                 ("check_ms", ctypes.c_double), ("loop_launches", ctypes.c_longlong), ("loop_ms", ctypes.c_double),
-                ("first_items", ctypes.c_longlong * 4)]
+                ("first_items", ctypes.c_longlong * 4), ("small_launches", ctypes.c_longlong),
+                ("small_items", ctypes.c_longlong), ("small_winners", ctypes.c_longlong), ("small_ms", ctypes.c_double)]
 
     def as_dict(self):
         d = {k: getattr(self, k) for k, _ in self._fields_ if k != "first_items"}
@@ -77,6 +78,41 @@ class BatchReport(ctypes.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class Tuning(ctypes.Structure):
+    """gqm_tuning: launch shape of a context's flip-flop loop (0 = default)."""
+    _fields_ = [("step_grid", ctypes.c_int), ("small_limit", ctypes.c_int), ("small_cluster", ctypes.c_int),
+                ("check_blocks_per_sm", ctypes.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+ARITH_SEPARATE, ARITH_CONTRACTED = 0, 1
+
+
+def arithmetic() -> int:
+    """ARITH_SEPARATE or ARITH_CONTRACTED: how the loaded library's refiner
+    kernels round (see gqm_arithmetic in include/gqm_refine.h)."""
+    return int(lib().gqm_arithmetic())
+
+
+def set_default_tuning(device=0, step_grid=0, small_limit=0, small_cluster=0, check_blocks_per_sm=0):
+    """Launch shape of the context refine() uses on `device` (gqm_set_default_tuning)."""
+    t = Tuning(step_grid, small_limit, small_cluster, check_blocks_per_sm)
+    rc = lib().gqm_set_default_tuning(int(device), ctypes.byref(t))
+    if rc != 0:
+        raise RefineError(rc, lib().gqm_status_string(rc).decode())
+
+
+def use_library(path):
+    """Load the refiner from another in-tree build (e.g. libgqm_b200_fma.so,
+    the contracted-arithmetic variant) for the calls that follow."""
+    global _lib
+    _native.CUDA_LIB = path
+    _lib = None
+    return lib()
 
 
 class RefineError(RuntimeError):
@@ -146,6 +182,17 @@ def lib() -> ctypes.CDLL:
             L.gqm_mlp_train.argtypes = [ctypes.c_int, fp, fp, fp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_float, ctypes.c_uint, fp]
             L.gqm_mlp_train.restype = ctypes.c_int
+        L.gqm_context_set_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
+        L.gqm_context_set_tuning.restype = ctypes.c_int
+        L.gqm_context_get_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
+        L.gqm_context_get_tuning.restype = ctypes.c_int
+        L.gqm_context_autotune.argtypes = [ctypes.c_void_p, ctypes.POINTER(CdtIn), ctypes.c_int,
+                                           ctypes.POINTER(Options), ctypes.c_int, ctypes.POINTER(Tuning),
+                                           ctypes.POINTER(ctypes.c_double)]
+        L.gqm_context_autotune.restype = ctypes.c_int
+        L.gqm_arithmetic.restype = ctypes.c_int
+        L.gqm_set_default_tuning.argtypes = [ctypes.c_int, ctypes.POINTER(Tuning)]
+        L.gqm_set_default_tuning.restype = ctypes.c_int
         L.gqm_context_probe.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.gqm_context_probe.restype = ctypes.c_int
         L.gqm_context_probe_read.argtypes = [ctypes.c_void_p, ctypes.POINTER(Probe)]
@@ -489,6 +536,32 @@ class Context:
         if rc != 0:
             raise RefineError(rc, "flip profile")
         return list(st), list(it)
+
+    def set_tuning(self, step_grid=0, small_limit=0, small_cluster=0, check_blocks_per_sm=0):
+        """Launch shape of the flip-flop loop (gqm_context_set_tuning); 0 keeps
+        a field's default, small_limit < 0 turns the small-step kernel off."""
+        t = Tuning(step_grid, small_limit, small_cluster, check_blocks_per_sm)
+        rc = self._lib.gqm_context_set_tuning(self._h, ctypes.byref(t))
+        if rc != 0:
+            raise RefineError(rc, self._lib.gqm_status_string(rc).decode())
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        rc = self._lib.gqm_context_get_tuning(self._h, ctypes.byref(t))
+        if rc != 0:
+            raise RefineError(rc, "tuning")
+        return t.as_dict()
+
+    def autotune(self, cdt: CDT, opt: Options, repeats=1):
+        """gqm_context_autotune on a host-array input: returns (chosen shape, its ms)."""
+        keep = []
+        cin = _cdt_in(cdt, keep)
+        t, ms = Tuning(), ctypes.c_double()
+        rc = self._lib.gqm_context_autotune(self._h, ctypes.byref(cin), 0, ctypes.byref(opt), int(repeats),
+                                            ctypes.byref(t), ctypes.byref(ms))
+        if rc != 0:
+            raise RefineError(rc, self._lib.gqm_status_string(rc).decode())
+        return t.as_dict(), ms.value
 
     def probe(self, enable=True):
         """Reset and enable (or disable) the launch timer of the flip-step check

@@ -127,11 +127,13 @@ int gqm_context_result(gqm_context *ctx, gqm_cdt_out *out);
 /* Sizes of the last result without copying it. */
 int gqm_context_result_sizes(gqm_context *ctx, int *npoints, int *ntriangles, int *nsegments);
 /* Measurement probe (no counterpart in the reference).  While enabled, the
- * flip-step check kernel (the refinement's most time-consuming kernel)
- * timestamps every launch on the device: from its first block's start to its
- * last block's end (%globaltimer), and CUDA events on the context's stream
- * bracket every launch of the flip loop.  gqm_context_probe(ctx, 1) resets and
- * enables, (ctx, 0) disables; gqm_context_probe_read sums since the reset. */
+ * two kernels that take most of the device time, the grid-wide flip-step check
+ * kernel and the small-step kernel (whole flip steps of small active sets in
+ * one launch), timestamp every launch on the device: from its first block's
+ * start to its last block's end (%globaltimer); CUDA events on the context's
+ * stream bracket every launch of the flip loop.  gqm_context_probe(ctx, 1)
+ * resets and enables, (ctx, 0) disables; gqm_context_probe_read sums since the
+ * reset. */
 typedef struct {
   long long check_launches; /* launches of the flip-step check kernel */
   long long check_items;    /* active triangles they checked */
@@ -139,6 +141,10 @@ typedef struct {
   long long loop_launches;  /* flip-loop graph launches */
   double loop_ms;           /* their summed time (CUDA events) */
   long long first_items[4]; /* active triangles of the first four check launches */
+  long long small_launches; /* launches of the small-step kernel */
+  long long small_items;    /* active triangles of the flip steps they ran */
+  long long small_winners;  /* flips and flops those steps applied */
+  double small_ms;          /* their summed execution time */
 } gqm_probe;
 int gqm_context_probe(gqm_context *ctx, int enable);
 int gqm_context_probe_read(gqm_context *ctx, gqm_probe *p);
@@ -150,13 +156,49 @@ int gqm_context_flip_profile(gqm_context *ctx, long long *steps, long long *item
 /* The CUDA stream the context launches on (a cudaStream_t). */
 void *gqm_context_stream(gqm_context *ctx);
 
+/* Launch shape of a context's flip-flop loop.  Replaces the reference's fixed
+ * BLOCK_SIZE (GPU_Refine/refine.h:19) and its per-kernel grid sizes
+ * (maxnumofblock, GPU_Refine/refine.cu:5223,5238,6538) for the loop that takes
+ * most of the device time (flipFlop, refine.cu:2328-2490).  No field changes a
+ * result: every flip step makes the reference's decisions whatever the launch
+ * shape.  Zero in a field means its default. */
+typedef struct {
+  int step_grid;           /* blocks of 256 threads of each grid-wide flip-step kernel (default 592, 4 per SM) */
+  int small_limit;         /* flip steps of at most this many active triangles run inside one launch of the
+                              small-step kernel (default 2048; negative: never) */
+  int small_cluster;       /* small-step kernel: 1 = one block of 512 threads (default); 8 or 16 = one
+                              thread-block cluster of that many 256-thread blocks */
+  int check_blocks_per_sm; /* register budget of the flip-step check kernel: 2 resident 256-thread blocks
+                              per SM (default; at most 128 registers) or 1 (up to 255) */
+} gqm_tuning;
+/* Set / read a context's launch shape.  Set returns GQM_ERR_ARGUMENT for a
+ * value out of range and GQM_ERR_CUDA when the device cannot run the requested
+ * cluster size; the context keeps its previous shape then. */
+int gqm_context_set_tuning(gqm_context *ctx, const gqm_tuning *t);
+int gqm_context_get_tuning(gqm_context *ctx, gqm_tuning *t);
+/* Autotuner (no counterpart in the reference): refines `in` (host or device
+ * arrays, as gqm_context_run) once per candidate launch shape, one field at a
+ * time (check kernel budget, small-step kernel, small-step limit, step grid),
+ * keeping each field's fastest value by the device time of the refinement
+ * (the best of `repeats` runs, at least 1).  The chosen shape is set on the
+ * context and written to *chosen; *best_ms (may be NULL) receives its time.
+ * `in` is typically a sample of the workload to be refined; its result is
+ * left in the context like any run's. */
+int gqm_context_autotune(gqm_context *ctx, const gqm_cdt_in *in, int in_on_device, const gqm_options *opt,
+                         int repeats, gqm_tuning *chosen, double *best_ms);
+/* Launch shape of the context that gqm_refine keeps for `device` (created by
+ * this call when it does not exist yet), e.g. a shape gqm_context_autotune
+ * chose on a sample of the caller's workload. */
+int gqm_set_default_tuning(int device, const gqm_tuning *t);
+
 /* Copy the last result of `ctx` into arrays the caller already owns, without
  * allocating any memory, host or device.
  *
  * No counterpart in the reference: its result path always allocates (new[] on
  * the host, device_vector on the GPU).  gqm_context_result() above also
- * allocates: it mallocs the host arrays and cudaMallocs device staging buffers
- * for every call, and cudaFree synchronizes the whole device.  Callers that
+ * allocates: it mallocs the host arrays on every call, and it grows its device
+ * and pinned staging buffers (cudaMalloc, and a cudaFree that synchronizes the
+ * whole device) whenever a result larger than any before arrives.  Callers that
  * cannot do that - a service that fixes its device memory budget at start-up
  * and reads many small results in a steady-state loop, or code sharing the GPU
  * with work that must not be stalled by an implicit device-wide sync - use
@@ -260,6 +302,19 @@ int gqm_mlp_train(int device, float *params, const float *features, const float 
 
 const char *gqm_status_string(int status);
 int gqm_version(void);
+
+/* Floating-point arithmetic the library's refiner kernels were compiled with.
+ * GQM_ARITH_SEPARATE (libgqm_b200.so): every product and sum rounded on its
+ * own (nvcc -fmad=false), the arithmetic of the reference built with
+ * -fmad=false, which the CPU oracle restates.  GQM_ARITH_CONTRACTED
+ * (libgqm_b200_fma.so): nvcc's default contraction of a product feeding an
+ * add or subtract into one fused multiply-add, the arithmetic of the reference
+ * as its project builds it (GPU_Refine/GPU_Refine.vcxproj sets no -fmad
+ * option).  The two give different meshes wherever a rounding decides a
+ * predicate or moves a Steiner point. */
+#define GQM_ARITH_SEPARATE 0
+#define GQM_ARITH_CONTRACTED 1
+int gqm_arithmetic(void);
 
 #ifdef __cplusplus
 }

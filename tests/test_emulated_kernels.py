@@ -223,3 +223,36 @@ def test_sharded_batch_default_engine_single_rank(emulated):
         want, _ = oracle_py.refine(d, t, 1, 1)
         for f in FIELDS:
             assert np.array_equal(getattr(g, f).view(np.uint8), getattr(want, f).view(np.uint8)), f
+
+
+@pytest.mark.parametrize("shape", [dict(small_cluster=8), dict(small_cluster=16, small_limit=8192),
+                                   dict(small_limit=-1), dict(check_blocks_per_sm=1, step_grid=296)])
+def test_emulated_launch_shapes_match_oracle(emulated, shape):
+    """Every launch shape of the flip-flop loop (the one-block and cluster
+    small-step kernels, grid steps only, another check-kernel budget) runs
+    the same steps: the oracle's output byte for byte."""
+    cdt = inputs.plain_small(seed=305, n=3000, nseg=150)
+    ctx = refine.Context(0)
+    try:
+        ctx.set_tuning(**shape)
+        assert all(ctx.tuning()[k] == v for k, v in shape.items())
+        ctx.run_host(cdt, refine.make_options(20.0, 1, 1))
+        got = ctx.result()
+    finally:
+        ctx.close()
+    want, _ = oracle_py.refine(cdt, 20.0, 1, 1)
+    _same(got, want)
+
+
+def test_emulated_autotune(emulated):
+    cdt = inputs.plain_small(seed=306, n=2000, nseg=100)
+    ctx = refine.Context(0)
+    try:
+        chosen, ms = ctx.autotune(cdt, refine.make_options(20.0, 1, 1))
+        assert chosen == ctx.tuning() and ms > 0
+        ctx.run_host(cdt, refine.make_options(20.0, 1, 1))
+        got = ctx.result()
+    finally:
+        ctx.close()
+    want, _ = oracle_py.refine(cdt, 20.0, 1, 1)
+    _same(got, want)

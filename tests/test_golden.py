@@ -8,8 +8,10 @@ digest trace of every flip step of those runs.
 The reference is not deterministic: two winners of one launch can store the
 two orientations of one subsegment into subseg2tri, and which store lands
 depends on timing (the runs then differ in which slots the same triangles
-occupy, and later in the mesh).  The oracle fixes that choice (the larger
-value wins).  So the oracle is held to:
+occupy, and later in the mesh).  The oracle fixes that choice by the order in
+which such stores were seen to land on a B200: within a warp the later store
+instruction, for two lanes of one instruction the lower lane, across warps
+the lower warp.  So the oracle is held to:
 
 * every flip step on which all reference runs agree: the oracle's trace line
   (digests of triangles, neighbours, subsegments, status, active list and

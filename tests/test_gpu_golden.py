@@ -1,13 +1,68 @@
-"""The sm_100a refiner against the reference's own runs: wherever every run of
-the reference produced the same output (all golden configurations whose runs
-agree, including those too large for the CPU oracle), the refiner's output
-is that output, byte for byte."""
+"""The sm_100a refiner against the reference's own runs.
+
+* libgqm_b200.so (every product and sum rounded on its own, -fmad=false):
+  wherever every run of the reference built with -fmad=false produced the same
+  output (all golden configurations whose runs agree, including those too large
+  for the CPU oracle), the refiner's output is that output, byte for byte.
+* libgqm_b200_fma.so (nvcc's default FMA contraction): wherever every run of
+  the reference as its project builds it (no -fmad option, so contraction on)
+  produced the same output, the contracted refiner's output is that output,
+  byte for byte.
+* Wherever the reference's runs differ (two winners of one launch racing to
+  store the two orientations of one subsegment, GPU_Refine/refine.cu:
+  1362-1372 and the like), the refiner's output sizes lie within the spread of
+  the reference's recorded runs (tests/golden/reference_spread.json), widened
+  by the spread's own width or 0.1 % of the size, whichever is larger.
+"""
+import json
+import os
+
 import pytest
 
-from gpu_cdt_refine_b200 import refine
+from gpu_cdt_refine_b200 import _native, refine
 from test_golden import configs, digests, golden_input, load
 
 pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SPREAD = os.path.join(HERE, "golden", "reference_spread.json")
+FMA_LIB = os.path.join(os.path.dirname(HERE), "gpu_cdt_refine_b200", "libgqm_b200_fma.so")
+
+
+def _spread():
+    with open(SPREAD) as f:
+        return json.load(f)
+
+
+def _spread_entry(name, cfg):
+    for e in _spread()["cases"][name]:
+        if (e["theta"], e["policy"], e["mode"]) == (cfg["theta"], cfg["policy"], cfg["mode"]):
+            return e
+    raise KeyError((name, cfg["theta"], cfg["policy"], cfg["mode"]))
+
+
+def _missing():
+    return [pytest.param(None, None, marks=pytest.mark.skip(reason="tests/golden/reference_spread.json missing"))]
+
+
+def contracted_configs():
+    """Golden configurations on which every recorded run of the reference as
+    built by its project (FMA contraction) gave the same output."""
+    if not os.path.exists(SPREAD):
+        return _missing()
+    out = []
+    for p in configs():
+        name, cfg = p.values
+        e = _spread_entry(name, cfg)
+        if e["fma_self_consistent"] and e["fma_sha256"] == cfg["fma"]["sha256"]:
+            out.append(p)
+    return out
+
+
+def varying_configs():
+    if not os.path.exists(SPREAD):
+        return _missing()
+    return [p for p in configs() if not p.values[1]["self_consistent"]]
 
 
 @pytest.mark.parametrize("name,cfg", configs(consistent_only=True))
@@ -18,3 +73,33 @@ def test_gpu_matches_reference(gpu, name, cfg):
     assert (got.numberofpoints, got.numberoftriangles, got.numberofsegments) == (
         ref["points"], ref["triangles"], ref["segments"])
     assert digests(got) == ref["sha256"]
+
+
+@pytest.fixture(scope="module")
+def contracted():
+    saved = _native.CUDA_LIB
+    refine.use_library(FMA_LIB)
+    assert refine.arithmetic() == refine.ARITH_CONTRACTED
+    yield
+    refine.use_library(saved)
+
+
+@pytest.mark.parametrize("name,cfg", contracted_configs())
+def test_contracted_matches_reference_as_built(gpu, contracted, name, cfg):
+    got, _ = refine.refine(golden_input(name), cfg["theta"], cfg["policy"], cfg["mode"])
+    ref = cfg["fma"]
+    assert (got.numberofpoints, got.numberoftriangles, got.numberofsegments) == (
+        ref["points"], ref["triangles"], ref["segments"])
+    assert digests(got) == ref["sha256"]
+
+
+@pytest.mark.parametrize("name,cfg", varying_configs())
+def test_sizes_within_reference_spread(gpu, name, cfg):
+    got, _ = refine.refine(golden_input(name), cfg["theta"], cfg["policy"], cfg["mode"])
+    sizes = [[r["points"], r["triangles"], r["segments"]] for r in cfg["runs"]]
+    sizes += _spread_entry(name, cfg)["nofma_sizes"]
+    mine = (got.numberofpoints, got.numberoftriangles, got.numberofsegments)
+    for k, what in enumerate(("points", "triangles", "segments")):
+        lo, hi = min(s[k] for s in sizes), max(s[k] for s in sizes)
+        slack = max(hi - lo, 0.001 * hi)
+        assert lo - slack <= mine[k] <= hi + slack, (what, mine[k], lo, hi)
