@@ -16,7 +16,8 @@ class _Cert(ctypes.Structure):
                 ("triangles_below_theta", ctypes.c_longlong), ("euler_defect", ctypes.c_longlong),
                 ("min_angle_deg", ctypes.c_double), ("theta", ctypes.c_double),
                 ("max_segment_deviation", ctypes.c_double), ("exempted", ctypes.c_longlong),
-                ("quality_violations", ctypes.c_longlong), ("goodcos2", ctypes.c_double)]
+                ("quality_violations", ctypes.c_longlong), ("goodcos2", ctypes.c_double),
+                ("tie_passed", ctypes.c_longlong)]
 
 
 def certify(out: CDT, inp: CDT, theta: float, goodcos2: float = 0.0) -> dict:
@@ -27,7 +28,10 @@ def certify(out: CDT, inp: CDT, theta: float, goodcos2: float = 0.0) -> dict:
     every triangle with an angle below theta (decided exactly against
     goodcos2, the FP64 cos^2(theta) of the refiner's bad-triangle test; 0 = the
     host's cos()) is one the reference's equidistant-split exemption covers
-    (``exempted``); the others are ``quality_violations``.  ``min_angle_deg``
+    (``exempted``, GPU_Refine/refine.cu:426-493) or one the reference's FP64
+    smallest-angle test passes because its two shortest edges compare equal
+    and the test then measures the angle opposite edge 2 (``tie_passed``,
+    refine.cu:343-358); the others are ``quality_violations``.  ``min_angle_deg``
     reports the smallest angle.
     """
     lib = _native.host()

@@ -36,8 +36,19 @@
 //      exactly for the FP64 constants 0.999 and 1.001).  Split points and
 //      their input segments come from the segment walk of check 3.  A
 //      triangle below theta that the exemption does not cover is a quality
-//      violation and fails the certificate;
-//   7. minimum angle statistics (degrees, FP64 atan2 of exact-enough
+//      violation and fails the certificate, unless rule 7 covers it;
+//   7. the reference's smallest-angle routine (GPU_Refine/refine.cu:317-374)
+//      picks the shortest edge with strict comparisons of FP64 squared
+//      lengths, so when the two shortest edges compare equal it falls through
+//      to edge 2 and measures the angle opposite edge 2 instead of the
+//      smallest one.  An isosceles triangle whose equal legs are its two
+//      shortest edges (an off-center on the bisector of a short edge makes
+//      them) can then pass the reference's bad test with an apex angle below
+//      theta.  A triangle below theta is "tie_passed" when the reference's
+//      FP64 test, evaluated as the reference writes it (every operation
+//      rounded on its own), takes such a tie and judges the triangle good
+//      (refine.cu:418-419);
+//   8. minimum angle statistics (degrees, FP64 atan2 of exact-enough
 //      cross/dot products).
 #include <algorithm>
 #include <cmath>
@@ -58,6 +69,7 @@ struct gqm_certificate {
   long long exempted;            /* triangles below theta that the reference's exemption covers */
   long long quality_violations;  /* triangles below theta that it does not */
   double goodcos2;               /* the cos^2(theta) the quality test used */
+  long long tie_passed;          /* triangles below theta that the reference's FP64 test passes on a length tie */
 };
 
 }  // extern "C"
@@ -115,6 +127,27 @@ int angle_below(const gqm_pt &o, const gqm_pt &p, const gqm_pt &q, double c2) {
   const Exp elu = ex_add(ex_mul(eux, eux), ex_mul(euy, euy)), elw = ex_add(ex_mul(ewx, ewx), ex_mul(ewy, ewy));
   const Exp d = ex_add(ex_mul(edot, edot), ex_neg(ex_scale(ex_mul(elu, elw), c2)));
   return ex_sign(d);
+}
+// The reference's bad-triangle test in FP64 (GPU_Refine/refine.cu:317-374,
+// 418-419) for a triangle (apex, org, dest), every operation rounded on its
+// own (this file is compiled with -ffp-contract=off).  Returns true when the
+// two shortest edges' squared lengths compare equal, so that the strict
+// comparisons fall through to edge 2, and the cos^2 then measured is at most
+// goodcos2 (the triangle passes as good).
+bool reference_tie_passes(const gqm_pt &apex, const gqm_pt &org, const gqm_pt &dest, double goodcos2) {
+  double dxod = org.x - dest.x, dyod = org.y - dest.y;
+  double dxda = dest.x - apex.x, dyda = dest.y - apex.y;
+  double dxao = apex.x - org.x, dyao = apex.y - org.y;
+  double dxod2 = dxod * dxod, dyod2 = dyod * dyod, dxda2 = dxda * dxda, dyda2 = dyda * dyda;
+  double dxao2 = dxao * dxao, dyao2 = dyao * dyao;
+  const double len_org = dxod2 + dyod2, len_dest = dxda2 + dyda2, len_apex = dxao2 + dyao2;
+  if (len_org < len_dest && len_org < len_apex) return false;
+  if (len_dest < len_org && len_dest < len_apex) return false;
+  // edge 2 is taken; a tie only if edge 2 is not itself strictly the shortest
+  if (len_apex < len_org && len_apex < len_dest) return false;
+  const double dot = dxod * dxda + dyod * dyda;
+  const double cos2 = dot * dot * len_apex / (len_org * len_dest * len_apex);
+  return cos2 <= goodcos2;
 }
 // exact squared distance of a and b
 Exp ex_dist2(const gqm_pt &a, const gqm_pt &b) {
@@ -314,6 +347,8 @@ int gqm_certify(int np, const double *pts, int nt, const int *tri, const int *nb
     }
     if (exempt)
       c->exempted++;
+    else if (reference_tie_passes(P[v[0]], P[v[1]], P[v[2]], goodcos2))
+      c->tie_passed++;
     else
       c->quality_violations++;
   }

@@ -69,3 +69,32 @@ def test_angle_test_is_exact_at_the_threshold():
     assert below == (1 if exact > 0 else 0)
     assert certify(tri, tri, 36.0, goodcos2=np.nextafter(c2, 0.0))["triangles_below_theta"] == 1
     assert certify(tri, tri, 36.0, goodcos2=np.nextafter(c2, 1.0))["triangles_below_theta"] == 0
+
+
+def _one_triangle(order):
+    """One flat isosceles triangle (base (0,0)-(2,0), top (1, 0.25): base
+    angles 14.04 degrees, legs of exactly equal FP64 length), all three edges
+    input segments, with its vertices listed starting at `order`."""
+    from gpu_cdt_refine_b200.cdtio import CDT
+    pts = np.array([[0.0, 0.0], [2.0, 0.0], [1.0, 0.25]])
+    tri = np.roll(np.array([0, 1, 2], dtype=np.int32), -order).reshape(1, 3)
+    return CDT(pointlist=pts, trianglelist=tri, neighborlist=np.full((1, 3), -1, dtype=np.int32),
+               segmentlist=np.array([[0, 1], [1, 2], [2, 0]], dtype=np.int32))
+
+
+@pytest.mark.parametrize("order,passes", [(0, True), (1, False), (2, False)])
+def test_length_tie_of_the_reference_test(order, passes):
+    """The reference's smallest-angle routine (GPU_Refine/refine.cu:317-374)
+    takes edge 2 whenever its strict comparisons of edges 0 and 1 tie.  Listed
+    as (0,0), (2,0), (1,0.25) the two equal legs are edges 0 and 1: edge 2 is
+    the base and the angle measured is the 152-degree top angle, so the
+    reference's test passes the triangle (tie_passed).  In the other two
+    vertex orders edge 2 is one of the legs and the test measures a 14-degree
+    base angle: a quality violation."""
+    c = _one_triangle(order)
+    cert = certify(c, c, 20.0)
+    assert cert["triangles_below_theta"] == 1 and cert["exempted"] == 0
+    assert cert["tie_passed"] == (1 if passes else 0)
+    assert cert["quality_violations"] == (0 if passes else 1)
+    assert cert["ok"] == passes
+    assert cert["min_angle_deg"] == pytest.approx(np.degrees(np.arctan(0.25)), abs=1e-9)
