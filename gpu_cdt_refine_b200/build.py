@@ -7,14 +7,18 @@ libgqm_b200.so : refine.cu (kernels, driver, C ABI) + batch.cu (persistent
                  (small flip steps on a thread-block cluster) + learned.cu (placement network training and
                  inference) + cdt_gpu.cu (CDT construction on the GPU) +
                  legacy.cpp (C++ drop-in)
-libgqm_b200_fma.so : the same with the refiner's kernels compiled under nvcc's
-                 default FMA contraction (-fmad=true), the arithmetic of the
-                 reference as its own project builds it
+libgqm_b200_fma.so : the same with GQM_CONTRACTED set: the products that the
+                 reference as its own project builds it (nvcc's default
+                 contraction) fuses into an add or subtract are fused here
+                 too, written out as fma() (gqm_madd in predicates.h)
 libgqm_host.so : cdt_build.cpp + synth.cpp + certify.cpp + regions.cpp
 
-In libgqm_b200.so every floating-point operation of the refiner is rounded on
-its own: nvcc -fmad=false and gcc -ffp-contract=off, the same arithmetic as
-the reference built with -fmad=false, which the CPU oracle restates.
+Both are compiled without compiler contraction (nvcc -fmad=false, gcc
+-ffp-contract=off), so the arithmetic is exactly the one the source writes: in
+libgqm_b200.so every floating-point operation of the refiner is rounded on its
+own (the reference built with -fmad=false), in libgqm_b200_fma.so the fused
+products are the reference build's own.  The CPU oracle restates both
+(oracle/_build/libgqm_oracle.so and libgqm_oracle_fma.so).
 """
 from __future__ import annotations
 
@@ -53,13 +57,12 @@ def build_host(force=False):
 # Refiner translation units: compiled once per arithmetic variant.
 REFINER_UNITS = ("refine.cu", "batch.cu", "flipcl.cu")
 # The arithmetic variants of the refiner:
-#   "separate"   every product and sum rounded on its own (-fmad=false): the
-#                reference built with -fmad=false, which the oracle restates;
-#   "contracted" nvcc's default contraction of a product feeding an add or a
-#                subtract into one fused multiply-add (-fmad=true): the
-#                reference as its project builds it (no -fmad option set).
+#   "separate"   every product and sum rounded on its own: the reference built
+#                with -fmad=false;
+#   "contracted" GQM_CONTRACTED=1: fma() exactly where the reference as its
+#                project builds it (no -fmad option, so nvcc contracts) fuses.
 VARIANTS = {"separate": ("libgqm_b200.so", "-fmad=false", "_build"),
-            "contracted": ("libgqm_b200_fma.so", "-fmad=true", os.path.join("_build", "fma"))}
+            "contracted": ("libgqm_b200_fma.so", "-fmad=false", os.path.join("_build", "fma"))}
 
 
 def _cuda_jobs(force=False, extra=None, variant="separate"):

@@ -727,13 +727,20 @@ __global__ void __launch_bounds__(NT, MINB) k_batch(Job *jobs, const int *order,
 // phases, compiled in block mode, separated by barriers), then it re-sets the
 // loop condition.  The steps and their results are the ones the grid kernels
 // would produce (every phase is decided by the reference's rules, not by the
-// thread layout).
+// thread layout).  The loop's control block (list lengths, stamps'
+// generation, launch epoch) is worked on in shared memory and written back
+// at exit: a step of a few triangles is a chain of dependent memory accesses,
+// and every counter read or atomic on shared memory instead of global memory
+// takes one L2 round trip out of that chain.
 constexpr int kSmallThreads = 512;
 template <int PRED>
 __global__ void __launch_bounds__(kSmallThreads, 1)
-    k_flip_small(Mesh M, FlipCtl *fc, int *act, uint8_t *clr, int *win, int *ll, int *sl, int *fq, int *tl,
+    k_flip_small(Mesh M, FlipCtl *gfc, int *act, uint8_t *clr, int *win, int *ll, int *sl, int *fq, int *tl,
                  int limit, cudaGraphConditionalHandle h, int graph, KTimer *tm) {
   __shared__ int go;
+  __shared__ FlipCtl sfc;
+  FlipCtl *fc = &sfc;
+  if (threadIdx.x == 0) sfc = *gfc;
   const int timed = tm->on;
   const unsigned long long start = timed ? global_ns() : 0;
   long long items = 0, wins = 0;  // thread 0's count of the launch's work (probe only)
@@ -767,6 +774,7 @@ __global__ void __launch_bounds__(kSmallThreads, 1)
     }
     SYNC();
   }
+  if (threadIdx.x == 0) *gfc = sfc;
 #ifndef GQM_HOST_EMU
   if (graph && threadIdx.x == 0) cudaGraphSetConditional(h, fc->cond);
 #endif

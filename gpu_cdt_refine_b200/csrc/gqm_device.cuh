@@ -127,6 +127,31 @@ __device__ __forceinline__ int win_rank(const Mesh &M, int index) {
     if ((c << 5) + j < w) b += __popc(M.wbits[(c << 5) + j]);
   return r + b + __popc(M.wbits[w] & ((1u << (index & 31)) - 1u));
 }
+// Slot in a list whose length *n many threads bump at once: the lanes of a
+// warp that arrive together take consecutive slots with one atomic, issued by
+// the lowest of them, instead of one atomic each on the same word.  The order
+// of the entries within a list is not used by any step.
+__device__ __forceinline__ int list_slot(int *n) {
+#ifdef GQM_HOST_EMU
+  return atomicAdd(n, 1);
+#else
+  const unsigned m = __activemask();
+  const int lane = (int)(threadIdx.x & 31u), leader = __ffs(m) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(n, __popc(m));
+  base = __shfl_sync(m, base, leader);
+  return base + __popc(m & ((1u << lane) - 1u));
+#endif
+}
+// The same for an event counter: one atomic per warp.
+__device__ __forceinline__ void count_event(unsigned long long *c) {
+#ifdef GQM_HOST_EMU
+  atomicAdd(c, 1ull);
+#else
+  const unsigned m = __activemask();
+  if ((int)(threadIdx.x & 31u) == __ffs(m) - 1) atomicAdd(c, (unsigned long long)__popc(m));
+#endif
+}
 // enter / leave the winner bitmap and its counts.  The two coarse counts
 // (2^15 and 2^20 slots) are few and hot, so the lanes of a warp that hit the
 // same one add together (one atomic per distinct counter); `on` says whether
@@ -204,11 +229,11 @@ __device__ __forceinline__ double incircle(double2 a, double2 b, double2 c, doub
 
 // checkseg4encroach, GPU_Refine/refine.cu:115-139 (goodcoss squared once).
 __device__ __forceinline__ bool encroached(double2 o, double2 d, double2 a, double gc2, int mode) {
-  double dot = (o.x - a.x) * (d.x - a.x) + (o.y - a.y) * (d.y - a.y);
+  double dot = gqm_madd(o.x - a.x, d.x - a.x, (o.y - a.y) * (d.y - a.y));
   if (dot < 0.0) {
     if (mode || dot * dot >= (2.0 * gc2 - 1.0) * (2.0 * gc2 - 1.0) *
-                                   ((o.x - a.x) * (o.x - a.x) + (o.y - a.y) * (o.y - a.y)) *
-                                   ((d.x - a.x) * (d.x - a.x) + (d.y - a.y) * (d.y - a.y)))
+                                   gqm_madd(o.x - a.x, o.x - a.x, (o.y - a.y) * (o.y - a.y)) *
+                                   gqm_madd(d.x - a.x, d.x - a.x, (d.y - a.y) * (d.y - a.y)))
       return true;
   }
   return false;

@@ -234,22 +234,24 @@ __device__ __forceinline__ double smallest_cos2(double2 pA, double2 pO, double2 
   double dxod = pO.x - pD.x, dyod = pO.y - pD.y;
   double dxda = pD.x - pA.x, dyda = pD.y - pA.y;
   double dxao = pA.x - pO.x, dyao = pA.y - pO.y;
-  double lenOrg = dxod * dxod + dyod * dyod;
-  double lenDest = dxda * dxda + dyda * dyda;
-  double lenApex = dxao * dxao + dyao * dyao;
+  // gqm_madd: the products the reference's contracted build fuses (see
+  // predicates.h); the sums are the same in either order
+  double lenOrg = gqm_madd(dyod, dyod, dxod * dxod);
+  double lenDest = gqm_madd(dyda, dyda, dxda * dxda);
+  double lenApex = gqm_madd(dxao, dxao, dyao * dyao);
   double ang, sh;
   if (lenOrg < lenDest && lenOrg < lenApex) {
     sh = lenOrg;
     *shortest = 0;
-    ang = dxda * dxao + dyda * dyao;
+    ang = gqm_madd(dyda, dyao, dxda * dxao);
   } else if (lenDest < lenOrg && lenDest < lenApex) {
     sh = lenDest;
     *shortest = 1;
-    ang = dxod * dxao + dyod * dyao;
+    ang = gqm_madd(dyod, dyao, dxod * dxao);
   } else {
     sh = lenApex;
     *shortest = 2;
-    ang = dxod * dxda + dyod * dyda;
+    ang = gqm_madd(dyod, dyda, dxod * dxda);
   }
   return ang * ang * sh / (lenOrg * lenDest * lenApex);
 }
@@ -303,8 +305,8 @@ GQM_KERNEL void k_mark_bad(Mesh M, int ntri) {
             double2 vo = (sh == 0) ? b : (sh == 1 ? c : a);
             double2 vd = (sh == 0) ? c : (sh == 1 ? a : b);
             double2 vc = M.pts[common];
-            double d1 = (vc.x - vo.x) * (vc.x - vo.x) + (vc.y - vo.y) * (vc.y - vo.y);
-            double d2 = (vc.x - vd.x) * (vc.x - vd.x) + (vc.y - vd.y) * (vc.y - vd.y);
+            double d1 = gqm_madd(vc.x - vo.x, vc.x - vo.x, (vc.y - vo.y) * (vc.y - vo.y));
+            double d2 = gqm_madd(vc.x - vd.x, vc.x - vd.x, (vc.y - vd.y) * (vc.y - vd.y));
             if ((d1 < 1.001 * d2) && (d1 > 0.999 * d2)) bad = false;
           }
         }
@@ -895,7 +897,7 @@ struct FlipQ {
 __device__ __forceinline__ void push_flag(const Mesh &M, const FlipQ &Q, int t) {
   M.tflip[t] = 1;
   int g = *Q.genp;
-  if (atomicExch(M.fstamp + t, g) != g) Q.q[atomicAdd(Q.qn, 1)] = t;
+  if (atomicExch(M.fstamp + t, g) != g) Q.q[list_slot(Q.qn)] = t;
 }
 struct TouchL {
   int *l;
@@ -904,7 +906,7 @@ struct TouchL {
 };
 __device__ __forceinline__ void touch(const Mesh &M, const TouchL &T, int t) {
   int g = *T.genp;
-  if (atomicExch(M.tstamp + t, g) != g) T.l[atomicAdd(T.n, 1)] = t;
+  if (atomicExch(M.tstamp + t, g) != g) T.l[list_slot(T.n)] = t;
 }
 __device__ __forceinline__ void claim(const Mesh &M, const TouchL &T, int t, int v) {
   atomicMin(M.tmark + t, v);
@@ -997,7 +999,7 @@ GQM_KERNEL void k_flip_filter(Mesh M, const int *q, const int *qn, int *act, int
   int n = *qn;
   GS_LOOP(k, n) {
     int t = q[k];
-    if (M.tflip[t] && (M.tst[t] & TS_NOTNULL)) act[atomicAdd(actn, 1)] = t;
+    if (M.tflip[t] && (M.tst[t] & TS_NOTNULL)) act[list_slot(actn)] = t;
   }
 }
 // tmark of the triangles claimed in this step back to "unclaimed"; also
@@ -1016,7 +1018,7 @@ GQM_KERNEL void k_flip_reset_filter(Mesh M, const int *tl, const int *tn, const 
   GS_LOOP(k, nt) M.tmark[tl[k]] = kMaxInt;
   GS_LOOP(k, nq) {
     const int t = q[k];
-    if (M.tflip[t] && (M.tst[t] & TS_NOTNULL)) act[atomicAdd(nextn, 1)] = t;
+    if (M.tflip[t] && (M.tst[t] & TS_NOTNULL)) act[list_slot(nextn)] = t;
   }
 }
 
@@ -1235,7 +1237,7 @@ GQM_KERNEL void k_flip_winner2(Mesh M, const int *act, const int *dn, const uint
     const int k = base + lane;
     const int index = k < n ? act[k] : -1;
     const bool w = k < n && flip_winner(M, Q, index, clr[k]);
-    if (w) win[atomicAdd(winn, 1)] = index;
+    if (w) win[list_slot(winn)] = index;
     win_mark(M, index, w);
   }
 }
@@ -1385,7 +1387,7 @@ GQM_KERNEL void GQM_WALK_BOUNDS k_insert_mid(Mesh M, const int *mids, const int 
     int4 v0 = M.tv[tri[0]];
     int p[3] = {comp(v0, m3(triOri[0] + 1)), comp(v0, m3(triOri[0] + 2)), comp(v0, triOri[0])};
     double2 a = M.pts[p[0]], b = M.pts[p[1]], c = M.pts[p[2]];
-    double segmentlength = sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
+    double segmentlength = sqrt(gqm_madd(a.x - b.x, a.x - b.x, (a.y - b.y) * (a.y - b.y)));
     double split = 0.5;
     if (acuteorg || acutedest) {
       double npt = 1.0;
@@ -1394,14 +1396,14 @@ GQM_KERNEL void GQM_WALK_BOUNDS k_insert_mid(Mesh M, const int *mids, const int 
       split = npt / segmentlength;
       if (acutedest) split = 1.0 - split;
     }
-    double2 m = make_double2(a.x + (b.x - a.x) * split, a.y + (b.y - a.y) * split);
+    double2 m = make_double2(gqm_madd(b.x - a.x, split, a.x), gqm_madd(b.y - a.y, split, a.y));
     double multiplier = gqm_orient_ref(a.x, a.y, b.x, b.y, m.x, m.y);
-    double divisor = ((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
+    double divisor = gqm_madd(a.x - b.x, a.x - b.x, (a.y - b.y) * (a.y - b.y));
     if ((multiplier != 0.0) && (divisor != 0.0)) {
       multiplier = multiplier / divisor;
       if (multiplier == multiplier) {
-        m.x += multiplier * (b.y - a.y);
-        m.y += multiplier * (a.x - b.x);
+        m.x = gqm_madd(multiplier, b.y - a.y, m.x);
+        m.y = gqm_madd(multiplier, a.x - b.x, m.y);
       }
     }
     M.pts[newp] = m;
@@ -1459,7 +1461,7 @@ GQM_KERNEL void GQM_WALK_BOUNDS k_insert_mid(Mesh M, const int *mids, const int 
     M.enc[sindex] = e_s;
     M.enc[nsub + tindex] = e_n;
     imark[tindex] = -1;
-    atomicAdd(counter, 1ull);
+    count_event(counter);
   }
 }
 
@@ -1539,35 +1541,37 @@ GQM_KERNEL void k_points_old(Mesh M, int npts) {
 // computeCircumcenter, refine.cu:3780-3868
 __device__ __forceinline__ double2 circumcenter(double2 vApex, double2 vOrg, double2 vDest, double offConstant,
                                                 bool offcenter) {
+  // gqm_madd: the products the reference's contracted build fuses (see
+  // predicates.h); the sums are the same in either order
   double xdo = vDest.x - vOrg.x, ydo = vDest.y - vOrg.y;
   double xao = vApex.x - vOrg.x, yao = vApex.y - vOrg.y;
-  double dodist = xdo * xdo + ydo * ydo;
-  double aodist = xao * xao + yao * yao;
-  double dadist = (vDest.x - vApex.x) * (vDest.x - vApex.x) + (vDest.y - vApex.y) * (vDest.y - vApex.y);
+  double dodist = gqm_madd(xdo, xdo, ydo * ydo);
+  double aodist = gqm_madd(xao, xao, yao * yao);
+  double dadist = gqm_madd(vDest.x - vApex.x, vDest.x - vApex.x, (vDest.y - vApex.y) * (vDest.y - vApex.y));
   double tmp = xdo * yao - xao * ydo;
   double denominator = (tmp != 0) ? 0.5 / tmp : 0.5 / gqm_orient_ref(vDest.x, vDest.y, vApex.x, vApex.y, vOrg.x, vOrg.y);
-  double dx = (yao * dodist - ydo * aodist) * denominator;
-  double dy = (xdo * aodist - xao * dodist) * denominator;
+  double dx = gqm_madd(yao, dodist, -(ydo * aodist)) * denominator;
+  double dy = gqm_madd(xdo, aodist, -(xao * dodist)) * denominator;
   if (offcenter && (offConstant > 0.0)) {
     double dxoff, dyoff;
     if ((dodist < aodist) && (dodist < dadist)) {
       dxoff = 0.5 * xdo - offConstant * ydo;
-      dyoff = 0.5 * ydo + offConstant * xdo;
-      if (dxoff * dxoff + dyoff * dyoff < dx * dx + dy * dy) {
+      dyoff = gqm_madd(offConstant, xdo, 0.5 * ydo);
+      if (gqm_madd(dxoff, dxoff, dyoff * dyoff) < gqm_madd(dx, dx, dy * dy)) {
         dx = dxoff;
         dy = dyoff;
       }
     } else if (aodist < dadist) {
       dxoff = 0.5 * xao + offConstant * yao;
       dyoff = 0.5 * yao - offConstant * xao;
-      if (dxoff * dxoff + dyoff * dyoff < dx * dx + dy * dy) {
+      if (gqm_madd(dxoff, dxoff, dyoff * dyoff) < gqm_madd(dx, dx, dy * dy)) {
         dx = dxoff;
         dy = dyoff;
       }
     } else {
       dxoff = 0.5 * (vApex.x - vDest.x) - offConstant * (vApex.y - vDest.y);
-      dyoff = 0.5 * (vApex.y - vDest.y) + offConstant * (vApex.x - vDest.x);
-      if (dxoff * dxoff + dyoff * dyoff < (dx - xdo) * (dx - xdo) + (dy - ydo) * (dy - ydo)) {
+      dyoff = gqm_madd(offConstant, vApex.x - vDest.x, 0.5 * (vApex.y - vDest.y));
+      if (gqm_madd(dxoff, dxoff, dyoff * dyoff) < gqm_madd(dx - xdo, dx - xdo, (dy - ydo) * (dy - ydo))) {
         dx = xdo + dxoff;
         dy = ydo + dyoff;
       }
@@ -1637,7 +1641,8 @@ GQM_KERNEL void k_locate(Mesh M, const int *bad, const int *dn, const double2 *c
       bool moveleft;
       if (detLeft < 0.0) {
         if (detRight < 0.0)
-          moveleft = (u[pDest].x - u[pOrg].x) * (cc.x - u[pApex].x) + (u[pDest].y - u[pOrg].y) * (cc.y - u[pApex].y) >
+          moveleft = gqm_madd(u[pDest].x - u[pOrg].x, cc.x - u[pApex].x,
+                              (u[pDest].y - u[pOrg].y) * (cc.y - u[pApex].y)) >
                      0.0;
         else
           moveleft = true;
@@ -1919,7 +1924,7 @@ GQM_KERNEL void k_insert_steiner(Mesh M, const int *wl, const int *dn, const int
         M.tfo[tri3] = 0;
       }
     }
-    atomicAdd(counter, 1ull);
+    count_event(counter);
   }
 }
 

@@ -41,28 +41,54 @@ typedef struct {
 // Reference-compatible arithmetic
 // ---------------------------------------------------------------------------
 
-// cuda_fast / cuda_ccw with zero error bounds (cudaCCW.h:487-565).
+// Product-sum a * b + c of the reference's arithmetic.  The reference as its
+// project builds it (nvcc's default -fmad=true) fuses some of its products into
+// the add or subtract that consumes them; which ones was measured on its
+// compiled kernels and predicates by comparing their outputs with every
+// candidate evaluation.  With GQM_CONTRACTED set, the expressions of the
+// reference's arithmetic use gqm_madd (one rounding, fma) exactly where that
+// build fuses; without it gqm_madd rounds the product and the sum on their own
+// (the reference built with -fmad=false).  Both variants are compiled without
+// compiler contraction (nvcc -fmad=false, gcc -ffp-contract=off), so the
+// arithmetic is the one written out here.
+#ifndef GQM_CONTRACTED
+#define GQM_CONTRACTED 0
+#endif
+GQM_HD double gqm_madd(double a, double b, double c) {
+#if GQM_CONTRACTED
+  return fma(a, b, c);
+#else
+  return a * b + c;
+#endif
+}
+
+// cuda_fast / cuda_ccw with zero error bounds (cudaCCW.h:487-565).  Both
+// products are rounded on their own in both builds of the reference (each is
+// also used by the sign tests and the error bound).
 GQM_HD double gqm_orient_ref(double ax, double ay, double bx, double by, double cx, double cy) {
   double detleft = (ax - cx) * (by - cy);
   double detright = (ay - cy) * (bx - cx);
   return detleft - detright;
 }
 
-// The plain incircle determinant of cuda_inCircle (cudaCCW.h:668-702).
+// The plain incircle determinant of cuda_inCircle (cudaCCW.h:668-702).  The
+// six cross products are rounded on their own in both builds of the reference
+// (each is also used by the error bound's permanent); its contracted build
+// fuses each lift's first square and the first and last terms of the sum.
 GQM_HD double gqm_incircle_det_ref(double pax, double pay, double pbx, double pby, double pcx, double pcy,
                                    double pdx, double pdy) {
   double adx = pax - pdx, bdx = pbx - pdx, cdx = pcx - pdx;
   double ady = pay - pdy, bdy = pby - pdy, cdy = pcy - pdy;
   double bdxcdy = bdx * cdy;
   double cdxbdy = cdx * bdy;
-  double alift = adx * adx + ady * ady;
+  double alift = gqm_madd(adx, adx, ady * ady);
   double cdxady = cdx * ady;
   double adxcdy = adx * cdy;
-  double blift = bdx * bdx + bdy * bdy;
+  double blift = gqm_madd(bdx, bdx, bdy * bdy);
   double adxbdy = adx * bdy;
   double bdxady = bdx * ady;
-  double clift = cdx * cdx + cdy * cdy;
-  return alift * (bdxcdy - cdxbdy) + blift * (cdxady - adxcdy) + clift * (adxbdy - bdxady);
+  double clift = gqm_madd(cdx, cdx, cdy * cdy);
+  return gqm_madd(clift, adxbdy - bdxady, gqm_madd(alift, bdxcdy - cdxbdy, blift * (cdxady - adxcdy)));
 }
 
 // --- expansion arithmetic with the reference's zero splitter ---------------

@@ -614,7 +614,7 @@ struct Refiner {
 #endif
   // steps whose active set has at most this many triangles run in one launch
 #ifndef GQM_SMALL_STEP
-#define GQM_SMALL_STEP 2048
+#define GQM_SMALL_STEP 1024
 #endif
   // Launch shape of the flip-flop loop (gqm_tuning).  None of it changes a
   // result: every step makes the reference's decisions whatever the grid.
@@ -1340,7 +1340,7 @@ int gqm_context_autotune(gqm_context *ctx, const gqm_cdt_in *in, int in_on_devic
   // device cannot run (a cluster size it cannot place) is skipped
   const int checks[] = {2, 1};
   const int clusters[] = {1, 8, 16};
-  const int limits[] = {1024, 2048, 4096, 8192};
+  const int limits[] = {512, 1024, 2048, 4096};
   const int grids[] = {148 * 2, 148 * 4, 148 * 8};
   for (int field = 0; field < 4; ++field) {
     const int *vals = field == 0 ? checks : field == 1 ? clusters : field == 2 ? limits : grids;

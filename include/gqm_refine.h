@@ -165,7 +165,7 @@ void *gqm_context_stream(gqm_context *ctx);
 typedef struct {
   int step_grid;           /* blocks of 256 threads of each grid-wide flip-step kernel (default 592, 4 per SM) */
   int small_limit;         /* flip steps of at most this many active triangles run inside one launch of the
-                              small-step kernel (default 2048; negative: never) */
+                              small-step kernel (default 1024; negative: never) */
   int small_cluster;       /* small-step kernel: 1 = one block of 512 threads (default); 8 or 16 = one
                               thread-block cluster of that many 256-thread blocks */
   int check_blocks_per_sm; /* register budget of the flip-step check kernel: 2 resident 256-thread blocks

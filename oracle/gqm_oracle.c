@@ -9,6 +9,11 @@
  *
  * Arithmetic.  Built with -ffp-contract=off: every FP64 operation is rounded
  * on its own, which matches the reference compiled with nvcc -fmad=false.
+ * Built with -DGQM_ORACLE_CONTRACTED=1 (libgqm_oracle_fma.so), madd() fuses
+ * the products that the reference as its project builds it (nvcc's default
+ * contraction) fuses, one rounding for the product and the add; which
+ * products those are was measured on the reference's compiled kernels and
+ * predicates, by comparing their outputs with every candidate evaluation.
  * The reference's device predicate constants are never initialised
  * (GPU_Refine/cudaCCW.h:41), so orientation is the plain determinant and
  * incircle falls back to an expansion with a zero splitter only when the plain
@@ -81,6 +86,18 @@ typedef struct {
   double x, y;
 } P2;
 
+#ifndef GQM_ORACLE_CONTRACTED
+#define GQM_ORACLE_CONTRACTED 0
+#endif
+/* a * b + c: fused where the reference's contracted build fuses, else two roundings */
+static inline double madd(double a, double b, double c) {
+#if GQM_ORACLE_CONTRACTED
+  return fma(a, b, c);
+#else
+  return a * b + c;
+#endif
+}
+
 /* ---------------- predicates (cudaCCW.h with zero constants) ---------------- */
 static double orient_ref(P2 a, P2 b, P2 c) {
   double detleft = (a.x - c.x) * (b.y - c.y);
@@ -92,12 +109,12 @@ static double incircle_det(P2 a, P2 b, P2 c, P2 d) {
   double adx = a.x - d.x, bdx = b.x - d.x, cdx = c.x - d.x;
   double ady = a.y - d.y, bdy = b.y - d.y, cdy = c.y - d.y;
   double bdxcdy = bdx * cdy, cdxbdy = cdx * bdy;
-  double alift = adx * adx + ady * ady;
+  double alift = madd(adx, adx, ady * ady);
   double cdxady = cdx * ady, adxcdy = adx * cdy;
-  double blift = bdx * bdx + bdy * bdy;
+  double blift = madd(bdx, bdx, bdy * bdy);
   double adxbdy = adx * bdy, bdxady = bdx * ady;
-  double clift = cdx * cdx + cdy * cdy;
-  return alift * (bdxcdy - cdxbdy) + blift * (cdxady - adxcdy) + clift * (adxbdy - bdxady);
+  double clift = madd(cdx, cdx, cdy * cdy);
+  return madd(clift, adxbdy - bdxady, madd(alift, bdxcdy - cdxbdy, blift * (cdxady - adxcdy)));
 }
 
 /* error-free transforms, cudaCCW.h:89-176 */
@@ -281,11 +298,11 @@ static double incircle_pair(P2 a, P2 b, P2 c, P2 d) {
 /* ---------------- geometry helpers ---------------- */
 /* checkseg4encroach, refine.cu:115-139 */
 static int encroached(P2 o, P2 d, P2 a, double goodcoss /* cos^2 */, int mode) {
-  double dot = (o.x - a.x) * (d.x - a.x) + (o.y - a.y) * (d.y - a.y);
+  double dot = madd(o.x - a.x, d.x - a.x, (o.y - a.y) * (d.y - a.y));
   if (dot < 0.0) {
     if (mode || dot * dot >= (2.0 * goodcoss - 1.0) * (2.0 * goodcoss - 1.0) *
-                                   ((o.x - a.x) * (o.x - a.x) + (o.y - a.y) * (o.y - a.y)) *
-                                   ((d.x - a.x) * (d.x - a.x) + (d.y - a.y) * (d.y - a.y)))
+                                   madd(o.x - a.x, o.x - a.x, (o.y - a.y) * (o.y - a.y)) *
+                                   madd(d.x - a.x, d.x - a.x, (d.y - a.y) * (d.y - a.y)))
       return 1;
   }
   return 0;
@@ -296,22 +313,21 @@ static double smallest_angle(P2 pApex, P2 pOrg, P2 pDest, int *shortestOri) {
   double dxod = pOrg.x - pDest.x, dyod = pOrg.y - pDest.y;
   double dxda = pDest.x - pApex.x, dyda = pDest.y - pApex.y;
   double dxao = pApex.x - pOrg.x, dyao = pApex.y - pOrg.y;
-  double dxod2 = dxod * dxod, dyod2 = dyod * dyod, dxda2 = dxda * dxda, dyda2 = dyda * dyda;
-  double dxao2 = dxao * dxao, dyao2 = dyao * dyao;
-  double lenOrg = dxod2 + dyod2, lenDest = dxda2 + dyda2, lenApex = dxao2 + dyao2;
+  double lenOrg = madd(dyod, dyod, dxod * dxod), lenDest = madd(dyda, dyda, dxda * dxda);
+  double lenApex = madd(dxao, dxao, dyao * dyao);
   double ang, sh;
   if (lenOrg < lenDest && lenOrg < lenApex) {
     sh = lenOrg;
     *shortestOri = 0;
-    ang = dxda * dxao + dyda * dyao;
+    ang = madd(dyda, dyao, dxda * dxao);
   } else if (lenDest < lenOrg && lenDest < lenApex) {
     sh = lenDest;
     *shortestOri = 1;
-    ang = dxod * dxao + dyod * dyao;
+    ang = madd(dyod, dyao, dxod * dxao);
   } else {
     sh = lenApex;
     *shortestOri = 2;
-    ang = dxod * dxda + dyod * dyda;
+    ang = madd(dyod, dyda, dxod * dxda);
   }
   return ang * ang * sh / (lenOrg * lenDest * lenApex);
 }
@@ -320,37 +336,37 @@ static double smallest_angle(P2 pApex, P2 pOrg, P2 pDest, int *shortestOri) {
 static P2 circumcenter(P2 vApex, P2 vOrg, P2 vDest, double offConstant, int offcenter) {
   double xdo = vDest.x - vOrg.x, ydo = vDest.y - vOrg.y;
   double xao = vApex.x - vOrg.x, yao = vApex.y - vOrg.y;
-  double dodist = xdo * xdo + ydo * ydo;
-  double aodist = xao * xao + yao * yao;
-  double dadist = (vDest.x - vApex.x) * (vDest.x - vApex.x) + (vDest.y - vApex.y) * (vDest.y - vApex.y);
+  double dodist = madd(xdo, xdo, ydo * ydo);
+  double aodist = madd(xao, xao, yao * yao);
+  double dadist = madd(vDest.x - vApex.x, vDest.x - vApex.x, (vDest.y - vApex.y) * (vDest.y - vApex.y));
   double denominator;
   double tmp = xdo * yao - xao * ydo;
   if (tmp != 0)
     denominator = 0.5 / tmp;
   else
     denominator = 0.5 / orient_ref(vDest, vApex, vOrg);
-  double dx = (yao * dodist - ydo * aodist) * denominator;
-  double dy = (xdo * aodist - xao * dodist) * denominator;
+  double dx = madd(yao, dodist, -(ydo * aodist)) * denominator;
+  double dy = madd(xdo, aodist, -(xao * dodist)) * denominator;
   if (offcenter && (offConstant > 0.0)) {
     double dxoff, dyoff;
     if ((dodist < aodist) && (dodist < dadist)) {
       dxoff = 0.5 * xdo - offConstant * ydo;
-      dyoff = 0.5 * ydo + offConstant * xdo;
-      if (dxoff * dxoff + dyoff * dyoff < dx * dx + dy * dy) {
+      dyoff = madd(offConstant, xdo, 0.5 * ydo);
+      if (madd(dxoff, dxoff, dyoff * dyoff) < madd(dx, dx, dy * dy)) {
         dx = dxoff;
         dy = dyoff;
       }
     } else if (aodist < dadist) {
       dxoff = 0.5 * xao + offConstant * yao;
       dyoff = 0.5 * yao - offConstant * xao;
-      if (dxoff * dxoff + dyoff * dyoff < dx * dx + dy * dy) {
+      if (madd(dxoff, dxoff, dyoff * dyoff) < madd(dx, dx, dy * dy)) {
         dx = dxoff;
         dy = dyoff;
       }
     } else {
       dxoff = 0.5 * (vApex.x - vDest.x) - offConstant * (vApex.y - vDest.y);
-      dyoff = 0.5 * (vApex.y - vDest.y) + offConstant * (vApex.x - vDest.x);
-      if (dxoff * dxoff + dyoff * dyoff < (dx - xdo) * (dx - xdo) + (dy - ydo) * (dy - ydo)) {
+      dyoff = madd(offConstant, vApex.x - vDest.x, 0.5 * (vApex.y - vDest.y));
+      if (madd(dxoff, dxoff, dyoff * dyoff) < madd(dx - xdo, dx - xdo, (dy - ydo) * (dy - ydo))) {
         dx = xdo + dxoff;
         dy = ydo + dyoff;
       }
@@ -1330,7 +1346,7 @@ static void insert_midpoint(St *S, int pos, int tindex, int *imarker, int nsub, 
   ts_setflipori(&S->ts[tri[1]], 0);
   for (int i = 0; i < 3; i++) p[i] = S->tri[tri[0] * 3 + (triOri[0] + i + 1) % 3];
   P2 a = S->pts[p[0]], b = S->pts[p[1]];
-  double segmentlength = sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
+  double segmentlength = sqrt(madd(a.x - b.x, a.x - b.x, (a.y - b.y) * (a.y - b.y)));
   double split = 0.5;
   if (acuteorg || acutedest) {
     double npt = 1.0;
@@ -1339,15 +1355,15 @@ static void insert_midpoint(St *S, int pos, int tindex, int *imarker, int nsub, 
     split = npt / segmentlength;
     if (acutedest) split = 1.0 - split;
   }
-  S->pts[newp].x = a.x + (b.x - a.x) * split;
-  S->pts[newp].y = a.y + (b.y - a.y) * split;
+  S->pts[newp].x = madd(b.x - a.x, split, a.x);
+  S->pts[newp].y = madd(b.y - a.y, split, a.y);
   double multiplier = orient_ref(a, b, S->pts[newp]);
-  double divisor = ((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
+  double divisor = madd(a.x - b.x, a.x - b.x, (a.y - b.y) * (a.y - b.y));
   if ((multiplier != 0.0) && (divisor != 0.0)) {
     multiplier = multiplier / divisor;
     if (multiplier == multiplier) {
-      S->pts[newp].x += multiplier * (b.y - a.y);
-      S->pts[newp].y += multiplier * (a.x - b.x);
+      S->pts[newp].x = madd(multiplier, b.y - a.y, S->pts[newp].x);
+      S->pts[newp].y = madd(multiplier, a.x - b.x, S->pts[newp].y);
     }
   }
   for (int i = 0; i < 3; i++) seg[i] = S->t2s[3 * tri[0] + (triOri[0] + i) % 3];
@@ -1644,8 +1660,8 @@ static void mark_bad_angle(St *S, int index) {
         common = pDest1;
       if (common != -1) {
         P2 vOrg = v[(shortest + 1) % 3], vDest = v[(shortest + 2) % 3], vCom = S->pts[common];
-        double d1 = (vCom.x - vOrg.x) * (vCom.x - vOrg.x) + (vCom.y - vOrg.y) * (vCom.y - vOrg.y);
-        double d2 = (vCom.x - vDest.x) * (vCom.x - vDest.x) + (vCom.y - vDest.y) * (vCom.y - vDest.y);
+        double d1 = madd(vCom.x - vOrg.x, vCom.x - vOrg.x, (vCom.y - vOrg.y) * (vCom.y - vOrg.y));
+        double d2 = madd(vCom.x - vDest.x, vCom.x - vDest.x, (vCom.y - vDest.y) * (vCom.y - vDest.y));
         if ((d1 < 1.001 * d2) && (d1 > 0.999 * d2)) {
           ts_set(ts, TS_BAD, 0);
           return;
@@ -1762,9 +1778,8 @@ static int locate_sink(St *S, int index, P2 cc) {
     int moveleft;
     if (detLeft < 0.0) {
       if (detRight < 0.0)
-        moveleft = (v[(curOri + 2) % 3].x - v[(curOri + 1) % 3].x) * (cc.x - v[curOri].x) +
-                       (v[(curOri + 2) % 3].y - v[(curOri + 1) % 3].y) * (cc.y - v[curOri].y) >
-                   0.0;
+        moveleft = madd(v[(curOri + 2) % 3].x - v[(curOri + 1) % 3].x, cc.x - v[curOri].x,
+                        (v[(curOri + 2) % 3].y - v[(curOri + 1) % 3].y) * (cc.y - v[curOri].y)) > 0.0;
       else
         moveleft = 1;
     } else {

@@ -1,4 +1,6 @@
-"""ctypes bindings of the test oracle (oracle/_build/libgqm_oracle.so).
+"""ctypes bindings of the test oracle (oracle/_build/libgqm_oracle.so, and
+libgqm_oracle_fma.so: the same restatement with the products fused that the
+reference as its project builds it fuses).
 
 Test infrastructure: imported only by tests/, __graft_entry__.smoke() and the
 CPU-baseline leg of bench.py.
@@ -12,6 +14,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libgqm_oracle.so")
+LIB_FMA = os.path.join(HERE, "_build", "libgqm_oracle_fma.so")
 
 
 class OracleOut(ctypes.Structure):
@@ -28,15 +31,15 @@ class OracleOut(ctypes.Structure):
                 ("midpoints_inserted", ctypes.c_longlong), ("bad_total", ctypes.c_longlong)]
 
 
-_lib = None
+_libs = {}
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB):
-            raise RuntimeError(f"{LIB} missing: run `make -C oracle oracle`")
-        L = ctypes.CDLL(LIB)
+def lib(contracted=False):
+    path = LIB_FMA if contracted else LIB
+    if path not in _libs:
+        if not os.path.exists(path):
+            raise RuntimeError(f"{path} missing: run `make -C oracle oracle`")
+        L = ctypes.CDLL(path)
         dp = ctypes.POINTER(ctypes.c_double)
         ip = ctypes.POINTER(ctypes.c_int)
         L.gqm_oracle_refine.argtypes = [ctypes.c_int, dp, ctypes.c_int, ip, ip, ctypes.c_int, ip, ctypes.c_double,
@@ -55,15 +58,16 @@ def lib():
             getattr(L, f).argtypes = [dp, dp, dp, dp]
             getattr(L, f).restype = ctypes.c_double
         L.gqm_oracle_circumcenter.argtypes = [dp, dp, dp, ctypes.c_double, ctypes.c_int, dp]
-        _lib = L
-    return _lib
+        _libs[path] = L
+    return _libs[path]
 
 
-def refine(cdt, theta=20.0, policy=1, mode=1, max_rounds=100000, goodcos2=None, max_area=0.0):
+def refine(cdt, theta=20.0, policy=1, mode=1, max_rounds=100000, goodcos2=None, max_area=0.0, contracted=False):
     """Run the oracle on a CDT; returns (CDT, info dict).  goodcos2: cos^2(theta)
-    as the device evaluates it (None: the host's cos())."""
+    as the device evaluates it (None: the host's cos()); contracted: the
+    arithmetic of the reference as its project builds it (fused products)."""
     from gpu_cdt_refine_b200.cdtio import CDT
-    L = lib()
+    L = lib(contracted)
     out = OracleOut()
     p = np.ascontiguousarray(cdt.pointlist, np.float64)
     t = np.ascontiguousarray(cdt.trianglelist, np.int32)

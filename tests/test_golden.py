@@ -120,3 +120,50 @@ def test_fixture_has_self_consistent_configs_of_every_mode():
     combos = {(c["policy"], c["mode"]) for case in load()["cases"].values() for c in case["configs"]
               if c["self_consistent"]}
     assert combos == {(0, 0), (0, 1), (1, 0), (1, 1)}
+
+
+# ---------------------------------------------------------------------------
+# The reference as its project builds it (nvcc's default FMA contraction)
+# ---------------------------------------------------------------------------
+SPREAD = os.path.join(HERE, "golden", "reference_spread.json")
+
+
+def _fma_entry(name, cfg):
+    with open(SPREAD) as f:
+        doc = json.load(f)
+    for e in doc["cases"][name]:
+        if (e["theta"], e["policy"], e["mode"]) == (cfg["theta"], cfg["policy"], cfg["mode"]):
+            return e
+    raise KeyError(name)
+
+
+def fma_consistent_configs():
+    """Configurations (CPU-sized, plus the 100,000-point hull-only one) on which
+    every recorded run of the stock build gave the same output."""
+    out = []
+    for p in configs():
+        name, cfg = p.values
+        if load()["cases"][name]["size"] != "small" and name != "h100k":
+            continue
+        e = _fma_entry(name, cfg)
+        if e["fma_self_consistent"] and e["fma_sha256"] == cfg["fma"]["sha256"]:
+            out.append(p)
+    return out
+
+
+@pytest.mark.parametrize("name,cfg", fma_consistent_configs())
+def test_contracted_oracle_matches_reference_as_built(name, cfg):
+    """The oracle with the stock build's fused products (libgqm_oracle_fma.so)
+    gives the stock build's output byte for byte."""
+    gc2 = load()["device_goodcos2"][repr(cfg["theta"])]
+    out, _ = oracle_py.refine(golden_input(name), cfg["theta"], cfg["policy"], cfg["mode"], goodcos2=gc2,
+                              contracted=True)
+    ref = cfg["fma"]
+    assert (out.numberofpoints, out.numberoftriangles, out.numberofsegments) == (
+        ref["points"], ref["triangles"], ref["segments"])
+    assert digests(out) == ref["sha256"]
+
+
+def test_contracted_configs_cover_every_mode():
+    combos = {(p.values[1]["policy"], p.values[1]["mode"]) for p in fma_consistent_configs()}
+    assert combos == {(0, 0), (0, 1), (1, 0), (1, 1)}

@@ -56,7 +56,7 @@ def oracle_runs(gpu):
     futs = {("c2",) + cfg: ex.submit(_oracle_job, "c2", *cfg, None) for cfg in C2_CFGS}
     futs[("c3",) + C3_CFG] = ex.submit(_oracle_job, "c3", *C3_CFG, st["goodcos2"])
     yield futs
-    ex.shutdown(wait=False, cancel_futures=True)
+    ex.shutdown(wait=True, cancel_futures=True)  # the workers hold the oracle meshes: release them now
 
 
 @pytest.fixture(scope="module")

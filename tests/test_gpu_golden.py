@@ -4,8 +4,9 @@
   wherever every run of the reference built with -fmad=false produced the same
   output (all golden configurations whose runs agree, including those too large
   for the CPU oracle), the refiner's output is that output, byte for byte.
-* libgqm_b200_fma.so (nvcc's default FMA contraction): wherever every run of
-  the reference as its project builds it (no -fmad option, so contraction on)
+* libgqm_b200_fma.so (GQM_CONTRACTED: fma() exactly at the products that the
+  reference as its project builds it fuses, gqm_madd in csrc/predicates.h):
+  wherever every run of that build (no -fmad option, so nvcc contracts)
   produced the same output, the contracted refiner's output is that output,
   byte for byte.
 * Wherever the reference's runs differ (two winners of one launch racing to
