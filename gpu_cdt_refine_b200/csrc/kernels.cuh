@@ -51,6 +51,23 @@ namespace gqm {
 
 #define GS_LOOP(i, n) for (int i = GQM_GTID; i < (n); i += GQM_GSIZE)
 
+// Counts and slot lists that some kernels take either as values (the
+// block-mode engine, whose driver holds them in registers) or as device words
+// that an earlier kernel of the same CUDA graph wrote (the single-domain
+// engine, whose driver state lives on the device).
+struct DevInt {
+  const int *p;
+};
+__device__ __forceinline__ int nval(int n) { return n; }
+__device__ __forceinline__ int nval(DevInt d) { return *d.p; }
+// free slots handed out from base[*off] on
+struct DevSlots {
+  const int *base;
+  const int *off;
+};
+__device__ __forceinline__ const int *slots_of(const int *p) { return p; }
+__device__ __forceinline__ const int *slots_of(DevSlots s) { return s.base + *s.off; }
+
 // ============================================================================
 // Initialisation (refine.cu:5557-5747, 3105-3151)
 // ============================================================================
@@ -207,7 +224,9 @@ GQM_KERNEL void k_pack_s2t(Mesh M, const int *s2t_int, int ns) {
 }
 
 // kernelMarkAllEncsegs, refine.cu:3105-3151
-GQM_KERNEL void k_mark_all_encsegs(Mesh M, int ns) {
+template <class N>
+GQM_KERNEL void k_mark_all_encsegs(Mesh M, N ns_) {
+  const int ns = nval(ns_);
   GS_LOOP(s, ns) {
     int e = -1;
     int otri = s2t_get(M, s);
@@ -258,7 +277,9 @@ __device__ __forceinline__ double smallest_cos2(double2 pA, double2 pO, double2 
 
 // kernelMarkBadTriangles, refine.cu:376-497, over every triangle slot below
 // ntri that is not null and has CHECK set.
-GQM_KERNEL void k_mark_bad(Mesh M, int ntri) {
+template <class N>
+GQM_KERNEL void k_mark_bad(Mesh M, N ntri_) {
+  const int ntri = nval(ntri_);
   GS_LOOP(t, ntri) {
     uint8_t st = M.tst[t];
     if (!(st & TS_NOTNULL) || !(st & TS_CHECK)) continue;
@@ -886,6 +907,8 @@ struct FlipCtl {
   int cond;         // loop condition of the last step
   long long cap;    // bound on the steps of one loop
   int *errp;        // device error word (GQM_ERR_ROUND_LIMIT on cap_hit)
+  // device time of the loops (%globaltimer at loop entry, summed at loop end)
+  unsigned long long loop_t0, loop_ns, loops;
   // step profile of the run: steps and active triangles by floor(log2 |A|)
   unsigned long long prof_steps[kFlipProfileBins], prof_items[kFlipProfileBins];
 };
@@ -935,6 +958,9 @@ __device__ __forceinline__ int flip_next(FlipCtl *c) {
     c->qn = 0;
     c->tn = 0;
     c->steps++;
+  } else {
+    c->loop_ns += global_ns() - c->loop_t0;
+    c->loops++;
   }
   c->cond = cond;
   return cond;
@@ -943,6 +969,7 @@ GQM_KERNEL void k_flip_prep(FlipCtl *c, cudaGraphConditionalHandle h, int use_gr
   if (GQM_BLOCK0 && threadIdx.x == 0) {
     c->entry_steps = c->steps;
     c->nact_next = 0;
+    c->loop_t0 = global_ns();
     int cond = flip_next(c);
 #ifndef GQM_HOST_EMU
     if (use_graph) cudaGraphSetConditional(h, cond);
@@ -988,7 +1015,9 @@ GQM_KERNEL void k_ctl_reset(FlipCtl *c, long long cap, int *errp) {
 
 
 // reset tmark / tfo before the first step of a flip-flop
-GQM_KERNEL void k_flip_entry_reset(Mesh M, int ntri) {
+template <class N>
+GQM_KERNEL void k_flip_entry_reset(Mesh M, N ntri_) {
+  const int ntri = nval(ntri_);
   GS_LOOP(t, ntri) {
     M.tmark[t] = kMaxInt;
     M.tfo[t] = 15;
@@ -1351,8 +1380,12 @@ GQM_KERNEL void k_mid_snapshot(Mesh M, const int *mids, const int *dn, const int
 }
 
 // kernelInsertMidPoints, refine.cu:2594-2927 (debug printing left out)
-GQM_KERNEL void GQM_WALK_BOUNDS k_insert_mid(Mesh M, const int *mids, const int *dn, int *imark, const int *snap, const int *pslots,
-                             const int *tslots, int nsub, const unsigned *ep, unsigned long long *counter) {
+template <class S, class N>
+GQM_KERNEL void GQM_WALK_BOUNDS k_insert_mid(Mesh M, const int *mids, const int *dn, int *imark, const int *snap,
+                                             S pslots_, S tslots_, N nsub_, const unsigned *ep,
+                                             unsigned long long *counter) {
+  const int *pslots = slots_of(pslots_), *tslots = slots_of(tslots_);
+  const int nsub = nval(nsub_);
   int n = *dn;
   uint32_t epoch = *ep;
   GS_LOOP(pos, n) {
@@ -1528,7 +1561,9 @@ GQM_KERNEL void k_update_mid_nbrs(Mesh M, const int *mids, const int *dn, const 
 }
 
 // kernelUpdatePStatus2Old, refine.cu:3072-3083
-GQM_KERNEL void k_points_old(Mesh M, int npts) {
+template <class N>
+GQM_KERNEL void k_points_old(Mesh M, N npts_) {
+  const int npts = nval(npts_);
   GS_LOOP(i, npts) {
     uint8_t s = M.ps[i];
     if (!(s & PS_DELETED)) M.ps[i] = (uint8_t)(s & ~PS_NEW);
@@ -1835,9 +1870,10 @@ GQM_KERNEL void k_reset_steiner(Mesh M, const int *wl, const int *dn, const int 
 }
 
 // kernelInsertSteinerPoints, refine.cu:4651-4900
+template <class S>
 GQM_KERNEL void k_insert_steiner(Mesh M, const int *wl, const int *dn, const int *sinks, const double2 *center,
-                                 const int *pslots, const int *tslots, const unsigned *ep,
-                                 unsigned long long *counter) {
+                                 S pslots_, S tslots_, const unsigned *ep, unsigned long long *counter) {
+  const int *pslots = slots_of(pslots_), *tslots = slots_of(tslots_);
   int n = *dn;
   uint32_t epoch = *ep;
   GS_LOOP(pos, n) {
@@ -1957,7 +1993,9 @@ GQM_KERNEL void k_update_steiner_nbrs(Mesh M, const int *wl, const int *dn, cons
 }
 
 // kernelUpdateSteinerOnsegs, refine.cu:5091-5105 (over all subsegments)
-GQM_KERNEL void k_onsegs_to_enc(Mesh M, const int *encl2, int ns) {
+template <class N>
+GQM_KERNEL void k_onsegs_to_enc(Mesh M, const int *encl2, N ns_) {
+  const int ns = nval(ns_);
   GS_LOOP(s, ns) if (encl2[s] >= 0) M.enc[s] = 1;
 }
 

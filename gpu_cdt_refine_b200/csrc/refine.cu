@@ -212,6 +212,297 @@ __global__ void k_set_count(int *dst, int v) {
 }
 
 // ============================================================================
+// The driver's state on the device.  The reference keeps its bookkeeping of
+// free slots (refine.cu:149-197, 3408-3444, 3545-3562, 5259-5296, 5354-5368)
+// and every count it branches on in host variables; here they live in one
+// DState block on the device, updated by one-thread kernels between the
+// steps, so that the whole refinement (the splitting of encroached
+// subsegments and the round loop, refine.cu:6830-7024) runs as one CUDA graph
+// whose loops and branches are conditional nodes decided on the device.
+// ============================================================================
+constexpr int kMaxNodes = 40;  // conditional nodes of the refinement graph
+struct DState {
+  int pcap, tcap;                  // the reference's logical capacities of points / triangles
+  int pphys, tphys, sphys, cav_cap;  // physical capacities of the buffers
+  int last_point, last_triangle, last_subseg;
+  int pointblock, triblock;
+  int nempty_p, nempty_t, lenp, lent;
+  int pslot, tslot;  // first free slot of the current batch: lenp - nempty_p, lent - nempty_t
+  int req_p, req_t, grew;  // the batch's request; whether a growth step happened
+  int nenc, nmark, ndel, nmid, nbad, nst;
+  // a physical capacity would be exceeded (1 points, 2 triangles, 4
+  // subsegments, 8 stored cavities): every loop ends and the host repeats the
+  // run with larger buffers (the result does not depend on them)
+  int need_grow;
+  int flag;  // value of the last condition (read by the host when no graph runs)
+  long long max_rounds, rounds, outer, inner, mid_iter, bad_total;
+  long long iters[kMaxNodes + 1];  // runs of each conditional node's body
+};
+
+// one-thread kernels of the driver: f(DState &, int *err) changes the state
+// (k_do) or returns a loop / branch condition (k_cond, which also sets the
+// graph's conditional handle when the graph runs)
+template <class F>
+__global__ void k_do(F f, DState *d, int *err) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) f(*d, err);
+}
+template <class F>
+__global__ void k_cond(F f, DState *d, int *err, cudaGraphConditionalHandle h, int graph, int node) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const int v = f(*d, err) ? 1 : 0;
+    d->flag = v;
+    if (v) d->iters[node]++;
+#ifndef GQM_HOST_EMU
+    if (graph) cudaGraphSetConditional(h, v);
+#endif
+    (void)h;
+    (void)graph;
+  }
+}
+__device__ __forceinline__ bool run_ok(const DState &d, const int *err) { return *err == 0 && d.need_grow == 0; }
+
+// splitEncsegs' outer loop (refine.cu:3180-3778): encroached subsegments remain
+struct CondEncroached {
+  __device__ bool operator()(DState &d, int *err) const {
+    if (!run_ok(d, err) || d.nenc == 0) return false;
+    if (++d.outer > d.max_rounds) {
+      atomicCAS(err, 0, GQM_ERR_ROUND_LIMIT);
+      return false;
+    }
+    d.nmark = d.nenc;
+    d.inner = 0;
+    d.mid_iter = 0;
+    return true;
+  }
+};
+// its deletion of free Steiner points inside diametral circles
+struct CondDelete {
+  __device__ bool operator()(DState &d, int *err) const {
+    if (!run_ok(d, err) || d.ndel == 0) return false;
+    if (++d.inner > d.max_rounds) {
+      atomicCAS(err, 0, GQM_ERR_ROUND_LIMIT);
+      return false;
+    }
+    d.nmark = d.ndel;
+    return true;
+  }
+};
+// its midpoint insertion passes
+struct CondMidpoints {
+  __device__ bool operator()(DState &d, int *err) const {
+    if (!run_ok(d, err) || d.nmid == 0) return false;
+    if (++d.mid_iter > 64 * d.max_rounds) {
+      atomicCAS(err, 0, GQM_ERR_ROUND_LIMIT);
+      return false;
+    }
+    return true;
+  }
+};
+// the round loop (refine.cu:6830-7024): bad triangles remain
+struct CondRound {
+  __device__ bool operator()(DState &d, int *err) const {
+    if (!run_ok(d, err) || d.nbad == 0) return false;
+    if (d.rounds >= d.max_rounds) {
+      atomicCAS(err, 0, GQM_ERR_ROUND_LIMIT);
+      return false;
+    }
+    d.bad_total += d.nbad;
+    return true;
+  }
+};
+// the growth steps of refine.cu:3408-3444 / 5259-5296
+struct CondNeedPoints {
+  __device__ bool operator()(DState &d, int *err) const { return run_ok(d, err) && d.req_p > d.nempty_p; }
+};
+struct CondNeedTris {
+  __device__ bool operator()(DState &d, int *err) const { return run_ok(d, err) && d.req_t > d.nempty_t; }
+};
+struct CondGrew {
+  __device__ bool operator()(DState &d, int *) const { return d.grew != 0; }
+};
+struct SlotsRequest {  // a batch of *n points and scale * *n triangles
+  const int *n;
+  int scale;
+  __device__ void operator()(DState &d, int *) const {
+    d.req_p = *n;
+    d.req_t = scale * *n;
+  }
+};
+struct RefreshedPoints {  // updateEmptyPoints done: the list holds lenp slots
+  __device__ void operator()(DState &d, int *) const { d.nempty_p = d.lenp; }
+};
+struct RefreshedTris {
+  __device__ void operator()(DState &d, int *) const { d.nempty_t = d.lent; }
+};
+struct GrowPoints {  // blocks of pointblock slots until the batch fits
+  __device__ void operator()(DState &d, int *err) const {
+    d.grew = 0;
+    if (d.pointblock <= 0) {
+      atomicCAS(err, 0, GQM_ERR_ARGUMENT);
+      return;
+    }
+    long long num = 0;
+    while (d.req_p > d.nempty_p + num * d.pointblock) num++;
+    if (!num) return;
+    const long long cap = d.pcap + num * d.pointblock;
+    if (cap > d.pphys) {
+      d.need_grow |= 1;
+      return;
+    }
+    d.pcap = (int)cap;
+    d.grew = 1;
+  }
+};
+struct GrowTris {
+  __device__ void operator()(DState &d, int *err) const {
+    d.grew = 0;
+    if (d.triblock <= 0) {
+      atomicCAS(err, 0, GQM_ERR_ARGUMENT);
+      return;
+    }
+    long long num = 0;
+    while (d.req_t > d.nempty_t + num * d.triblock) num++;
+    if (!num) return;
+    const long long cap = d.tcap + num * d.triblock;
+    if (cap > d.tphys) {
+      d.need_grow |= 2;
+      return;
+    }
+    d.tcap = (int)cap;
+    d.grew = 1;
+  }
+};
+struct SlotsReady {  // the batch's first free slots; no batch when the run must be repeated
+  int *n;
+  __device__ void operator()(DState &d, int *err) const {
+    d.pslot = d.lenp - d.nempty_p;
+    d.tslot = d.lent - d.nempty_t;
+    if (!run_ok(d, err)) *n = 0;
+  }
+};
+// slot bookkeeping after an insertion batch (refine.cu:3545-3559, 5354-5368)
+struct ConsumeSlots {
+  const int *n;
+  int scale;
+  __device__ void operator()(DState &d, int *) const {
+    const int npts = *n, ntris = scale * *n;
+    int slot_after = d.pcap - d.last_point;
+    int slot_before = d.nempty_p - slot_after;
+    if (slot_before < npts) d.last_point += npts - slot_before;
+    d.nempty_p -= npts;
+    slot_after = d.tcap - d.last_triangle;
+    slot_before = d.nempty_t - slot_after;
+    if (slot_before < ntris) d.last_triangle += ntris - slot_before;
+    d.nempty_t -= ntris;
+  }
+};
+struct SubsegRoom {  // the new subsegments of a midpoint batch fit
+  __device__ void operator()(DState &d, int *) const {
+    if (d.last_subseg + d.nenc > d.sphys) {
+      d.need_grow |= 4;
+      d.nenc = 0;
+    }
+  }
+};
+struct SubsegsAdded {
+  __device__ void operator()(DState &d, int *) const { d.last_subseg += d.nenc; }
+};
+struct CavityRoom {  // the candidates' cavities fit their store
+  __device__ void operator()(DState &d, int *) const {
+    if (d.nbad > d.cav_cap) {
+      d.need_grow |= 8;
+      d.nbad = 0;
+    }
+  }
+};
+struct OuterReset {
+  __device__ void operator()(DState &d, int *) const { d.outer = 0; }
+};
+struct RoundDone {
+  __device__ void operator()(DState &d, int *) const { d.rounds++; }
+};
+
+// fills whose count (and offset) an earlier kernel wrote
+__global__ void k_fill_n(int *a, DevInt n, int v) {
+  const int cnt = nval(n);
+  GS_LOOP(i, cnt) a[i] = v;
+}
+__global__ void k_fill_at(int *base, DevInt off, DevInt n, int v) {
+  int *a = base + nval(off);
+  const int cnt = nval(n);
+  GS_LOOP(i, cnt) a[i] = v;
+}
+
+// Ordered compaction over [0, *hi) whose bound an earlier kernel wrote: a
+// fixed grid of kDevCompactBlocks blocks, each covering a contiguous chunk
+// (whole tiles), then the same scan and emit as above.
+constexpr int kDevCompactBlocks = 296;
+__device__ __forceinline__ int dev_chunk(int n) {
+  int chunk = (n + kDevCompactBlocks - 1) / kDevCompactBlocks;
+  chunk = max(chunk, kCompactTile);
+  return (chunk + kCompactTile - 1) / kCompactTile * kCompactTile;
+}
+template <class F>
+__global__ void __launch_bounds__(kCompactThreads) k_cnt_dev(F f, DevInt hi_, int *bc) {
+  const int hi = nval(hi_), chunk = dev_chunk(hi);
+  const int b0 = min(hi, (int)blockIdx.x * chunk), b1 = min(hi, b0 + chunk);
+  int c = 0;
+  for (int s = b0 + threadIdx.x * kCompactItems; s < b1; s += kCompactTile) {
+#pragma unroll
+    for (int j = 0; j < kCompactItems; ++j)
+      if (s + j < b1 && f(s + j)) ++c;
+  }
+  __shared__ int red[32];
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    int v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) bc[blockIdx.x] = v;
+  }
+}
+template <class F, class Mp>
+__global__ void __launch_bounds__(kCompactThreads) k_emit_dev(F f, Mp m, DevInt hi_, const int *bc, int *out) {
+  const int hi = nval(hi_), chunk = dev_chunk(hi);
+  const int b0 = min(hi, (int)blockIdx.x * chunk), b1 = min(hi, b0 + chunk);
+  if (b0 >= b1) return;  // the whole block leaves: no barrier below is skipped by part of it
+  __shared__ int wsum[kCompactThreads / 32];
+  int base = bc[blockIdx.x];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int tile = b0; tile < b1; tile += kCompactTile) {
+    const int s = tile + threadIdx.x * kCompactItems;
+    unsigned bits = 0;
+#pragma unroll
+    for (int j = 0; j < kCompactItems; ++j)
+      if (s + j < b1 && f(s + j)) bits |= 1u << j;
+    const int c = __popc(bits);
+    int x = c;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    int woff = 0, tot = 0;
+#pragma unroll
+    for (int w = 0; w < kCompactThreads / 32; ++w) {
+      const int v = wsum[w];
+      woff += (w < warp) ? v : 0;
+      tot += v;
+    }
+    int pos = base + woff + x - c;
+    while (bits) {
+      const int j = __ffs(bits) - 1;
+      bits &= bits - 1;
+      out[pos++] = m(s + j);
+    }
+    base += tot;
+    __syncthreads();
+  }
+}
+
+// ============================================================================
 // Refiner
 // ============================================================================
 struct Refiner {
@@ -224,7 +515,7 @@ struct Refiner {
   // reference logical state
   long pcap = 0, tcap = 0;
   int last_point = 0, last_triangle = 0, last_subseg = 0, nseg_in = 0;
-  int pointblock = 0, triblock = 0, nempty_p = 0, nempty_t = 0, lenp = 0, lent = 0;
+  int pointblock = 0, triblock = 0;
   // per-triangle scratch (capacity tphys)
   int *emptyt = nullptr, *bad = nullptr, *imark = nullptr, *ilist = nullptr, *sinks = nullptr, *wl = nullptr;
   int *act = nullptr, *win = nullptr, *neg = nullptr, *ll = nullptr, *sl = nullptr, *newidx = nullptr;
@@ -237,17 +528,20 @@ struct Refiner {
   FlipCtl *fc = nullptr;             // flip-loop control block (device)
   KTimer *ktm = nullptr;             // launch timer of the flip-step check kernel
   KTimer *stm = nullptr;             // launch timer of the small-step kernel
-  bool probing = false;              // events around every flip-loop launch
-  std::vector<cudaEvent_t> loop_ev;  // pairs, reused every run
-  size_t loop_ev_used = 0;
-  double probe_loop_ms = 0.0;
-  long long probe_loops = 0;
-  // the flip-flop loop as a CUDA graph with a device-side while condition
-  bool use_graph = true;
-  cudaGraph_t flip_graph = nullptr;
-  cudaGraphExec_t flip_exec = nullptr;
-  Mesh flip_graph_mesh{};
-  int flip_graph_pred = -1;
+  // the driver's state on the device, and the refinement captured as one
+  // CUDA graph (loops and branches as conditional nodes)
+  DState *ds = nullptr;
+  DState hds{};             // host copy: written before a run, read after it
+  bool use_graph = true;    // false: the host reads each condition (GQM_NO_GRAPH=1, emulated build)
+  bool capturing = false;   // the refinement graph is being captured
+  cudaGraph_t ref_graph = nullptr;
+  cudaGraphExec_t ref_exec = nullptr;
+  long buf_gen = 0;         // bumped whenever a device buffer is allocated again
+  int node_count = 0, cur_node = 0, node_id = 0;
+  long long node_kernels[kMaxNodes + 1] = {};  // kernels in each conditional node's body; [kMaxNodes]: top level
+  // physical capacities that a repeated run asks for (a run that would exceed
+  // one stops and is repeated with larger buffers)
+  long want_p = 0, want_t = 0, want_s = 0, want_cav = 0;
   // per-point scratch (capacity pphys)
   int *emptyp = nullptr, *pnew = nullptr;
   // per-subsegment scratch (capacity sphys)
@@ -334,21 +628,13 @@ struct Refiner {
     return cudaSuccess;
   }
 
-  void drop_flip_graph() {
-#ifndef GQM_HOST_EMU
-    if (flip_exec) cudaGraphExecDestroy(flip_exec);
-    if (flip_graph) cudaGraphDestroy(flip_graph);
-#endif
-    flip_exec = nullptr;
-    flip_graph = nullptr;
-  }
-
   void release() {
-    drop_flip_graph();
+    drop_ref_graph();
     void *ptrs[] = {M.pts, M.ps, M.pred, M.tv, M.tn, M.tsg, M.tst, M.tflip, M.tfo, M.flip0, M.tmark, M.tpos,
                     M.s2t, M.s2seg, M.enc, M.err, stm, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
                     newidx, tail, center, emptyp, pnew, enclist, encl2, smark, mids, snap, segs, dcount, bc,
-                    dctr, dgc, dinput, mlp_w, mlp_b, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wsup, M.wmeg};
+                    dctr, dgc, dinput, mlp_w, mlp_b, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wsup, M.wmeg,
+                    ds};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     if (hcount) cudaFreeHost(hcount);
@@ -362,9 +648,7 @@ struct Refiner {
     stm = nullptr;
     mlp_w = nullptr;
     mlp_b = nullptr;
-    for (cudaEvent_t e : loop_ev) cudaEventDestroy(e);
-    loop_ev.clear();
-    loop_ev_used = 0;
+    ds = nullptr;
     center = nullptr;
     cav = cavn = nullptr;
     cav_cap = 0;
@@ -398,7 +682,7 @@ struct Refiner {
     if (!ev1) cudaEventCreate(&ev1);
     if (!dcount) {
       if (dalloc(&dcount, 16) || dalloc(&bc, kMaxCompactBlocks + 1) || dalloc(&dctr, 8) || dalloc(&dgc, 2) ||
-          dalloc(&M.err, 1) || dalloc(&fc, 1) || dalloc(&ktm, 1) || dalloc(&stm, 1))
+          dalloc(&M.err, 1) || dalloc(&fc, 1) || dalloc(&ktm, 1) || dalloc(&stm, 1) || dalloc(&ds, 1))
         return GQM_ERR_MEMORY;
       cudaMemsetAsync(fc, 0, sizeof(FlipCtl), st);
       cudaMemsetAsync(ktm, 0, sizeof(KTimer), st);  // off until gqm_context_probe
@@ -429,7 +713,7 @@ struct Refiner {
 #define LAUNCH(kernel, n, ...)                   \
   do {                                           \
     KL(kernel, grid_for(n), 256)(__VA_ARGS__);   \
-    stats.kernel_launches++;                     \
+    count_launch(1);                             \
   } while (0)
 
   // Ordered compaction over [lo, hi) into out; the count lands in dcount[slot].
@@ -495,6 +779,7 @@ struct Refiner {
       cudaMemsetAsync(M.pts + old, 0, sizeof(double2) * (n - old), st);
     }
     pphys = n;
+    buf_gen++;
     return GQM_OK;
   }
   int alloc_tris(long n) {
@@ -526,6 +811,7 @@ struct Refiner {
       cudaMemsetAsync(M.tstamp + old, 0, sizeof(int) * (n - old), st);
     }
     tphys = n;
+    buf_gen++;
     return GQM_OK;
   }
   int alloc_subsegs(long n) {
@@ -537,73 +823,181 @@ struct Refiner {
     // new subsegment entries start at epoch 0 so that the first tagged store wins
     cudaMemsetAsync(M.s2t + old, 0, sizeof(s2t_t) * (n - old), st);
     sphys = n;
+    buf_gen++;
     return GQM_OK;
   }
 
-  // updateEmptyPoints / updateEmptyTriangles (refine.cu:149-197)
-  int refresh_points() {
-    compact(PPtDeleted{M.ps}, Ident{}, 0, (int)pcap, emptyp, C_MISC);
-    lenp = fetch(C_MISC);
-    return lenp;
+  // ==========================================================================
+  // Control flow of the driver.  Every count and every piece of the
+  // reference's slot bookkeeping lives in DState on the device.  While the
+  // refinement graph is captured (capturing), a loop or a branch becomes a
+  // conditional node of the graph whose condition a one-thread kernel sets on
+  // the device; otherwise (the emulated build, GQM_NO_GRAPH=1) the same kernel
+  // writes the condition to ds->flag and the host reads it.  Either way the
+  // device runs the same kernels in the same order.
+  // ==========================================================================
+  static constexpr int kDevGrid = 148 * 8;  // grid of the kernels whose count is read on the device
+#define DLAUNCH(kernel, ...)                  \
+  do {                                        \
+    KL(kernel, kDevGrid, 256)(__VA_ARGS__);   \
+    count_launch(1);                          \
+  } while (0)
+#define DSTEP(f)                               \
+  do {                                         \
+    KL(k_do, 1, 32)(f, ds, M.err);             \
+    count_launch(1);                           \
+  } while (0)
+  void count_launch(int n) {
+    if (capturing)
+      node_kernels[cur_node]++;
+    else
+      stats.kernel_launches += n;
   }
-  int refresh_tris() {
-    compact(PTriNull{M.tst}, Ident{}, 0, (int)tcap, emptyt, C_MISC);
-    lent = fetch(C_MISC);
-    return lent;
-  }
-  // growth steps of refine.cu:3408-3444 / 5259-5296
-  int ensure_slots(int npts, int ntris) {
-    if (npts > nempty_p) {
-      nempty_p = refresh_points();
-      long num = 0;
-      while (npts > nempty_p + num * pointblock) num++;
-      if (num) {
-        long ncap = pcap + num * pointblock;
-        if (ncap > pphys) {
-#ifdef GQM_TEST_TIGHT_BUFFERS
-          int rc = alloc_points(ncap);
-#else
-          int rc = alloc_points(std::max(ncap, pphys + pphys / 2));
-#endif
-          if (rc) return rc;
-        }
-        pcap = ncap;
-        nempty_p = refresh_points();
-      }
-    }
-    if (ntris > nempty_t) {
-      nempty_t = refresh_tris();
-      long num = 0;
-      while (ntris > nempty_t + num * triblock) num++;
-      if (num) {
-        long ncap = tcap + num * triblock;
-        if (ncap > tphys) {
-#ifdef GQM_TEST_TIGHT_BUFFERS
-          int rc = alloc_tris(ncap);
-#else
-          int rc = alloc_tris(std::max(ncap, tphys + tphys / 2));
-#endif
-          if (rc) return rc;
-        }
-        tcap = ncap;
-        nempty_t = refresh_tris();
-      }
-    }
+  int read_word(const int *dword, int *v) {
+    cudaMemcpyAsync(hcount + C_MISC, dword, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_ERR_CUDA;
+    stats.host_syncs++;
+    *v = hcount[C_MISC];
     return GQM_OK;
   }
-  // slot bookkeeping after an insertion batch (refine.cu:3545-3559, 5354-5368)
-  void consume_slots(int npts, int ntris) {
-    int slot_after = (int)(pcap - last_point);
-    int slot_before = nempty_p - slot_after;
-    if (slot_before < npts) last_point += npts - slot_before;
-    nempty_p -= npts;
-    slot_after = (int)(tcap - last_triangle);
-    slot_before = nempty_t - slot_after;
-    if (slot_before < ntris) last_triangle += ntris - slot_before;
-    nempty_t -= ntris;
+  // A loop (WHILE) or branch (IF).  pre(h, graph) launches the kernel that sets
+  // the first condition, body(h, graph) the body's kernels; flag is the word
+  // the condition kernels write.  For a loop, the body ends by setting the
+  // next condition: itself (body_sets_cond) or with pre's kernel again.
+  template <class Pre, class Body>
+  int cond_node(bool loop, Pre pre, Body body, const int *flag, bool body_sets_cond) {
+    cudaGraphConditionalHandle h{};
+    if (!capturing) {
+      pre(h, 0);
+      for (;;) {
+        int v = 0;
+        int rc = read_word(flag, &v);
+        if (rc || !v) return rc;
+        rc = body(h, 0);
+        if (rc || !loop) return rc;
+        if (!body_sets_cond) pre(h, 0);
+      }
+    }
+#ifdef GQM_HOST_EMU
+    return GQM_ERR_CUDA;
+#else
+    if (node_count >= kMaxNodes) return GQM_ERR_CUDA;
+    const int id = node_count++;
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd) != cudaSuccess ||
+        cs != cudaStreamCaptureStatusActive)
+      return GQM_ERR_CUDA;
+    if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return GQM_ERR_CUDA;
+    node_id = id;
+    pre(h, 1);
+    if (cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd) != cudaSuccess) return GQM_ERR_CUDA;
+    std::vector<cudaGraphNode_t> dv(deps, deps + nd);
+    cudaGraph_t ended = nullptr;
+    if (cudaStreamEndCapture(st, &ended) != cudaSuccess) return GQM_ERR_CUDA;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = loop ? cudaGraphCondTypeWhile : cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (cudaGraphAddNode(&node, g, dv.data(), dv.size(), &cp) != cudaSuccess) return GQM_ERR_CUDA;
+    if (cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return GQM_ERR_CUDA;
+    const int outer = cur_node;
+    cur_node = id;
+    int rc = body(h, 1);
+    if (rc == 0 && loop && !body_sets_cond) {
+      node_id = id;
+      pre(h, 1);
+    }
+    cur_node = outer;
+    cudaGraph_t bg = nullptr;
+    if (cudaStreamEndCapture(st, &bg) != cudaSuccess && rc == 0) rc = GQM_ERR_CUDA;
+    if (rc) return rc;
+    if (cudaStreamBeginCaptureToGraph(st, g, &node, nullptr, 1, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      return GQM_ERR_CUDA;
+    return GQM_OK;
+#endif
   }
-  const int *pslots() const { return emptyp + (lenp - nempty_p); }
-  const int *tslots() const { return emptyt + (lent - nempty_t); }
+  // a loop or branch on a DState condition functor
+  template <class C, class Body>
+  int dev_while(C c, Body body) {
+    return cond_node(
+        true,
+        [&](cudaGraphConditionalHandle h, int graph) {
+          KL(k_cond, 1, 32)(c, ds, M.err, h, graph, graph ? node_id : kMaxNodes);
+          count_launch(1);
+        },
+        [&](cudaGraphConditionalHandle, int) { return body(); }, &ds->flag, false);
+  }
+  template <class C, class Body>
+  int dev_if(C c, Body body) {
+    return cond_node(
+        false,
+        [&](cudaGraphConditionalHandle h, int graph) {
+          KL(k_cond, 1, 32)(c, ds, M.err, h, graph, graph ? node_id : kMaxNodes);
+          count_launch(1);
+        },
+        [&](cudaGraphConditionalHandle, int) { return body(); }, &ds->flag, false);
+  }
+  // ordered compaction over [0, *hi) into out, count into *cnt
+  template <class F, class Mp>
+  void compact_dev(F f, Mp m, const int *hi, int *out, int *cnt) {
+#ifdef GQM_HOST_EMU
+    int c = 0;
+    for (int i = 0; i < *hi; ++i)
+      if (f(i)) out[c++] = m(i);
+    *cnt = c;
+    count_launch(3);
+#else
+    KL(k_cnt_dev, kDevCompactBlocks, kCompactThreads)(f, DevInt{hi}, bc);
+    KL(k_scan, 1, 1024)(bc, kDevCompactBlocks, cnt);
+    KL(k_emit_dev, kDevCompactBlocks, kCompactThreads)(f, m, DevInt{hi}, bc, out);
+    count_launch(3);
+#endif
+  }
+
+  // ---- free-slot bookkeeping (refine.cu:149-197, 3408-3444, 5259-5296) ----
+  // updateEmptyPoints / updateEmptyTriangles
+  void refresh_points() {
+    compact_dev(PPtDeleted{M.ps}, Ident{}, &ds->pcap, emptyp, &ds->lenp);
+    DSTEP(RefreshedPoints{});
+  }
+  void refresh_tris() {
+    compact_dev(PTriNull{M.tst}, Ident{}, &ds->tcap, emptyt, &ds->lent);
+    DSTEP(RefreshedTris{});
+  }
+  // room for *n points and scale * *n triangles; *n becomes 0 when the run
+  // has to be repeated with larger buffers
+  int ensure_slots(int *n, int scale) {
+    DSTEP((SlotsRequest{n, scale}));
+    int rc = dev_if(CondNeedPoints{}, [&] {
+      refresh_points();
+      DSTEP(GrowPoints{});
+      return dev_if(CondGrew{}, [&] {
+        refresh_points();
+        return GQM_OK;
+      });
+    });
+    if (rc) return rc;
+    rc = dev_if(CondNeedTris{}, [&] {
+      refresh_tris();
+      DSTEP(GrowTris{});
+      return dev_if(CondGrew{}, [&] {
+        refresh_tris();
+        return GQM_OK;
+      });
+    });
+    if (rc) return rc;
+    DSTEP(SlotsReady{n});
+    return GQM_OK;
+  }
+  DevSlots pslots() const { return DevSlots{emptyp, &ds->pslot}; }
+  DevSlots tslots() const { return DevSlots{emptyt, &ds->tslot}; }
 
   // ---- flip-flop (refine.cu:2328-2490), driven by active sets ----
   // One step: check (A) -> winners (W) -> link+phase 1 -> phase 2 -> phase 3
@@ -627,7 +1021,7 @@ struct Refiner {
       return step_grid == o.step_grid && small_limit == o.small_limit && small_cluster == o.small_cluster &&
              check_minb == o.check_minb;
     }
-  } tune, flip_graph_tune;
+  } tune;
   template <int PRED>
   void launch_check(const TouchL &T) {
     void (*check)(Mesh, const int *, const int *, uint8_t *, TouchL, KTimer *) =
@@ -661,227 +1055,227 @@ struct Refiner {
   }
   // kernels one grid step of the loop body launches (with its condition kernel)
   int step_kernels() const { return tune.small_limit > 0 ? 9 : 8; }
-  int build_flip_graph() {
-#ifdef GQM_HOST_EMU
-    return GQM_ERR_CUDA;
-#else
-    drop_flip_graph();
-    cudaGraph_t g = nullptr;
-    if (cudaGraphCreate(&g, 0) != cudaSuccess) return GQM_ERR_CUDA;
-    cudaGraphConditionalHandle h;
-    if (cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) {
-      cudaGraphDestroy(g);
-      return GQM_ERR_CUDA;
-    }
-    // node 1: k_flip_prep sets the condition for the first step
-    if (cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
-      cudaGraphDestroy(g);
-      return GQM_ERR_CUDA;
-    }
-    k_flip_prep<<<1, 32, 0, st>>>(fc, h, 1);
-    cudaGraph_t gc = nullptr;
-    if (cudaStreamEndCapture(st, &gc) != cudaSuccess) {
-      cudaGraphDestroy(g);
-      return GQM_ERR_CUDA;
-    }
-    cudaGraphNode_t prep = nullptr;
-    size_t nn = 1;
-    if (cudaGraphGetNodes(g, &prep, &nn) != cudaSuccess || nn != 1) {
-      cudaGraphDestroy(g);
-      return GQM_ERR_CUDA;
-    }
-    // node 2: while (condition) { step }
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    cudaGraphNode_t cn = nullptr;
-    if (cudaGraphAddNode(&cn, g, &prep, 1, &cp) != cudaSuccess) {
-      cudaGraphDestroy(g);
-      return GQM_ERR_CUDA;
-    }
-    cudaGraph_t body = cp.conditional.phGraph_out[0];
-    if (cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) !=
-        cudaSuccess) {
-      cudaGraphDestroy(g);
-      return GQM_ERR_CUDA;
-    }
-    flip_body(h, 1);
-    cudaGraph_t bc2 = nullptr;
-    if (cudaStreamEndCapture(st, &bc2) != cudaSuccess) {
-      cudaGraphDestroy(g);
-      return GQM_ERR_CUDA;
-    }
-    if (cudaGraphInstantiate(&flip_exec, g, 0) != cudaSuccess) {
-      cudaGraphDestroy(g);
-      flip_exec = nullptr;
-      return GQM_ERR_CUDA;
-    }
-    flip_graph = g;
-    flip_graph_mesh = M;
-    flip_graph_pred = pred_mode;
-    flip_graph_tune = tune;
-    return GQM_OK;
-#endif
-  }
-  // next pair of probe events (nullptr when none can be created)
-  cudaEvent_t *loop_events() {
-    while (loop_ev.size() < 2 * (loop_ev_used + 1)) {
-      cudaEvent_t e;
-      if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
-      loop_ev.push_back(e);
-    }
-    return &loop_ev[2 * loop_ev_used++];
-  }
-  // after the run's final sync: add the probe events' intervals to the totals
-  void collect_loop_events() {
-    for (size_t i = 0; i < loop_ev_used; ++i) {
-      float ms = 0.0f;
-      if (cudaEventElapsedTime(&ms, loop_ev[2 * i], loop_ev[2 * i + 1]) == cudaSuccess) probe_loop_ms += ms;
-      probe_loops++;
-    }
-    loop_ev_used = 0;
-  }
-  int flip_flop(int ntri) {
+
+  // ---- flip-flop (refine.cu:2328-2490) over the triangles flagged below last_triangle ----
+  int flip_flop() {
     NvtxRange nvtx("gqm:flip_flop");
-    LAUNCH(k_flip_entry_reset, ntri, M, ntri);
-    compact_to(PNotNullFlag{M.tst, M.tflip}, Ident{}, 0, ntri, act, &fc->nact);
-    if (use_graph) {
-      if (!flip_exec || memcmp(&flip_graph_mesh, &M, sizeof(Mesh)) != 0 || flip_graph_pred != pred_mode ||
-          !(flip_graph_tune == tune)) {
-        if (build_flip_graph() != GQM_OK) {
-          use_graph = false;
-          cudaGetLastError();
-        }
-      }
-    }
-    if (use_graph) {
-      cudaEvent_t *ev = probing ? loop_events() : nullptr;
-      if (ev) cudaEventRecord(ev[0], st);
-      if (cudaGraphLaunch(flip_exec, st) != cudaSuccess) return GQM_ERR_CUDA;
-      if (ev) cudaEventRecord(ev[1], st);
-      stats.kernel_launches++;
-      return GQM_OK;
-    }
-    cudaGraphConditionalHandle h{};
-    KL(k_flip_prep, 1, 32)(fc, h, 0);
-    stats.kernel_launches++;
-    for (;;) {
-      cudaMemcpyAsync(hcount + C_MISC, &fc->cond, sizeof(int), cudaMemcpyDeviceToHost, st);
-      cudaStreamSynchronize(st);
-      stats.host_syncs++;
-      if (!hcount[C_MISC]) break;
-      flip_body(h, 0);
-      stats.kernel_launches += step_kernels();
-    }
-    return GQM_OK;
+    DLAUNCH(k_flip_entry_reset, M, DevInt{&ds->last_triangle});
+    compact_dev(PNotNullFlag{M.tst, M.tflip}, Ident{}, &ds->last_triangle, act, &fc->nact);
+    return cond_node(
+        true,
+        [&](cudaGraphConditionalHandle h, int graph) {
+          KL(k_flip_prep, 1, 32)(fc, h, graph);
+          count_launch(1);
+        },
+        [&](cudaGraphConditionalHandle h, int graph) {
+          flip_body(h, graph);
+          // in a graph the steps are counted after the run (FlipCtl::steps)
+          if (!capturing) stats.kernel_launches += step_kernels();
+          return GQM_OK;
+        },
+        &fc->cond, true);
   }
 
   // ---- splitEncsegs (refine.cu:3180-3778) ----
   int split_encsegs() {
     NvtxRange nvtx("gqm:split_encsegs");
-    long long outer = 0;
-    for (;;) {
-      compact(PNonNeg{M.enc}, Ident{}, 0, last_subseg, enclist, C_LIST0);
-      int nenc = fetch(C_LIST0);
-      if (nenc == 0) break;
-      if (++outer > max_rounds) return GQM_ERR_ROUND_LIMIT;
+    DSTEP(OuterReset{});
+    compact_dev(PNonNeg{M.enc}, Ident{}, &ds->last_subseg, enclist, &ds->nenc);
+    return dev_while(CondEncroached{}, [&] {
       // delete free Steiner points inside diametral circles
-      LAUNCH(k_copy, nenc, smark, enclist, dcount + C_LIST0);
-      int nmark = nenc;
-      long long inner = 0;
-      for (;;) {
-        compact(PNonNeg{smark}, ValueOf{smark}, 0, nmark, mids, C_LIST1);
-        int ndel = fetch(C_LIST1);
-        if (ndel == 0) break;
-        if (++inner > max_rounds) return GQM_ERR_ROUND_LIMIT;
-        nmark = ndel;
-        LAUNCH(k_mark_redundant, ndel, M, smark, mids, dcount + C_LIST1);
-        int rc = flip_flop(last_triangle);
-        if (rc) return rc;
-      }
-      int rc = ensure_slots(nenc, 2 * nenc);
+      DLAUNCH(k_copy, smark, enclist, &ds->nenc);
+      compact_dev(PNonNeg{smark}, ValueOf{smark}, &ds->nmark, mids, &ds->ndel);
+      int rc = dev_while(CondDelete{}, [&] {
+        DLAUNCH(k_mark_redundant, M, smark, mids, &ds->ndel);
+        int r = flip_flop();
+        if (r) return r;
+        compact_dev(PNonNeg{smark}, ValueOf{smark}, &ds->nmark, mids, &ds->ndel);
+        return GQM_OK;
+      });
       if (rc) return rc;
-      if (last_subseg + nenc > sphys) {
-        rc = alloc_subsegs(std::max<long>(last_subseg + nenc, sphys + sphys / 2));
-        if (rc) return rc;
-      }
-      LAUNCH(k_fill, nenc, M.enc + last_subseg, nenc, -1);
-      LAUNCH(k_copy, nenc, smark, enclist, dcount + C_LIST0);
-      long long mid_iter = 0;
-      for (;;) {
-        compact(PNonNeg{smark}, Ident{}, 0, nenc, mids, C_LIST1);
-        int nmid = fetch(C_LIST1);
-        if (nmid == 0) break;
-        if (++mid_iter > 64 * max_rounds) return GQM_ERR_ROUND_LIMIT;
-        LAUNCH(k_reset_mid, nmid, M, mids, dcount + C_LIST1, smark);
-        LAUNCH(k_mark_mid, nmid, M, mids, dcount + C_LIST1, smark);
-        LAUNCH(k_mid_snapshot, nmid, M, mids, dcount + C_LIST1, smark, snap);
+      // insert the midpoints of the encroached subsegments
+      rc = ensure_slots(&ds->nenc, 2);
+      if (rc) return rc;
+      DSTEP(SubsegRoom{});
+      DLAUNCH(k_fill_at, M.enc, DevInt{&ds->last_subseg}, DevInt{&ds->nenc}, -1);
+      DLAUNCH(k_copy, smark, enclist, &ds->nenc);
+      compact_dev(PNonNeg{smark}, Ident{}, &ds->nenc, mids, &ds->nmid);
+      rc = dev_while(CondMidpoints{}, [&] {
+        DLAUNCH(k_reset_mid, M, mids, &ds->nmid, smark);
+        DLAUNCH(k_mark_mid, M, mids, &ds->nmid, smark);
+        DLAUNCH(k_mid_snapshot, M, mids, &ds->nmid, smark, snap);
         KL(k_bump_epoch, 1, 32)(fc);
-        LAUNCH(k_insert_mid, nmid, M, mids, dcount + C_LIST1, smark, snap, pslots(), tslots(), last_subseg,
-               &fc->epoch, dctr + 1);
-        LAUNCH(k_update_mid_nbrs, nmid, M, mids, dcount + C_LIST1, smark, enclist);
-      }
-      consume_slots(nenc, 2 * nenc);
-      last_subseg += nenc;
-      rc = flip_flop(last_triangle);
+        count_launch(1);
+        DLAUNCH(k_insert_mid, M, mids, &ds->nmid, smark, snap, pslots(), tslots(), DevInt{&ds->last_subseg},
+                &fc->epoch, dctr + 1);
+        DLAUNCH(k_update_mid_nbrs, M, mids, &ds->nmid, smark, enclist);
+        compact_dev(PNonNeg{smark}, Ident{}, &ds->nenc, mids, &ds->nmid);
+        return GQM_OK;
+      });
       if (rc) return rc;
+      DSTEP((ConsumeSlots{&ds->nenc, 2}));
+      DSTEP(SubsegsAdded{});
+      rc = flip_flop();
+      if (rc) return rc;
+      compact_dev(PNonNeg{M.enc}, Ident{}, &ds->last_subseg, enclist, &ds->nenc);
+      return GQM_OK;
+    });
+  }
+
+  // ---- splitTriangles (refine.cu:5107-5547) on the ds->nbad triangles in `bad` ----
+  int split_triangles() {
+    NvtxRange nvtx("gqm:split_triangles");
+    const int *dn = &ds->nbad;
+    DSTEP(CavityRoom{});
+    DLAUNCH(k_copy, imark, bad, dn);
+    DLAUNCH(k_copy, ilist, bad, dn);
+    DLAUNCH(k_circumcenter, M, bad, dn, (double)offconstant, offcenter, center);
+    if (col_feat) DLAUNCH(k_collect, M, bad, dn, center, col_feat, col_tgt, col_cnt, col_cap);
+    if (placement == GQM_PLACE_LEARNED) {  // two warps of a block take 64 candidates per pass
+      KL(k_learned_place, kDevGrid, 64)(M, bad, dn, mlp_dev(mlp_w, mlp_b), center, dctr + 4);
+      count_launch(1);
     }
+    DLAUNCH(k_fill_n, M.tmark, DevInt{&ds->last_triangle}, kMaxInt);
+    if (pred_mode)
+      DLAUNCH(k_locate<1>, M, bad, dn, center, sinks);
+    else
+      DLAUNCH(k_locate<0>, M, bad, dn, center, sinks);
+    DLAUNCH(k_remove_losers, M, bad, dn, sinks, imark);
+    DLAUNCH(k_fill_n, M.tmark, DevInt{&ds->last_triangle}, kMaxInt);
+    // stored cavities: kCavityCap rows of cav_cap entries
+    if (pred_mode)
+      DLAUNCH(k_cavity_mark<1>, M, dn, sinks, center, imark, ilist, cav, cavn, (int)cav_cap);
+    else
+      DLAUNCH(k_cavity_mark<0>, M, dn, sinks, center, imark, ilist, cav, cavn, (int)cav_cap);
+    DLAUNCH(k_cavity_check, M, dn, cav, cavn, (int)cav_cap, imark, ilist);
+    compact_dev(PNonNeg{imark}, Ident{}, dn, wl, &ds->nst);
+    DLAUNCH(k_fill_n, encl2, DevInt{&ds->last_subseg}, -1);
+    DLAUNCH(k_mark_onsegs, M, wl, &ds->nst, sinks, encl2);
+    int rc = ensure_slots(&ds->nst, 2);
+    if (rc) return rc;
+    DLAUNCH(k_reset_steiner, M, wl, &ds->nst, sinks);
+    KL(k_bump_epoch, 1, 32)(fc);
+    count_launch(1);
+    DLAUNCH(k_insert_steiner, M, wl, &ds->nst, sinks, center, pslots(), tslots(), &fc->epoch, dctr + 0);
+    DLAUNCH(k_update_steiner_nbrs, M, wl, &ds->nst, sinks);
+    DSTEP((ConsumeSlots{&ds->nst, 2}));
+    rc = flip_flop();
+    if (rc) return rc;
+    DLAUNCH(k_onsegs_to_enc, M, encl2, DevInt{&ds->last_subseg});
     return GQM_OK;
   }
 
-  // ---- splitTriangles (refine.cu:5107-5547) ----
-  int split_triangles(int nbad) {
-    NvtxRange nvtx("gqm:split_triangles");
-    int *dn = dcount + C_LIST2;  // number of bad triangles
-    LAUNCH(k_copy, nbad, imark, bad, dn);
-    LAUNCH(k_copy, nbad, ilist, bad, dn);
-    LAUNCH(k_circumcenter, nbad, M, bad, dn, (double)offconstant, offcenter, center);
-    if (col_feat) LAUNCH(k_collect, nbad, M, bad, dn, center, col_feat, col_tgt, col_cnt, col_cap);
-    if (placement == GQM_PLACE_LEARNED) {  // two warps of a block take 64 candidates per pass
-      KL(k_learned_place, std::max(1, std::min((nbad + 63) / 64, 148 * 8)), 64)(M, bad, dn, mlp_dev(mlp_w, mlp_b),
-                                                                                center, dctr + 4);
-      stats.kernel_launches++;
-    }
-    LAUNCH(k_fill, last_triangle, M.tmark, last_triangle, kMaxInt);
-    if (pred_mode)
-      LAUNCH(k_locate<1>, nbad, M, bad, dn, center, sinks);
-    else
-      LAUNCH(k_locate<0>, nbad, M, bad, dn, center, sinks);
-    LAUNCH(k_remove_losers, nbad, M, bad, dn, sinks, imark);
-    LAUNCH(k_fill, last_triangle, M.tmark, last_triangle, kMaxInt);
-    if (nbad > cav_cap) {  // stored cavities: kCavityCap rows of nbad entries
-      long cap = std::max<long>(nbad, 2 * cav_cap);
-      cudaStreamSynchronize(st);
-      if (cav) cudaFree(cav);
-      if (cavn) cudaFree(cavn);
-      cav = cavn = nullptr;
-      cav_cap = 0;
-      if (dalloc(&cav, (size_t)kCavityCap * cap) || dalloc(&cavn, cap)) return GQM_ERR_MEMORY;
-      cav_cap = cap;
-    }
-    if (pred_mode)
-      LAUNCH(k_cavity_mark<1>, nbad, M, dn, sinks, center, imark, ilist, cav, cavn, nbad);
-    else
-      LAUNCH(k_cavity_mark<0>, nbad, M, dn, sinks, center, imark, ilist, cav, cavn, nbad);
-    LAUNCH(k_cavity_check, nbad, M, dn, cav, cavn, nbad, imark, ilist);
-    compact(PNonNeg{imark}, Ident{}, 0, nbad, wl, C_LIST1);
-    int nst = fetch(C_LIST1);
-    int *dw = dcount + C_LIST1;
-    LAUNCH(k_fill, last_subseg, encl2, last_subseg, -1);
-    LAUNCH(k_mark_onsegs, nst, M, wl, dw, sinks, encl2);
-    int rc = ensure_slots(nst, 2 * nst);
+  // ---- the refinement proper (refine.cu:6830-7024), from the initialised mesh ----
+  int refine_body() {
+    refresh_points();
+    refresh_tris();
+    DLAUNCH(k_mark_all_encsegs, M, DevInt{&ds->last_subseg});  // last_subseg = the input's subsegments here
+    int rc = split_encsegs();
     if (rc) return rc;
-    LAUNCH(k_reset_steiner, nst, M, wl, dw, sinks);
-    KL(k_bump_epoch, 1, 32)(fc);
-    LAUNCH(k_insert_steiner, nst, M, wl, dw, sinks, center, pslots(), tslots(), &fc->epoch, dctr + 0);
-    LAUNCH(k_update_steiner_nbrs, nst, M, wl, dw, sinks);
-    consume_slots(nst, 2 * nst);
-    rc = flip_flop(last_triangle);
-    if (rc) return rc;
-    LAUNCH(k_onsegs_to_enc, last_subseg, M, encl2, last_subseg);
+    DLAUNCH(k_mark_bad, M, DevInt{&ds->last_triangle});
+    compact_dev(PBad{M.tst}, Ident{}, &ds->last_triangle, bad, &ds->nbad);
+    return dev_while(CondRound{}, [&] {
+      int r = split_triangles();
+      if (r) return r;
+      r = split_encsegs();
+      if (r) return r;
+      DLAUNCH(k_points_old, M, DevInt{&ds->last_point});
+      DSTEP(RoundDone{});
+      DLAUNCH(k_mark_bad, M, DevInt{&ds->last_triangle});
+      compact_dev(PBad{M.tst}, Ident{}, &ds->last_triangle, bad, &ds->nbad);
+      return GQM_OK;
+    });
+  }
+
+  // Everything the captured refinement graph depends on besides DState: a
+  // change in any of it captures the graph again.
+  struct RefKey {
+    Mesh M;
+    long buf_gen;
+    int pred_mode, placement, offcenter, offconstant;
+    const void *col_feat, *mlp_w;
+    unsigned long long col_cap;
+    Tuning tune;
+  };
+  RefKey ref_key{};  // what the captured graph was built for
+  RefKey ref_key_now() const {
+    RefKey k;
+    memset(&k, 0, sizeof(k));
+    k.M = M;
+    k.buf_gen = buf_gen;
+    k.pred_mode = pred_mode;
+    k.placement = placement;
+    k.offcenter = offcenter;
+    k.offconstant = offconstant;
+    k.col_feat = col_feat;
+    k.mlp_w = mlp_w;
+    k.col_cap = col_cap;
+    k.tune = tune;
+    return k;
+  }
+  void drop_ref_graph() {
+#ifndef GQM_HOST_EMU
+    if (ref_exec) cudaGraphExecDestroy(ref_exec);
+    if (ref_graph) cudaGraphDestroy(ref_graph);
+#endif
+    ref_exec = nullptr;
+    ref_graph = nullptr;
+  }
+  int capture_refinement() {
+#ifdef GQM_HOST_EMU
+    return GQM_ERR_CUDA;
+#else
+    drop_ref_graph();
+    node_count = 0;
+    cur_node = kMaxNodes;
+    memset(node_kernels, 0, sizeof(node_kernels));
+    cudaGraph_t g = nullptr;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) return GQM_ERR_CUDA;
+    if (cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return GQM_ERR_CUDA;
+    }
+    capturing = true;
+    const long long launches = stats.kernel_launches;
+    int rc = refine_body();
+    capturing = false;
+    stats.kernel_launches = launches;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(st, &cs);
+    if (cs != cudaStreamCaptureStatusNone) {
+      cudaGraph_t t = nullptr;
+      if (cudaStreamEndCapture(st, &t) != cudaSuccess && rc == 0) rc = GQM_ERR_CUDA;
+    }
+    if (rc == 0 && cudaGraphInstantiate(&ref_exec, g, 0) != cudaSuccess) {
+      ref_exec = nullptr;
+      rc = GQM_ERR_CUDA;
+    }
+    if (rc) {
+      cudaGraphDestroy(g);
+      cudaGetLastError();
+      return rc;
+    }
+    ref_graph = g;
+    ref_key = ref_key_now();
     return GQM_OK;
+#endif
+  }
+  // one refinement from the initialised mesh: the captured graph (captured
+  // again when what it depends on changed), or the same steps driven from the
+  // host
+  int run_refinement() {
+    if (use_graph) {
+      const RefKey k = ref_key_now();
+      if (!ref_exec || memcmp(&k, &ref_key, sizeof(k)) != 0) {
+        if (capture_refinement() != GQM_OK) use_graph = false;  // the host-driven steps below
+      }
+      if (use_graph) {
+        if (cudaGraphLaunch(ref_exec, st) != cudaSuccess) return GQM_ERR_CUDA;
+        stats.kernel_launches += node_kernels[kMaxNodes];
+        return GQM_OK;
+      }
+    }
+    return refine_body();
   }
 
   // ---- output compaction (refine.cu:5758-6428) ----
@@ -951,21 +1345,7 @@ struct Refiner {
     triblock = 2 * pointblock;
     pcap = np + pointblock;
     tcap = nt + triblock;
-#ifdef GQM_TEST_TIGHT_BUFFERS
-    // test builds: physical buffers exactly the logical capacity, so every
-    // growth step goes through the reallocation path
-    rc = alloc_points(std::max<long>(pcap, pphys));
-    if (rc) return rc;
-    rc = alloc_tris(std::max<long>(tcap, tphys));
-    if (rc) return rc;
-#else
-    rc = alloc_points(std::max<long>(pcap + 3L * pointblock, pphys));
-    if (rc) return rc;
-    rc = alloc_tris(std::max<long>(tcap + 4L * triblock, tphys));
-    if (rc) return rc;
-#endif
-    rc = alloc_subsegs(std::max<long>(4L * ns + 1024, sphys));
-    if (rc) return rc;
+    want_p = want_t = want_s = want_cav = 0;
     // inputs
     const double *dpts;
     const int *dtri_in, *dnbr_in, *dseg_in;
@@ -1002,6 +1382,36 @@ struct Refiner {
       dtri_in = in->trianglelist;
       dnbr_in = in->neighborlist;
       dseg_in = in->segmentlist;
+    }
+    int attempt = 0;
+  restart:
+    // physical buffers (logical capacities are tracked in DState)
+#ifdef GQM_TEST_TIGHT_BUFFERS
+    // test builds: physical buffers exactly the logical capacity, so a run
+    // that grows the logical capacity is repeated with larger buffers
+    rc = alloc_points(std::max<long>(std::max<long>(pcap, pphys), want_p));
+    if (rc) return rc;
+    rc = alloc_tris(std::max<long>(std::max<long>(tcap, tphys), want_t));
+    if (rc) return rc;
+#else
+    rc = alloc_points(std::max<long>(std::max<long>(pcap + 3L * pointblock, pphys), want_p));
+    if (rc) return rc;
+    rc = alloc_tris(std::max<long>(std::max<long>(tcap + 4L * triblock, tphys), want_t));
+    if (rc) return rc;
+#endif
+    rc = alloc_subsegs(std::max<long>(std::max<long>(4L * ns + 1024, sphys), want_s));
+    if (rc) return rc;
+    {  // stored cavities of the Steiner candidates: kCavityCap rows of cav_cap entries
+      const long want = std::max<long>(std::max<long>(tcap / 4, 1024), want_cav);
+      if (cav_cap < want) {
+        if (cav) cudaFree(cav);
+        if (cavn) cudaFree(cavn);
+        cav = cavn = nullptr;
+        cav_cap = 0;
+        if (dalloc(&cav, (size_t)kCavityCap * want) || dalloc(&cavn, want)) return GQM_ERR_MEMORY;
+        cav_cap = want;
+        buf_gen++;
+      }
     }
     cudaEventRecord(ev0, st);
     if (grow_dev(&segs, &segs_cap, (size_t)ns + 1)) return GQM_ERR_MEMORY;
@@ -1059,45 +1469,50 @@ struct Refiner {
       LAUNCH(k_init_subsegs, nt, M, nt, hkeys, hvals, hsz - 1, s2ti);
       LAUNCH(k_pack_s2t, ns, M, s2ti, ns);
     }
-    last_point = np;
-    last_triangle = nt;
-    last_subseg = ns;
-    nempty_p = refresh_points();
-    nempty_t = refresh_tris();
-    LAUNCH(k_mark_all_encsegs, ns, M, ns);
-    rc = split_encsegs();
-    int rounds = 0;
-    while (rc == 0) {
-      LAUNCH(k_mark_bad, last_triangle, M, last_triangle);
-      compact(PBad{M.tst}, Ident{}, 0, last_triangle, bad, C_LIST2);
-      // the bad count and the device error word in one round trip
-      cudaMemcpyAsync(hcount + C_LIST2, dcount + C_LIST2, sizeof(int), cudaMemcpyDeviceToHost, st);
-      cudaMemcpyAsync(hcount + C_MISC, M.err, sizeof(int), cudaMemcpyDeviceToHost, st);
-      if (cudaStreamSynchronize(st) != cudaSuccess) {
-        rc = GQM_ERR_CUDA;
-        break;
-      }
+    // the driver's state on the device: the reference's logical capacities
+    // and high-water marks, and the physical capacities a run must stay in
+    hds = DState{};
+    hds.pcap = (int)pcap;
+    hds.tcap = (int)tcap;
+    hds.pphys = (int)pphys;
+    hds.tphys = (int)tphys;
+    hds.sphys = (int)sphys;
+    hds.cav_cap = (int)cav_cap;
+    hds.last_point = np;
+    hds.last_triangle = nt;
+    hds.last_subseg = ns;
+    hds.pointblock = pointblock;
+    hds.triblock = triblock;
+    hds.max_rounds = max_rounds;
+    cudaMemcpyAsync(ds, &hds, sizeof(DState), cudaMemcpyHostToDevice, st);
+    rc = run_refinement();
+    if (rc == 0) {
+      cudaMemcpyAsync(&hds, ds, sizeof(DState), cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) rc = GQM_ERR_CUDA;
       stats.host_syncs++;
-      const int nbad = hcount[C_LIST2];
-      const int derr = hcount[C_MISC];
-      if (derr) {
-        rc = derr;
-        break;
-      }
-      if (nbad == 0) break;
-      if (rounds >= max_rounds) {
-        rc = GQM_ERR_ROUND_LIMIT;
-        break;
-      }
-      stats.bad_total += nbad;
-      rc = split_triangles(nbad);
-      if (rc) break;
-      rc = split_encsegs();
-      if (rc) break;
-      LAUNCH(k_points_old, last_point, M, last_point);
-      rounds++;
     }
-    stats.rounds = rounds;
+    if (rc == 0 && hds.need_grow) {
+      // a physical capacity would have been exceeded: repeat the run with
+      // larger buffers (the result does not depend on them)
+      if (++attempt > 8) return GQM_ERR_MEMORY;
+      if (hds.need_grow & 1) want_p = 2 * pphys;
+      if (hds.need_grow & 2) want_t = 2 * tphys;
+      if (hds.need_grow & 4) want_s = 2 * sphys;
+      if (hds.need_grow & 8) want_cav = 2 * cav_cap;
+      pcap = np + pointblock;
+      tcap = nt + triblock;
+      stats = gqm_stats{};
+      goto restart;
+    }
+    last_point = hds.last_point;
+    last_triangle = hds.last_triangle;
+    last_subseg = hds.last_subseg;
+    pcap = hds.pcap;
+    tcap = hds.tcap;
+    stats.rounds = (int)hds.rounds;
+    stats.bad_total = hds.bad_total;
+    if (use_graph)  // kernels of the conditional nodes' bodies, times the bodies ran
+      for (int i = 0; i < node_count; ++i) stats.kernel_launches += hds.iters[i] * node_kernels[i];
     if (rc == 0) rc = check_device_error();
     if (rc == 0) rc = compact_output();
     cudaEventRecord(ev1, st);
@@ -1110,7 +1525,6 @@ struct Refiner {
     float ms = 0;
     cudaEventElapsedTime(&ms, ev0, ev1);
     stats.device_ms = ms;
-    collect_loop_events();
     unsigned long long hc[8];
     cudaMemcpy(hc, dctr, sizeof(hc), cudaMemcpyDeviceToHost);
     stats.learned_candidates = (long long)hc[4];
@@ -1118,9 +1532,9 @@ struct Refiner {
     FlipCtl hf;
     cudaMemcpy(&hf, fc, sizeof(hf), cudaMemcpyDeviceToHost);
     stats.flip_steps = hf.steps;
-    // each graph launch counted one kernel (its loop-entry kernel); the nine
-    // kernels of every loop iteration it ran (a grid step, its condition and
-    // the single-block kernel that runs the small steps after it) are added here
+    // with the graph, the kernels of every grid step of the flip-flop loops (a
+    // grid step, its condition and the single-block kernel that runs the small
+    // steps after it) are added here
     if (use_graph) stats.kernel_launches += (long long)step_kernels() * (hf.steps - hf.small_steps);
     for (int b = 0; b < kFlipProfileBins; ++b) {
       flip_prof_steps[b] = (long long)hf.prof_steps[b];
@@ -1255,9 +1669,9 @@ int gqm_context_probe(gqm_context *ctx, int enable) {
   gqm::k_ktimer_reset<<<1, 32, 0, r.st>>>(r.ktm, enable ? 1 : 0);
   gqm::k_ktimer_reset<<<1, 32, 0, r.st>>>(r.stm, enable ? 1 : 0);
 #endif
-  r.probing = enable != 0;
-  r.probe_loop_ms = 0.0;
-  r.probe_loops = 0;
+  // the device time of the flip-flop loops since this reset (FlipCtl)
+  cudaMemsetAsync(&r.fc->loop_ns, 0, sizeof(r.fc->loop_ns), r.st);
+  cudaMemsetAsync(&r.fc->loops, 0, sizeof(r.fc->loops), r.st);
   return cudaStreamSynchronize(r.st) == cudaSuccess ? GQM_OK : GQM_ERR_CUDA;
 }
 int gqm_context_probe_read(gqm_context *ctx, gqm_probe *p) {
@@ -1265,9 +1679,11 @@ int gqm_context_probe_read(gqm_context *ctx, gqm_probe *p) {
   gqm::Refiner &r = ctx->r;
   if (cudaSetDevice(r.device) != cudaSuccess) return GQM_ERR_CUDA;
   gqm::KTimer h, hs;
+  gqm::FlipCtl hf;
   if (cudaStreamSynchronize(r.st) != cudaSuccess ||
       cudaMemcpy(&h, r.ktm, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess ||
-      cudaMemcpy(&hs, r.stm, sizeof(hs), cudaMemcpyDeviceToHost) != cudaSuccess)
+      cudaMemcpy(&hs, r.stm, sizeof(hs), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(&hf, r.fc, sizeof(hf), cudaMemcpyDeviceToHost) != cudaSuccess)
     return GQM_ERR_CUDA;
   p->small_launches = (long long)hs.launches;
   p->small_items = (long long)hs.items;
@@ -1277,8 +1693,8 @@ int gqm_context_probe_read(gqm_context *ctx, gqm_probe *p) {
   p->check_items = (long long)h.items;
   p->check_ms = (double)h.total_ns * 1e-6;
   for (int i = 0; i < 4; ++i) p->first_items[i] = (long long)h.first_items[i];
-  p->loop_launches = r.probe_loops;
-  p->loop_ms = r.probe_loop_ms;
+  p->loop_launches = (long long)hf.loops;
+  p->loop_ms = (double)hf.loop_ns * 1e-6;
   return GQM_OK;
 }
 int gqm_context_set_tuning(gqm_context *ctx, const gqm_tuning *t) {

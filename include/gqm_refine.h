@@ -130,16 +130,16 @@ int gqm_context_result_sizes(gqm_context *ctx, int *npoints, int *ntriangles, in
  * two kernels that take most of the device time, the grid-wide flip-step check
  * kernel and the small-step kernel (whole flip steps of small active sets in
  * one launch), timestamp every launch on the device: from its first block's
- * start to its last block's end (%globaltimer); CUDA events on the context's
- * stream bracket every launch of the flip loop.  gqm_context_probe(ctx, 1)
+ * start to its last block's end (%globaltimer); the flip-flop loops are timed
+ * on the device as well, from entry to their last step.  gqm_context_probe(ctx, 1)
  * resets and enables, (ctx, 0) disables; gqm_context_probe_read sums since the
  * reset. */
 typedef struct {
   long long check_launches; /* launches of the flip-step check kernel */
   long long check_items;    /* active triangles they checked */
   double check_ms;          /* their summed execution time */
-  long long loop_launches;  /* flip-loop graph launches */
-  double loop_ms;           /* their summed time (CUDA events) */
+  long long loop_launches;  /* flip-flop loops run */
+  double loop_ms;           /* their summed device time (%globaltimer at loop entry and end) */
   long long first_items[4]; /* active triangles of the first four check launches */
   long long small_launches; /* launches of the small-step kernel */
   long long small_items;    /* active triangles of the flip steps they ran */
