@@ -4,6 +4,7 @@
 #include <sys/mman.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <initializer_list>
@@ -32,6 +33,61 @@ static inline void host_copy(std::initializer_list<HostCopy> list) {
     pool.emplace_back([&, t] {
       for (size_t k = t; k < pieces.size(); k += nt) memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
     });
+  for (auto &th : pool) th.join();
+}
+
+// host_copy into one contiguous destination, with the destination handed on
+// while the copy runs: `ready(offset, bytes)` is called (on the calling
+// thread) for every range [offset, offset + bytes) of the destination whose
+// copy is complete, in order, at least `step` bytes at a time, so that the
+// caller can start its upload of the front while the back is still being
+// copied.  The list's destinations must follow one another from dst_base on;
+// the pieces are taken in order by the worker threads and the calling thread.
+template <class Ready>
+static inline void host_copy_streamed(std::initializer_list<HostCopy> list, char *dst_base, size_t step,
+                                      Ready ready) {
+  constexpr size_t kPiece = 4u << 20;
+  std::vector<HostCopy> pieces;
+  for (const HostCopy &c : list)
+    for (size_t o = 0; o < c.bytes; o += kPiece)
+      pieces.push_back({(char *)c.dst + o, (const char *)c.src + o, std::min(kPiece, c.bytes - o)});
+  const size_t np = pieces.size();
+  std::vector<std::atomic<int>> done(np);
+  for (auto &d : done) d.store(0);
+  std::atomic<size_t> next{0};
+  auto work = [&] {
+    for (size_t k = next.fetch_add(1); k < np; k = next.fetch_add(1)) {
+      memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
+      done[k].store(1, std::memory_order_release);
+    }
+  };
+  const int nt = (int)std::min<size_t>(np, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+  // the calling thread hands on the completed front, and copies when it has nothing to hand on
+  size_t front = 0;         // pieces known complete
+  size_t handed = 0;        // destination bytes handed on
+  size_t complete_end = 0;  // destination end of the completed prefix
+  while (front < np || handed < complete_end) {
+    size_t k = front;
+    while (k < np && done[k].load(std::memory_order_acquire)) {
+      complete_end = (size_t)((char *)pieces[k].dst + pieces[k].bytes - dst_base);
+      ++k;
+    }
+    front = k;
+    if (complete_end - handed >= step || (front == np && complete_end > handed)) {
+      ready(handed, complete_end - handed);
+      handed = complete_end;
+      continue;
+    }
+    const size_t j = next.fetch_add(1);
+    if (j < np) {
+      memcpy(pieces[j].dst, pieces[j].src, pieces[j].bytes);
+      done[j].store(1, std::memory_order_release);
+    } else {
+      std::this_thread::yield();
+    }
+  }
   for (auto &th : pool) th.join();
 }
 

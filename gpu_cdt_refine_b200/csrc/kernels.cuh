@@ -1751,32 +1751,59 @@ GQM_KERNEL void k_remove_losers(Mesh M, const int *bad, const int *dn, const int
 // to a triangle already in the region, and neither changes while the walk runs.
 // So each stack frame keeps the edge to resume at: the same triangles are
 // visited and claimed in the same order, each neighbour tested once.
+//
+// The three neighbours of a triangle are tested together when the walk first
+// reaches it, with all their loads in flight at once (rows, then points), and
+// the outcomes are kept in the frame; which edge the walk takes is still decided
+// edge by edge from the resume point, with the region as it is then.  Nothing a
+// test reads changes during the walk (only claim markers do), so the walk takes
+// the same edges as one that tests each neighbour when it gets to it.
 template <int PRED>
 __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, int badIndex, int *out,
                            int stride) {
   int region[kCavityCap], loop[kCavityCap];  // loop: (triangle << 2) | edge to resume at
+  uint8_t inside[kCavityCap];                // per frame: neighbours whose circumcircle holds cc
   int rsize = 0, lsize = 0;
   int cur = sink, start = 0;
   for (int guard = 0; guard < 4 * kCavityCap * 3 + 16; ++guard) {
+    int4 nb = make_int4(-1, -1, -1, -1);
     if (start == 0) {  // first visit (a return always resumes past the edge it left by)
       if (rsize == kCavityCap || lsize == kCavityCap) return -1;
       region[rsize++] = cur;
       loop[lsize++] = cur << 2;
       atomicMin(M.tmark + cur, badIndex);
+      const int4 sg = M.tsg[cur];
+      nb = M.tn[cur];
+      int tt[3];
+      int4 q[3];
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const int si = comp(sg, i);
+        bool ok = comp(nb, i) != -1;
+        if (cur == sink) {
+          if (direction == 3 && si != -1) ok = false;
+          if (direction < 3 && si != -1 && i != direction) ok = false;
+        } else if (si != -1) {
+          ok = false;
+        }
+        tt[i] = ok ? dtri(comp(nb, i)) : -1;
+      }
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+        if (tt[i] >= 0) q[i] = M.tv[tt[i]];
+      unsigned bits = 0;
+#pragma unroll
+      for (int i = 0; i < 3; i++)
+        if (tt[i] >= 0 && incircle<PRED>(M.pts[q[i].x], M.pts[q[i].y], M.pts[q[i].z], cc) > 0) bits |= 1u << i;
+      inside[lsize - 1] = (uint8_t)bits;
+    } else if (inside[lsize - 1] >> start) {
+      nb = M.tn[cur];
     }
     int nIdx = -1, taken = -1;
-    int4 sg = M.tsg[cur];
-    int4 nb = M.tn[cur];
+    const unsigned bits = inside[lsize - 1];
     for (int i = start; i < 3; i++) {
-      int si = comp(sg, i);
-      if (cur == sink) {
-        if (direction == 3 && si != -1) continue;
-        if (direction < 3 && si != -1 && i != direction) continue;
-      } else if (si != -1)
-        continue;
-      int neighbor = comp(nb, i);
-      if (neighbor == -1) continue;
-      int t = dtri(neighbor);
+      if (!((bits >> i) & 1u)) continue;
+      const int t = dtri(comp(nb, i));
       bool seen = false;
       for (int r = 0; r < rsize; ++r)
         if (region[r] == t) {
@@ -1784,13 +1811,9 @@ __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, i
           break;
         }
       if (seen) continue;
-      int4 q = M.tv[t];
-      double r = incircle<PRED>(M.pts[q.x], M.pts[q.y], M.pts[q.z], cc);
-      if (r > 0) {
-        nIdx = t;
-        taken = i;
-        break;
-      }
+      nIdx = t;
+      taken = i;
+      break;
     }
     if (taken >= 0) {
       loop[lsize - 1] = (cur << 2) | (taken + 1);

@@ -59,6 +59,68 @@ int gqm_fallbacks_cluster(unsigned long long *sum, int reset, cudaStream_t st);
 namespace gqm {
 
 // ============================================================================
+// Pinned blocks for large results.  A result of gqm_refine /
+// gqm_context_result of at least kPoolMinBytes is downloaded straight into a
+// block of pinned host memory that the caller then owns until
+// gqm_free_result, which gives the block back for the next result: no second
+// copy from a staging buffer and no page faults on fresh memory.  The pool
+// holds at most kPoolMaxBytes; when no block fits and the limit is reached,
+// the result takes the malloc path (staging buffer, then copies).
+// ============================================================================
+constexpr size_t kPoolMinBytes = 16ull << 20;
+constexpr size_t kPoolMaxBytes = 2ull << 30;
+struct PoolBlock {
+  char *p;
+  size_t cap;
+  bool in_use;
+};
+static std::mutex g_pool_mutex;
+static std::vector<PoolBlock> g_pool;
+static size_t g_pool_bytes = 0;
+// a block of at least `bytes`, or nullptr
+static char *pool_take(size_t bytes) {
+  if (bytes < kPoolMinBytes) return nullptr;
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  PoolBlock *best = nullptr;
+  for (PoolBlock &b : g_pool)
+    if (!b.in_use && b.cap >= bytes && (!best || b.cap < best->cap)) best = &b;
+  if (best) {
+    best->in_use = true;
+    return best->p;
+  }
+  // make room: drop free blocks, which are all too small
+  for (size_t k = 0; k < g_pool.size() && g_pool_bytes + bytes > kPoolMaxBytes;) {
+    if (!g_pool[k].in_use) {
+      cudaFreeHost(g_pool[k].p);
+      g_pool_bytes -= g_pool[k].cap;
+      g_pool.erase(g_pool.begin() + (long)k);
+    } else {
+      ++k;
+    }
+  }
+  if (g_pool_bytes + bytes > kPoolMaxBytes) return nullptr;
+  char *p = nullptr;
+  if (cudaMallocHost((void **)&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  g_pool.push_back(PoolBlock{p, bytes, true});
+  g_pool_bytes += bytes;
+  return p;
+}
+// true when p is a lent pool block (now free again)
+static bool pool_give(const void *p) {
+  if (!p) return false;
+  std::lock_guard<std::mutex> lock(g_pool_mutex);
+  for (PoolBlock &b : g_pool)
+    if (b.p == p && b.in_use) {
+      b.in_use = false;
+      return true;
+    }
+  return false;
+}
+
+// ============================================================================
 // Ordered stream compaction: out[k] = map(i) for the k-th i in [lo, hi) with
 // pred(i), in ascending i.  Three launches: per-block counts, one-block scan,
 // per-block ordered emit (warp ballots).  No spin waits.
@@ -433,51 +495,91 @@ __global__ void k_fill_at(int *base, DevInt off, DevInt n, int v) {
   GS_LOOP(i, cnt) a[i] = v;
 }
 
-// Ordered compaction over [0, *hi) whose bound an earlier kernel wrote: a
-// fixed grid of kDevCompactBlocks blocks, each covering a contiguous chunk
-// (whole tiles), then the same scan and emit as above.
+// Ordered compaction over [0, *hi) whose bound an earlier kernel wrote, in one
+// launch of kDevCompactBlocks blocks: each block takes the next chunk (whole
+// tiles) in the order the blocks start (a claimed counter, so every chunk
+// before a block's own belongs to a block that is already running), counts
+// it, publishes the count, adds up its predecessors' published values back to
+// the nearest full prefix (decoupled look-back, 32 predecessors at a time),
+// publishes its own prefix and emits.  The last block to finish writes the
+// total and clears the published words and the counters for the next call.
+// Every wait is bounded: a wait that runs out records GQM_ERR_TOPOLOGY and the
+// block goes on.
 constexpr int kDevCompactBlocks = 296;
+constexpr long long kLookbackSpins = 1ll << 22;
+struct CompactSync {
+  unsigned long long word[kDevCompactBlocks];  // (state << 32) | value; state 1: count, 2: prefix through the chunk
+  unsigned next_chunk, finished;
+};
 __device__ __forceinline__ int dev_chunk(int n) {
   int chunk = (n + kDevCompactBlocks - 1) / kDevCompactBlocks;
   chunk = max(chunk, kCompactTile);
   return (chunk + kCompactTile - 1) / kCompactTile * kCompactTile;
 }
-template <class F>
-__global__ void __launch_bounds__(kCompactThreads) k_cnt_dev(F f, DevInt hi_, int *bc) {
+template <class F, class Mp>
+__global__ void __launch_bounds__(kCompactThreads) k_compact1(F f, Mp m, DevInt hi_, int *out, int *total,
+                                                              CompactSync *cs, int *err) {
+  __shared__ int wsum[kCompactThreads / 32];
+  __shared__ int sh_chunk, sh_base;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (threadIdx.x == 0) sh_chunk = (int)atomicAdd(&cs->next_chunk, 1u);
+  __syncthreads();
+  const int b = sh_chunk;
   const int hi = nval(hi_), chunk = dev_chunk(hi);
-  const int b0 = min(hi, (int)blockIdx.x * chunk), b1 = min(hi, b0 + chunk);
+  const int b0 = min(hi, b * chunk), b1 = min(hi, b0 + chunk);
+  // count
   int c = 0;
   for (int s = b0 + threadIdx.x * kCompactItems; s < b1; s += kCompactTile) {
 #pragma unroll
     for (int j = 0; j < kCompactItems; ++j)
       if (s + j < b1 && f(s + j)) ++c;
   }
-  __shared__ int red[32];
   for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+  if (lane == 0) wsum[warp] = c;
   __syncthreads();
-  if (threadIdx.x < 32) {
-    int v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0;
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (threadIdx.x == 0) bc[blockIdx.x] = v;
+  if (warp == 0) {  // publish, then look back 32 predecessors at a time
+    int cnt = 0;
+    for (int w = 0; w < kCompactThreads / 32; ++w) cnt += wsum[w];
+    volatile unsigned long long *word = cs->word;
+    int prefix = 0;
+    if (b == 0) {
+      if (lane == 0) atomicExch(&cs->word[0], (2ull << 32) | (unsigned)cnt);
+    } else {
+      if (lane == 0) atomicExch(&cs->word[b], (1ull << 32) | (unsigned)cnt);
+      for (int top = b - 1; top >= 0; top -= 32) {
+        const int j = top - lane;
+        unsigned long long v = 2ull << 32;  // before chunk 0: a prefix of zero
+        if (j >= 0) {
+          v = word[j];
+          long long spins = 0;
+          while ((v >> 32) == 0 && ++spins < kLookbackSpins) v = word[j];
+          if ((v >> 32) == 0) {  // gave up: the count is wrong, and the run reports it
+            atomicCAS(err, 0, GQM_ERR_TOPOLOGY);
+            v = 2ull << 32;
+          }
+        }
+        const unsigned full = __ballot_sync(0xffffffffu, (v >> 32) == 2);
+        const int stop = full ? __ffs(full) - 1 : 31;  // the nearest full prefix (lane 0 is the nearest chunk)
+        int x = lane <= stop ? (int)(unsigned)v : 0;
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+        prefix += __shfl_sync(0xffffffffu, x, 0);
+        if (full) break;
+      }
+      if (lane == 0) atomicExch(&cs->word[b], (2ull << 32) | (unsigned)(prefix + cnt));
+    }
+    if (lane == 0) sh_base = prefix;
   }
-}
-template <class F, class Mp>
-__global__ void __launch_bounds__(kCompactThreads) k_emit_dev(F f, Mp m, DevInt hi_, const int *bc, int *out) {
-  const int hi = nval(hi_), chunk = dev_chunk(hi);
-  const int b0 = min(hi, (int)blockIdx.x * chunk), b1 = min(hi, b0 + chunk);
-  if (b0 >= b1) return;  // the whole block leaves: no barrier below is skipped by part of it
-  __shared__ int wsum[kCompactThreads / 32];
-  int base = bc[blockIdx.x];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  // emit
+  int base = sh_base;
   for (int tile = b0; tile < b1; tile += kCompactTile) {
     const int s = tile + threadIdx.x * kCompactItems;
     unsigned bits = 0;
 #pragma unroll
     for (int j = 0; j < kCompactItems; ++j)
       if (s + j < b1 && f(s + j)) bits |= 1u << j;
-    const int c = __popc(bits);
-    int x = c;
+    const int cc = __popc(bits);
+    int x = cc;
     for (int o = 1; o < 32; o <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, x, o);
       if (lane >= o) x += y;
@@ -491,7 +593,7 @@ __global__ void __launch_bounds__(kCompactThreads) k_emit_dev(F f, Mp m, DevInt 
       woff += (w < warp) ? v : 0;
       tot += v;
     }
-    int pos = base + woff + x - c;
+    int pos = base + woff + x - cc;
     while (bits) {
       const int j = __ffs(bits) - 1;
       bits &= bits - 1;
@@ -499,6 +601,18 @@ __global__ void __launch_bounds__(kCompactThreads) k_emit_dev(F f, Mp m, DevInt 
     }
     base += tot;
     __syncthreads();
+  }
+  // the last block: total, and a clean slate for the next call
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(&cs->finished, 1u) == kDevCompactBlocks - 1) {
+      __threadfence();
+      *total = (int)(unsigned)((volatile unsigned long long *)cs->word)[kDevCompactBlocks - 1];
+      for (int j = 0; j < kDevCompactBlocks; ++j) cs->word[j] = 0;
+      cs->next_chunk = 0;
+      cs->finished = 0;
+      __threadfence();
+    }
   }
 }
 
@@ -531,6 +645,7 @@ struct Refiner {
   // the driver's state on the device, and the refinement captured as one
   // CUDA graph (loops and branches as conditional nodes)
   DState *ds = nullptr;
+  CompactSync *csync = nullptr;  // look-back words of the one-launch compactions (zero between calls)
   DState hds{};             // host copy: written before a run, read after it
   bool use_graph = true;    // false: the host reads each condition (GQM_NO_GRAPH=1, emulated build)
   bool capturing = false;   // the refinement graph is being captured
@@ -634,7 +749,7 @@ struct Refiner {
                     M.s2t, M.s2seg, M.enc, M.err, stm, emptyt, bad, imark, ilist, sinks, wl, act, win, neg, ll, sl,
                     newidx, tail, center, emptyp, pnew, enclist, encl2, smark, mids, snap, segs, dcount, bc,
                     dctr, dgc, dinput, mlp_w, mlp_b, M.fstamp, M.tstamp, fq, tl, clr, fc, cav, cavn, ktm, M.wbits, M.wcnt, M.wsup, M.wmeg,
-                    ds};
+                    ds, csync};
     for (void *p : ptrs)
       if (p) cudaFree(p);
     if (hcount) cudaFreeHost(hcount);
@@ -649,6 +764,7 @@ struct Refiner {
     mlp_w = nullptr;
     mlp_b = nullptr;
     ds = nullptr;
+    csync = nullptr;
     center = nullptr;
     cav = cavn = nullptr;
     cav_cap = 0;
@@ -682,8 +798,10 @@ struct Refiner {
     if (!ev1) cudaEventCreate(&ev1);
     if (!dcount) {
       if (dalloc(&dcount, 16) || dalloc(&bc, kMaxCompactBlocks + 1) || dalloc(&dctr, 8) || dalloc(&dgc, 2) ||
-          dalloc(&M.err, 1) || dalloc(&fc, 1) || dalloc(&ktm, 1) || dalloc(&stm, 1) || dalloc(&ds, 1))
+          dalloc(&M.err, 1) || dalloc(&fc, 1) || dalloc(&ktm, 1) || dalloc(&stm, 1) || dalloc(&ds, 1) ||
+          dalloc(&csync, 1))
         return GQM_ERR_MEMORY;
+      cudaMemsetAsync(csync, 0, sizeof(CompactSync), st);
       cudaMemsetAsync(fc, 0, sizeof(FlipCtl), st);
       cudaMemsetAsync(ktm, 0, sizeof(KTimer), st);  // off until gqm_context_probe
       cudaMemsetAsync(stm, 0, sizeof(KTimer), st);
@@ -952,12 +1070,10 @@ struct Refiner {
     for (int i = 0; i < *hi; ++i)
       if (f(i)) out[c++] = m(i);
     *cnt = c;
-    count_launch(3);
+    count_launch(1);
 #else
-    KL(k_cnt_dev, kDevCompactBlocks, kCompactThreads)(f, DevInt{hi}, bc);
-    KL(k_scan, 1, 1024)(bc, kDevCompactBlocks, cnt);
-    KL(k_emit_dev, kDevCompactBlocks, kCompactThreads)(f, m, DevInt{hi}, bc, out);
-    count_launch(3);
+    KL(k_compact1, kDevCompactBlocks, kCompactThreads)(f, m, DevInt{hi}, out, cnt, csync, M.err);
+    count_launch(1);
 #endif
   }
 
@@ -1193,7 +1309,7 @@ struct Refiner {
     Mesh M;
     long buf_gen;
     int pred_mode, placement, offcenter, offconstant;
-    const void *col_feat, *mlp_w;
+    const void *col_feat, *col_tgt, *col_cnt, *mlp_w, *mlp_b;
     unsigned long long col_cap;
     Tuning tune;
   };
@@ -1208,7 +1324,10 @@ struct Refiner {
     k.offcenter = offcenter;
     k.offconstant = offconstant;
     k.col_feat = col_feat;
+    k.col_tgt = col_tgt;
+    k.col_cnt = col_cnt;
     k.mlp_w = mlp_w;
+    k.mlp_b = mlp_b;
     k.col_cap = col_cap;
     k.tune = tune;
     return k;
@@ -1366,13 +1485,15 @@ struct Refiner {
       int *t0 = (int *)(base + sizeof(double) * 2 * np);
       int *n0 = t0 + 3L * nt;
       int *s0 = n0 + 3L * nt;
-      // the caller's arrays are packed into pinned memory on the host's cores,
-      // then uploaded with one copy
+      // the caller's arrays are packed into pinned memory on the host's cores
+      // and uploaded in pieces of 32 MB, the front while the back is packed
       if (grow_pinned(need)) return GQM_ERR_MEMORY;
       const size_t bp = sizeof(double) * 2 * np, bt = sizeof(int) * 3 * nt, bs = sizeof(int) * 2 * ns;
-      host_copy({{h_stage, in->pointlist, bp}, {h_stage + bp, in->trianglelist, bt},
-                 {h_stage + bp + bt, in->neighborlist, bt}, {h_stage + bp + 2 * bt, in->segmentlist, bs}});
-      cudaMemcpyAsync(base, h_stage, bp + 2 * bt + bs, cudaMemcpyHostToDevice, st);
+      host_copy_streamed({{h_stage, in->pointlist, bp}, {h_stage + bp, in->trianglelist, bt},
+                          {h_stage + bp + bt, in->neighborlist, bt}, {h_stage + bp + 2 * bt, in->segmentlist, bs}},
+                         h_stage, 32u << 20, [&](size_t off, size_t bytes) {
+                           cudaMemcpyAsync(base + off, h_stage + off, bytes, cudaMemcpyHostToDevice, st);
+                         });
       dpts = p0;
       dtri_in = t0;
       dnbr_in = n0;
@@ -1571,6 +1692,23 @@ struct Refiner {
     LAUNCH(k_emit_output, std::max(nt, ns), M, (int)nt, (int)ns, (int *)(d_out + o_tri), (int *)(d_out + o_nbr),
            (int *)(d_out + o_seg), (uint8_t *)(d_out + o_ts));
     LAUNCH(k_emit_pstatus, np, M, (int)np, (uint8_t *)(d_out + o_ps));
+    if (char *blk = pool_take(bytes)) {  // straight into a pinned block the caller owns until gqm_free_result
+      cudaMemcpyAsync(blk, d_out, bytes, cudaMemcpyDeviceToHost, st);
+      if (cudaStreamSynchronize(st) != cudaSuccess) {
+        pool_give(blk);
+        return GQM_ERR_CUDA;
+      }
+      out->numberofpoints = (int)np;
+      out->numberoftriangles = (int)nt;
+      out->numberofsegments = (int)ns;
+      out->pointlist = (double *)blk;
+      out->trianglelist = (int *)(blk + o_tri);
+      out->neighborlist = (int *)(blk + o_nbr);
+      out->segmentlist = (int *)(blk + o_seg);
+      out->pstatus = (unsigned char *)(blk + o_ps);
+      out->tstatus = (unsigned char *)(blk + o_ts);
+      return GQM_OK;
+    }
     cudaMemcpyAsync(h_stage, d_out, bytes, cudaMemcpyDeviceToHost, st);
     out->numberofpoints = (int)np;
     out->numberoftriangles = (int)nt;
@@ -1934,6 +2072,10 @@ int gqm_refine_batch(int ndomains, const gqm_cdt_in *in, gqm_cdt_out *out, const
 
 void gqm_free_result(gqm_cdt_out *out) {
   if (!out) return;
+  if (gqm::pool_give(out->pointlist)) {  // one pinned block holds all six arrays
+    memset(out, 0, sizeof(*out));
+    return;
+  }
   free(out->pointlist);
   free(out->trianglelist);
   free(out->neighborlist);

@@ -62,9 +62,13 @@ typedef struct {
   const int *segmentlist;    /* 2 * numberofsegments */
 } gqm_cdt_in;
 
-/* Output CDT.  Arrays are allocated by the library with malloc() and released
- * with gqm_free_result().  pstatus / tstatus hold the reference's PStatus /
- * TStatus bytes of the compacted points / triangles (refine.h:36-205). */
+/* Output CDT.  Arrays are allocated by the library and released with
+ * gqm_free_result() (never free() them one by one): a result of 16 MB or more
+ * lives in one block of pinned host memory that the library downloads into
+ * directly and reuses for a later result once it is released (at most 2 GB of
+ * such blocks); a smaller one is malloc()ed.  pstatus / tstatus hold the
+ * reference's PStatus / TStatus bytes of the compacted points / triangles
+ * (refine.h:36-205). */
 typedef struct {
   int numberofpoints;
   double *pointlist;

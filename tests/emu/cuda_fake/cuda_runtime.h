@@ -102,6 +102,11 @@ inline int atomicExch(int *a, int v) {
   *a = v;
   return o;
 }
+inline unsigned long long atomicExch(unsigned long long *a, unsigned long long v) {
+  unsigned long long o = *a;
+  *a = v;
+  return o;
+}
 inline int atomicAdd(int *a, int v) {
   int o = *a;
   *a += v;
