@@ -57,11 +57,11 @@ METRIC = "output triangles/s at theta=20 deg, 1 B200 (learned vs plain); output 
 CHECK_BYTES_PER_ITEM = 4 + 36 + 3 + 48 + 66 + 1
 # DRAM bytes (read + write) per active triangle of the same kernel, from
 # `ncu --set full` on its first launch of the 1,000,000-point clustered case
-# (profiles/k_check_flip2_clustered1M.md: 72.92 MB for 162,684 triangles).
-CHECK_DRAM_BYTES_PER_ITEM = 72.92e6 / 162684
+# (profiles/k_check_flip2_clustered1M.md: 72.22 MB for 162,684 triangles).
+CHECK_DRAM_BYTES_PER_ITEM = 72.22e6 / 162684
 # FP64-pipe utilisation of the same launch (sm__inst_executed_pipe_fp64, % of
 # peak sustained active): the exact-predicate filters are a small part of its work.
-CHECK_FP64_PIPE_PCT = 4.36
+CHECK_FP64_PIPE_PCT = 4.26
 # Algorithmic bytes of one whole flip step, for the small-step kernel (it runs
 # every phase of a step in one launch), per active triangle: the check
 # (CHECK_BYTES_PER_ITEM), the winner test (list entry 4, deferred-clear byte

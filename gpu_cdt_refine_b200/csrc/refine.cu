@@ -501,10 +501,11 @@ __global__ void k_fill_at(int *base, DevInt off, DevInt n, int v) {
 // before a block's own belongs to a block that is already running), counts
 // it, publishes the count, adds up its predecessors' published values back to
 // the nearest full prefix (decoupled look-back, 32 predecessors at a time),
-// publishes its own prefix and emits.  The last block to finish writes the
-// total and clears the published words and the counters for the next call.
-// Every wait is bounded: a wait that runs out records GQM_ERR_TOPOLOGY and the
-// block goes on.
+// publishes its own prefix and emits.  Chunks past the end of the range are
+// skipped (a short range is one block's work, with no look-back), the block
+// of the last chunk writes the total, and the last block to finish clears the
+// published words and the counters for the next call.  Every wait is
+// bounded: a wait that runs out records GQM_ERR_TOPOLOGY and the block goes on.
 constexpr int kDevCompactBlocks = 296;
 constexpr long long kLookbackSpins = 1ll << 22;
 struct CompactSync {
@@ -526,89 +527,94 @@ __global__ void __launch_bounds__(kCompactThreads) k_compact1(F f, Mp m, DevInt 
   __syncthreads();
   const int b = sh_chunk;
   const int hi = nval(hi_), chunk = dev_chunk(hi);
-  const int b0 = min(hi, b * chunk), b1 = min(hi, b0 + chunk);
-  // count
-  int c = 0;
-  for (int s = b0 + threadIdx.x * kCompactItems; s < b1; s += kCompactTile) {
+  const int last = hi > 0 ? (hi - 1) / chunk : 0;  // the last chunk with elements (0 for an empty range)
+  if (b <= last) {  // (the same for the whole block)
+    const int b0 = min(hi, b * chunk), b1 = min(hi, b0 + chunk);
+    // count
+    int c = 0;
+    for (int s = b0 + threadIdx.x * kCompactItems; s < b1; s += kCompactTile) {
 #pragma unroll
-    for (int j = 0; j < kCompactItems; ++j)
-      if (s + j < b1 && f(s + j)) ++c;
-  }
-  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
-  if (lane == 0) wsum[warp] = c;
-  __syncthreads();
-  if (warp == 0) {  // publish, then look back 32 predecessors at a time
-    int cnt = 0;
-    for (int w = 0; w < kCompactThreads / 32; ++w) cnt += wsum[w];
-    volatile unsigned long long *word = cs->word;
-    int prefix = 0;
-    if (b == 0) {
-      if (lane == 0) atomicExch(&cs->word[0], (2ull << 32) | (unsigned)cnt);
-    } else {
-      if (lane == 0) atomicExch(&cs->word[b], (1ull << 32) | (unsigned)cnt);
-      for (int top = b - 1; top >= 0; top -= 32) {
-        const int j = top - lane;
-        unsigned long long v = 2ull << 32;  // before chunk 0: a prefix of zero
-        if (j >= 0) {
-          v = word[j];
-          long long spins = 0;
-          while ((v >> 32) == 0 && ++spins < kLookbackSpins) v = word[j];
-          if ((v >> 32) == 0) {  // gave up: the count is wrong, and the run reports it
-            atomicCAS(err, 0, GQM_ERR_TOPOLOGY);
-            v = 2ull << 32;
+      for (int j = 0; j < kCompactItems; ++j)
+        if (s + j < b1 && f(s + j)) ++c;
+    }
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+    if (lane == 0) wsum[warp] = c;
+    __syncthreads();
+    if (warp == 0) {  // publish, then look back 32 predecessors at a time
+      int cnt = 0;
+      for (int w = 0; w < kCompactThreads / 32; ++w) cnt += wsum[w];
+      volatile unsigned long long *word = cs->word;
+      int prefix = 0;
+      if (b == 0) {
+        if (lane == 0) atomicExch(&cs->word[0], (2ull << 32) | (unsigned)cnt);
+      } else {
+        if (lane == 0) atomicExch(&cs->word[b], (1ull << 32) | (unsigned)cnt);
+        for (int top = b - 1; top >= 0; top -= 32) {
+          const int j = top - lane;
+          unsigned long long v = 2ull << 32;  // before chunk 0: a prefix of zero
+          if (j >= 0) {
+            v = word[j];
+            long long spins = 0;
+            while ((v >> 32) == 0 && ++spins < kLookbackSpins) v = word[j];
+            if ((v >> 32) == 0) {  // gave up: the count is wrong, and the run reports it
+              atomicCAS(err, 0, GQM_ERR_TOPOLOGY);
+              v = 2ull << 32;
+            }
           }
+          const unsigned full = __ballot_sync(0xffffffffu, (v >> 32) == 2);
+          const int stop = full ? __ffs(full) - 1 : 31;  // the nearest full prefix (lane 0 is the nearest chunk)
+          int x = lane <= stop ? (int)(unsigned)v : 0;
+          for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+          prefix += __shfl_sync(0xffffffffu, x, 0);
+          if (full) break;
         }
-        const unsigned full = __ballot_sync(0xffffffffu, (v >> 32) == 2);
-        const int stop = full ? __ffs(full) - 1 : 31;  // the nearest full prefix (lane 0 is the nearest chunk)
-        int x = lane <= stop ? (int)(unsigned)v : 0;
-        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-        prefix += __shfl_sync(0xffffffffu, x, 0);
-        if (full) break;
+        if (lane == 0) atomicExch(&cs->word[b], (2ull << 32) | (unsigned)(prefix + cnt));
       }
-      if (lane == 0) atomicExch(&cs->word[b], (2ull << 32) | (unsigned)(prefix + cnt));
+      if (lane == 0) {
+        sh_base = prefix;
+        if (b == last) *total = prefix + cnt;
+      }
     }
-    if (lane == 0) sh_base = prefix;
-  }
-  __syncthreads();
-  // emit
-  int base = sh_base;
-  for (int tile = b0; tile < b1; tile += kCompactTile) {
-    const int s = tile + threadIdx.x * kCompactItems;
-    unsigned bits = 0;
-#pragma unroll
-    for (int j = 0; j < kCompactItems; ++j)
-      if (s + j < b1 && f(s + j)) bits |= 1u << j;
-    const int cc = __popc(bits);
-    int x = cc;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
-    }
-    if (lane == 31) wsum[warp] = x;
     __syncthreads();
-    int woff = 0, tot = 0;
+    // emit
+    int base = sh_base;
+    for (int tile = b0; tile < b1; tile += kCompactTile) {
+      const int s = tile + threadIdx.x * kCompactItems;
+      unsigned bits = 0;
 #pragma unroll
-    for (int w = 0; w < kCompactThreads / 32; ++w) {
-      const int v = wsum[w];
-      woff += (w < warp) ? v : 0;
-      tot += v;
+      for (int j = 0; j < kCompactItems; ++j)
+        if (s + j < b1 && f(s + j)) bits |= 1u << j;
+      const int cc = __popc(bits);
+      int x = cc;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) wsum[warp] = x;
+      __syncthreads();
+      int woff = 0, tot = 0;
+#pragma unroll
+      for (int w = 0; w < kCompactThreads / 32; ++w) {
+        const int v = wsum[w];
+        woff += (w < warp) ? v : 0;
+        tot += v;
+      }
+      int pos = base + woff + x - cc;
+      while (bits) {
+        const int j = __ffs(bits) - 1;
+        bits &= bits - 1;
+        out[pos++] = m(s + j);
+      }
+      base += tot;
+      __syncthreads();
     }
-    int pos = base + woff + x - cc;
-    while (bits) {
-      const int j = __ffs(bits) - 1;
-      bits &= bits - 1;
-      out[pos++] = m(s + j);
-    }
-    base += tot;
-    __syncthreads();
   }
-  // the last block: total, and a clean slate for the next call
+  // the last block to finish: a clean slate for the next call
   if (threadIdx.x == 0) {
     __threadfence();
     if (atomicAdd(&cs->finished, 1u) == kDevCompactBlocks - 1) {
       __threadfence();
-      *total = (int)(unsigned)((volatile unsigned long long *)cs->word)[kDevCompactBlocks - 1];
-      for (int j = 0; j < kDevCompactBlocks; ++j) cs->word[j] = 0;
+      for (int j = 0; j <= last; ++j) cs->word[j] = 0;
       cs->next_chunk = 0;
       cs->finished = 0;
       __threadfence();
