@@ -365,11 +365,13 @@ def run_construction(pts, seg, e2e_ms, local_rank):
     except Exception as e:  # the reference build is test infrastructure; report, do not fail
         res["triangle_ms"] = None
         res["triangle_unavailable"] = str(e)
+    # the first call builds the contexts, the second allocates the second pinned
+    # result block (the first result is still held): both are set-up, not steady state
     walls = []
-    for i in range(3):
+    for i in range(5):
         t0 = time.perf_counter()
         out, _, _ = triangulate.triangulate_refine(pts, seg, device=local_rank)
-        if i:
+        if i >= 2:
             walls.append((time.perf_counter() - t0) * 1e3)
     res["points_to_refined_mesh_ms"] = float(np.median(walls))
     res["points_to_refined_mesh_triangles"] = out.numberoftriangles
