@@ -322,6 +322,10 @@ def run_learned(cdt, args, local_rank):
                            "fallback_rate": 1.0 - sl["learned_used"] / max(sl["learned_candidates"], 1),
                            "certified": bool(cert["ok"]), "min_angle_deg": cert["min_angle_deg"],
                            "triangles_below_theta": cert["triangles_below_theta"]}
+    # the network alone: one inference launch over as many rows as the run had
+    # candidates (the run spreads them over its rounds, with the features)
+    mlp_ms = refine.mlp_time(params, sl["learned_candidates"], device=local_rank)
+    res["clustered_2M"].update({"mlp_ms_all_candidates": mlp_ms, "mlp_share_of_learned_run": mlp_ms / sl["device_ms"]})
     doms, _ = inputs.batch_domains(256, seed=20261209)
     gp, _, rp = refine.refine_batch_persistent(doms, 20.0, device=local_rank, with_report=True)
     gl, stl, rl = refine.refine_batch_persistent(doms, 20.0, device=local_rank, with_report=True, mlp=params)

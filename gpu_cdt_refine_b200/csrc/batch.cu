@@ -30,6 +30,8 @@
 #include <thread>
 #include <vector>
 
+#include "host_copy.h"
+
 #include "../../include/gqm_refine.h"
 #include "kernels.cuh"
 
@@ -993,17 +995,25 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
       return GQM_ERR_MEMORY;
     C.jobs_cap = n;
   }
-  // inputs packed into pinned memory, one upload
+  // inputs packed into pinned memory on the host's cores and uploaded in
+  // pieces of 32 MB, the front while the back is packed
   std::vector<Job> jobs(n);
-  parallel_for(n, [&](int k) {
-    const gqm_cdt_in &D = in[ids[k]];
-    char *h = C.h_in + in_off[k];
-    const size_t bp = up256(16ull * D.numberofpoints), bt = up256(12ull * D.numberoftriangles);
-    memcpy(h, D.pointlist, 16ull * D.numberofpoints);
-    memcpy(h + bp, D.trianglelist, 12ull * D.numberoftriangles);
-    memcpy(h + bp + bt, D.neighborlist, 12ull * D.numberoftriangles);
-    if (D.numberofsegments) memcpy(h + bp + 2 * bt, D.segmentlist, 8ull * D.numberofsegments);
-  });
+  {
+    std::vector<HostCopy> parts;
+    parts.reserve(4 * (size_t)n);
+    for (int k = 0; k < n; ++k) {
+      const gqm_cdt_in &D = in[ids[k]];
+      char *h = C.h_in + in_off[k];
+      const size_t bp = up256(16ull * D.numberofpoints), bt = up256(12ull * D.numberoftriangles);
+      parts.push_back({h, D.pointlist, 16ull * D.numberofpoints});
+      parts.push_back({h + bp, D.trianglelist, 12ull * D.numberoftriangles});
+      parts.push_back({h + bp + bt, D.neighborlist, 12ull * D.numberoftriangles});
+      if (D.numberofsegments) parts.push_back({h + bp + 2 * bt, D.segmentlist, 8ull * D.numberofsegments});
+    }
+    host_copy_streamed(parts, C.h_in, 32u << 20, [&](size_t off, size_t bytes) {
+      cudaMemcpyAsync(C.d_in + off, C.h_in + off, bytes, cudaMemcpyHostToDevice, C.st);
+    });
+  }
   for (int k = 0; k < n; ++k) {
     const int d = ids[k];
     const gqm_cdt_in &D = in[d];
@@ -1068,7 +1078,6 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
   std::vector<int> order(n);
   for (int k = 0; k < n; ++k) order[k] = k;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return jobs[a].np > jobs[b].np; });
-  cudaMemcpyAsync(C.d_in, C.h_in, in_bytes, cudaMemcpyHostToDevice, C.st);
   cudaMemcpyAsync(C.d_jobs, jobs.data(), sizeof(Job) * n, cudaMemcpyHostToDevice, C.st);
   cudaMemcpyAsync(C.d_order, order.data(), sizeof(int) * n, cudaMemcpyHostToDevice, C.st);
   cudaMemsetAsync(C.d_next, 0, sizeof(int), C.st);
@@ -1095,10 +1104,24 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
   unsigned long long used = 0;
   cudaMemcpy(jobs.data(), C.d_jobs, sizeof(Job) * n, cudaMemcpyDeviceToHost);
   cudaMemcpy(&used, C.d_used, sizeof(used), cudaMemcpyDeviceToHost);
+  // a large output region is downloaded straight into a pinned block that the
+  // domains' results share (released by the last gqm_free_result); a smaller
+  // one through the staging buffer into malloc()ed arrays
+  char *blk = nullptr;
   if (keep_outputs) {
-    if (grow_host(&C.h_out, &C.h_out_cap, (size_t)used)) return GQM_ERR_MEMORY;
-    if (used && cudaMemcpy(C.h_out, C.d_out, (size_t)used, cudaMemcpyDeviceToHost) != cudaSuccess)
-      return GQM_ERR_CUDA;
+    int nres = 0;
+    for (int k = 0; k < n; ++k) nres += jobs[k].status == GQM_OK;
+    blk = gqm_pinned_take((size_t)used, nres);
+    if (blk) {
+      if (cudaMemcpy(blk, C.d_out, (size_t)used, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        for (int k = 0; k < nres; ++k) gqm_pinned_give(blk);
+        return GQM_ERR_CUDA;
+      }
+    } else {
+      if (grow_host(&C.h_out, &C.h_out_cap, (size_t)used)) return GQM_ERR_MEMORY;
+      if (used && cudaMemcpy(C.h_out, C.d_out, (size_t)used, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return GQM_ERR_CUDA;
+    }
   }
   int alloc_fail = 0;
   for (int k = 0; k < n; ++k) {
@@ -1126,6 +1149,17 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
     R.numberofpoints = J.out_np;
     R.numberoftriangles = J.out_nt;
     R.numberofsegments = J.out_ns;
+    if (blk) {
+      const OutLayout L = out_layout(J.out_np, J.out_nt, J.out_ns);
+      char *o = blk + J.ooff;
+      R.pointlist = reinterpret_cast<double *>(o + L.pts);
+      R.trianglelist = reinterpret_cast<int *>(o + L.tri);
+      R.neighborlist = reinterpret_cast<int *>(o + L.nbr);
+      R.segmentlist = reinterpret_cast<int *>(o + L.seg);
+      R.pstatus = reinterpret_cast<unsigned char *>(o + L.ps);
+      R.tstatus = reinterpret_cast<unsigned char *>(o + L.ts);
+      continue;
+    }
     R.pointlist = (double *)malloc(16ull * J.out_np + 16);
     R.trianglelist = (int *)malloc(12ull * J.out_nt + 16);
     R.neighborlist = (int *)malloc(12ull * J.out_nt + 16);
@@ -1136,7 +1170,7 @@ int run_batch(DevCache &C, const std::vector<int> &ids, const gqm_cdt_in *in, gq
       alloc_fail = 1;
   }
   if (alloc_fail) return GQM_ERR_MEMORY;  // the caller releases every out[]
-  if (keep_outputs)
+  if (keep_outputs && !blk)
     parallel_for(n, [&](int k) {
       const Job &J = jobs[k];
       if (J.status != GQM_OK) return;

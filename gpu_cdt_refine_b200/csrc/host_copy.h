@@ -11,6 +11,14 @@
 #include <thread>
 #include <vector>
 
+// Pinned result blocks shared with the batch engine (csrc/refine.cu): a block
+// of at least `bytes` held by `refs` results (nullptr below the pool's minimum
+// size or when the pool is full), and the release of one holder's share by
+// any address inside the block.  (Global names: the batch engine's unit
+// renames the gqm namespace.)
+char *gqm_pinned_take(size_t bytes, int refs);
+bool gqm_pinned_give(const void *p);
+
 struct HostCopy {
   void *dst;
   const void *src;
@@ -41,11 +49,11 @@ static inline void host_copy(std::initializer_list<HostCopy> list) {
 // thread) for every range [offset, offset + bytes) of the destination whose
 // copy is complete, in order, at least `step` bytes at a time, so that the
 // caller can start its upload of the front while the back is still being
-// copied.  The list's destinations must follow one another from dst_base on;
+// copied.  The list's destinations must follow one another from dst_base on,
+// in ascending order (gaps between them are handed on with their neighbours);
 // the pieces are taken in order by the worker threads and the calling thread.
-template <class Ready>
-static inline void host_copy_streamed(std::initializer_list<HostCopy> list, char *dst_base, size_t step,
-                                      Ready ready) {
+template <class List, class Ready>
+static inline void host_copy_streamed(const List &list, char *dst_base, size_t step, Ready ready) {
   constexpr size_t kPiece = 4u << 20;
   std::vector<HostCopy> pieces;
   for (const HostCopy &c : list)

@@ -2265,4 +2265,151 @@ GQM_KERNEL void k_collect(Mesh M, const int *bad, const int *dn, const double2 *
   }
 }
 
+// ---------------------------------------------------------------------------
+// Exploration runs for descendant-count labels (gqm_learn_explore).  Every
+// bad triangle's candidate gets one row; the candidate inserts its point at
+// t = j / (levels - 1) of the way from the off-center to the circumcenter, j
+// drawn from a seeded hash of the triangle's vertices.  Lineage: every vertex
+// inserted during the run carries the row of the candidate it descends from
+// (vrow); a candidate's parent is the youngest such row among its bad
+// triangle's vertices (the vertex whose insertion, directly or through the
+// flips that followed it, made the triangle), and a midpoint descends from the
+// youngest row among the vertices of the two triangles on its subsegment (the
+// encroaching vertex is the apex of one of them).
+// ---------------------------------------------------------------------------
+struct ExploreDev {
+  float *feat;     // [cap][kFeat]
+  int *level;      // level j drawn (-1: off-center and circumcenter coincide)
+  float *tused;    // t of the inserted point (0 when the drawn point would encroach)
+  int *parent;     // parent row or -1
+  uint8_t *ins;    // 1 once the candidate's point is in the mesh
+  int *mids;       // midpoints that descend from the row directly
+  unsigned long long *cnt;
+  unsigned long long cap;
+  int *vrow;       // per vertex slot: row it descends from (-1: input vertex)
+  int *crow;       // per bad-list position: the candidate's row (-1: beyond cap)
+  int *mlin;       // per midpoint position: its lineage, between the two kernels around k_insert_mid
+  int levels;
+  unsigned seed;
+  // exploration around a network: with probability 1 - eps (per triangle,
+  // from the same hash) the candidate takes the network's t (level -2)
+  MlpDev net;
+  int use_net;
+  float eps;
+};
+
+// murmur3's 32-bit finaliser over the seed and the sorted vertex ids
+__device__ __forceinline__ unsigned explore_mix(unsigned h) {
+  h ^= h >> 16;
+  h *= 0x85ebca6bu;
+  h ^= h >> 13;
+  h *= 0xc2b2ae35u;
+  h ^= h >> 16;
+  return h;
+}
+__device__ __forceinline__ unsigned explore_draw(unsigned seed, int a, int b, int c) {
+  int lo = min(a, min(b, c)), hi = max(a, max(b, c)), mid = a + b + c - lo - hi;
+  unsigned h = explore_mix(seed ^ 0x9e3779b9u);
+  h = explore_mix(h ^ (unsigned)lo);
+  h = explore_mix(h ^ (unsigned)mid);
+  return explore_mix(h ^ (unsigned)hi);
+}
+__device__ __forceinline__ int explore_youngest(const int *vrow, int4 v) {
+  return max(vrow[v.x], max(vrow[v.y], vrow[v.z]));
+}
+
+// after k_circumcenter: rows of the candidates, the drawn points into center
+GQM_KERNEL void k_explore_place(Mesh M, const int *bad, const int *dn, double2 *center, ExploreDev E) {
+  const int n = *dn;
+  GS_LOOP(k, n) {
+    const int t = bad[k];
+    const int4 v = M.tv[t];
+    const double2 coff = center[k];
+    const double2 cc = circumcenter(M.pts[v.x], M.pts[v.y], M.pts[v.z], 0.0, false);
+    const bool cand = (coff.x != cc.x || coff.y != cc.y);
+    float f[kFeat];
+    for (int q = 0; q < kFeat; ++q) f[q] = 0.0f;
+    if (cand) features_of(M, t, bisector_of(M, t), 0.0, f);
+    int j = -1;
+    float tu = 0.0f;
+    if (cand) {
+      const unsigned h = explore_draw(E.seed, v.x, v.y, v.z);
+      double tj = 0.0;
+      if (E.use_net && (float)(explore_mix(h) >> 8) * (1.0f / 16777216.0f) >= E.eps) {
+        j = -2;
+        const float y = mlp_forward_row(E.net, f);
+        tj = (y > 0.0f && y < 1.0f) ? (double)y : 0.0;
+      } else {
+        j = (int)(h % (unsigned)E.levels);
+        tj = (double)j / (double)(E.levels - 1);
+      }
+      if (tj > 0.0) {
+        const double2 p = make_double2(coff.x + tj * (cc.x - coff.x), coff.y + tj * (cc.y - coff.y));
+        if (!encroaches_near(M, t, p)) {
+          center[k] = p;
+          tu = (float)tj;
+        }
+      }
+    }
+    const unsigned long long row = atomicAdd(E.cnt, 1ull);
+    E.crow[k] = row < E.cap ? (int)row : -1;
+    if (row >= E.cap) continue;
+    for (int q = 0; q < kFeat; ++q) E.feat[row * kFeat + q] = f[q];
+    E.level[row] = j;
+    E.tused[row] = tu;
+    E.parent[row] = explore_youngest(E.vrow, v);
+    E.ins[row] = 0;
+    E.mids[row] = 0;
+  }
+}
+
+// after k_insert_steiner: the inserted points take their candidates' rows
+// (a winner on a subsegment is not inserted and leaves its slot deleted)
+template <class S>
+GQM_KERNEL void k_explore_steiner(Mesh M, const int *wl, const int *dn, const double2 *center, S pslots_,
+                                  ExploreDev E) {
+  const int *pslots = slots_of(pslots_);
+  const int n = *dn;
+  GS_LOOP(pos, n) {
+    const int k = wl[pos];
+    const int newp = pslots[pos];
+    if (M.ps[newp] != (PS_STEINER | PS_NEW)) continue;
+    const double2 p = M.pts[newp], c = center[k];
+    if (p.x != c.x || p.y != c.y) continue;
+    const int row = E.crow[k];
+    E.vrow[newp] = row;
+    if (row >= 0) E.ins[row] = 1;
+  }
+}
+
+// after k_mid_snapshot, before k_insert_mid: each midpoint's lineage
+GQM_KERNEL void k_explore_mid_pre(Mesh M, const int *dn, const int *snap, ExploreDev E) {
+  const int n = *dn;
+  GS_LOOP(pos, n) {
+    const int otri = snap[pos];
+    const int t0 = dtri(otri);
+    int lin = -1;
+    if (t0 >= 0) {
+      lin = explore_youngest(E.vrow, M.tv[t0]);
+      const int on = ld1(M.tn, t0, dori(otri));
+      if (on >= 0) lin = max(lin, explore_youngest(E.vrow, M.tv[dtri(on)]));
+    }
+    E.mlin[pos] = lin;
+  }
+}
+
+// after k_insert_mid: the inserted midpoints take their lineage
+template <class S>
+GQM_KERNEL void k_explore_mid_post(Mesh M, const int *mids, const int *dn, S pslots_, ExploreDev E) {
+  const int *pslots = slots_of(pslots_);
+  const int n = *dn;
+  GS_LOOP(pos, n) {
+    const int newp = pslots[mids[pos]];
+    if (M.ps[newp] != (PS_STEINER | PS_NEW | PS_SEGSPLIT)) continue;
+    const int lin = E.mlin[pos];
+    E.vrow[newp] = lin;
+    if (lin >= 0) atomicAdd(E.mids + lin, 1);
+  }
+}
+
 }  // namespace gqm

@@ -235,6 +235,43 @@ int gqm_mlp_infer(int device, const float *params, const float *features, long l
   return rc;
 }
 
+int gqm_mlp_time(int device, const float *params, long long n, int iters, float *ms) {
+  using namespace gqm;
+  if (!params || !ms || n <= 0 || n > (1LL << 28) || iters <= 0) return GQM_ERR_ARGUMENT;
+  if (cudaSetDevice(device) != cudaSuccess) return GQM_ERR_NO_DEVICE;
+  cudaStream_t st;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return GQM_ERR_CUDA;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  MlpBuf B;
+  float *dX = nullptr, *dY = nullptr;
+  int rc = B.upload(params, st);
+  if (!rc) rc = dmalloc(&dX, (size_t)n * kFeat);
+  if (!rc) rc = dmalloc(&dY, (size_t)n);
+  if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) rc = GQM_ERR_CUDA;
+  if (!rc) {
+    cudaMemsetAsync(dX, 0, sizeof(float) * kFeat * n, st);
+    const long long nw = (n + 31) / 32;
+    const int blocks = (int)std::min<long long>((nw + kWarpsPerBlock - 1) / kWarpsPerBlock, 148 * 16);
+    k_mlp_infer<<<blocks, 32 * kWarpsPerBlock, 0, st>>>(B.dev(), dX, n, dY);
+    cudaEventRecord(e0, st);
+    for (int i = 0; i < iters; ++i) k_mlp_infer<<<blocks, 32 * kWarpsPerBlock, 0, st>>>(B.dev(), dX, n, dY);
+    cudaEventRecord(e1, st);
+    float t = 0.0f;
+    if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess ||
+        cudaEventElapsedTime(&t, e0, e1) != cudaSuccess)
+      rc = GQM_ERR_CUDA;
+    else
+      *ms = t / (float)iters;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (dX) cudaFree(dX);
+  if (dY) cudaFree(dY);
+  B.release();
+  cudaStreamDestroy(st);
+  return rc;
+}
+
 int gqm_mlp_grad(int device, const float *params, const float *features, const float *targets, long long n,
                  float *loss, float *grad) {
   using namespace gqm;

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -60,37 +61,41 @@ namespace gqm {
 
 // ============================================================================
 // Pinned blocks for large results.  A result of gqm_refine /
-// gqm_context_result of at least kPoolMinBytes is downloaded straight into a
-// block of pinned host memory that the caller then owns until
-// gqm_free_result, which gives the block back for the next result: no second
-// copy from a staging buffer and no page faults on fresh memory.  The pool
-// holds at most kPoolMaxBytes; when no block fits and the limit is reached,
-// the result takes the malloc path (staging buffer, then copies).
+// gqm_context_result of at least kPoolMinBytes, and the results of a
+// persistent batch together, are downloaded straight into a block of pinned
+// host memory that the callers then own until gqm_free_result, which gives
+// their share back (a batch's block is shared by its domains and is free again
+// once every domain's result is released): no second copy from a staging
+// buffer and no page faults on fresh memory.  The pool holds at most
+// kPoolMaxBytes; when no block fits and the limit is reached, the result takes
+// the malloc path (staging buffer, then copies).
 // ============================================================================
 constexpr size_t kPoolMinBytes = 16ull << 20;
-constexpr size_t kPoolMaxBytes = 2ull << 30;
+constexpr size_t kPoolMaxBytes = 8ull << 30;
 struct PoolBlock {
   char *p;
   size_t cap;
-  bool in_use;
+  int refs;  // results still holding the block (0: free)
 };
 static std::mutex g_pool_mutex;
 static std::vector<PoolBlock> g_pool;
 static size_t g_pool_bytes = 0;
-// a block of at least `bytes`, or nullptr
-static char *pool_take(size_t bytes) {
-  if (bytes < kPoolMinBytes) return nullptr;
+}  // namespace gqm
+// a block of at least `bytes` held by `refs` results, or nullptr
+char *gqm_pinned_take(size_t bytes, int refs) {
+  using namespace gqm;
+  if (bytes < kPoolMinBytes || refs <= 0) return nullptr;
   std::lock_guard<std::mutex> lock(g_pool_mutex);
   PoolBlock *best = nullptr;
   for (PoolBlock &b : g_pool)
-    if (!b.in_use && b.cap >= bytes && (!best || b.cap < best->cap)) best = &b;
+    if (!b.refs && b.cap >= bytes && (!best || b.cap < best->cap)) best = &b;
   if (best) {
-    best->in_use = true;
+    best->refs = refs;
     return best->p;
   }
   // make room: drop free blocks, which are all too small
   for (size_t k = 0; k < g_pool.size() && g_pool_bytes + bytes > kPoolMaxBytes;) {
-    if (!g_pool[k].in_use) {
+    if (!g_pool[k].refs) {
       cudaFreeHost(g_pool[k].p);
       g_pool_bytes -= g_pool[k].cap;
       g_pool.erase(g_pool.begin() + (long)k);
@@ -104,21 +109,26 @@ static char *pool_take(size_t bytes) {
     cudaGetLastError();
     return nullptr;
   }
-  g_pool.push_back(PoolBlock{p, bytes, true});
+  g_pool.push_back(PoolBlock{p, bytes, refs});
   g_pool_bytes += bytes;
   return p;
 }
-// true when p is a lent pool block (now free again)
-static bool pool_give(const void *p) {
+// true when p lies in a lent pool block (whose count of holders drops by one)
+bool gqm_pinned_give(const void *p) {
+  using namespace gqm;
   if (!p) return false;
+  const char *q = static_cast<const char *>(p);
   std::lock_guard<std::mutex> lock(g_pool_mutex);
   for (PoolBlock &b : g_pool)
-    if (b.p == p && b.in_use) {
-      b.in_use = false;
+    if (b.refs > 0 && q >= b.p && q < b.p + b.cap) {
+      --b.refs;
       return true;
     }
   return false;
 }
+namespace gqm {
+static char *pool_take(size_t bytes) { return gqm_pinned_take(bytes, 1); }
+static bool pool_give(const void *p) { return gqm_pinned_give(p); }
 
 // ============================================================================
 // Ordered stream compaction: out[k] = map(i) for the k-th i in [lo, hi) with
@@ -691,6 +701,12 @@ struct Refiner {
   // training-data collection (gqm_learn_collect): device rows and their count
   float *col_feat = nullptr, *col_tgt = nullptr;
   unsigned long long *col_cnt = nullptr, col_cap = 0;
+  // exploration run for descendant-count labels (gqm_learn_explore): the
+  // rows' device arrays, and per-slot lineage sized with the mesh buffers at
+  // the start of every attempt (a run is host-driven while exploring)
+  bool explore = false;
+  ExploreDev ex{};
+  size_t ex_vrow_n = 0, ex_crow_n = 0, ex_mlin_n = 0;
   double theta = 20.0;
   long long max_rounds = 1000000;
   gqm_stats stats{};
@@ -788,6 +804,10 @@ struct Refiner {
     hkeys = nullptr;
     hvals = s2ti = nullptr;
     h_stage_cap = d_out_cap = segs_cap = hash_cap = 0;
+    for (void *q : {(void *)ex.vrow, (void *)ex.crow, (void *)ex.mlin})
+      if (q) cudaFree(q);
+    ex.vrow = ex.crow = ex.mlin = nullptr;
+    ex_vrow_n = ex_crow_n = ex_mlin_n = 0;
     pphys = tphys = sphys = 0;
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -1226,10 +1246,12 @@ struct Refiner {
         DLAUNCH(k_reset_mid, M, mids, &ds->nmid, smark);
         DLAUNCH(k_mark_mid, M, mids, &ds->nmid, smark);
         DLAUNCH(k_mid_snapshot, M, mids, &ds->nmid, smark, snap);
+        if (explore) DLAUNCH(k_explore_mid_pre, M, &ds->nmid, snap, ex);
         KL(k_bump_epoch, 1, 32)(fc);
         count_launch(1);
         DLAUNCH(k_insert_mid, M, mids, &ds->nmid, smark, snap, pslots(), tslots(), DevInt{&ds->last_subseg},
                 &fc->epoch, dctr + 1);
+        if (explore) DLAUNCH(k_explore_mid_post, M, mids, &ds->nmid, pslots(), ex);
         DLAUNCH(k_update_mid_nbrs, M, mids, &ds->nmid, smark, enclist);
         compact_dev(PNonNeg{smark}, Ident{}, &ds->nenc, mids, &ds->nmid);
         return GQM_OK;
@@ -1253,6 +1275,7 @@ struct Refiner {
     DLAUNCH(k_copy, ilist, bad, dn);
     DLAUNCH(k_circumcenter, M, bad, dn, (double)offconstant, offcenter, center);
     if (col_feat) DLAUNCH(k_collect, M, bad, dn, center, col_feat, col_tgt, col_cnt, col_cap);
+    if (explore) DLAUNCH(k_explore_place, M, bad, dn, center, ex);
     if (placement == GQM_PLACE_LEARNED) {  // two warps of a block take 64 candidates per pass
       KL(k_learned_place, kDevGrid, 64)(M, bad, dn, mlp_dev(mlp_w, mlp_b), center, dctr + 4);
       count_launch(1);
@@ -1279,6 +1302,7 @@ struct Refiner {
     KL(k_bump_epoch, 1, 32)(fc);
     count_launch(1);
     DLAUNCH(k_insert_steiner, M, wl, &ds->nst, sinks, center, pslots(), tslots(), &fc->epoch, dctr + 0);
+    if (explore) DLAUNCH(k_explore_steiner, M, wl, &ds->nst, center, pslots(), ex);
     DLAUNCH(k_update_steiner_nbrs, M, wl, &ds->nst, sinks);
     DSTEP((ConsumeSlots{&ds->nst, 2}));
     rc = flip_flop();
@@ -1288,7 +1312,32 @@ struct Refiner {
   }
 
   // ---- the refinement proper (refine.cu:6830-7024), from the initialised mesh ----
+  // the network's device copy (bf16 weights, fp32 biases)
+  int set_network(const float *params) {
+    if (!mlp_w && (dalloc(&mlp_w, kMlpW) || dalloc(&mlp_b, kMlpB))) return GQM_ERR_MEMORY;
+    std::vector<uint16_t> hw(kMlpW);
+    std::vector<float> hb(kMlpB);
+    mlp_pack(params, hw.data(), hb.data());
+    cudaMemcpyAsync(mlp_w, hw.data(), sizeof(uint16_t) * kMlpW, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(mlp_b, hb.data(), sizeof(float) * kMlpB, cudaMemcpyHostToDevice, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_ERR_CUDA;
+    return GQM_OK;
+  }
+  // lineage arrays sized with this attempt's buffers, rows counted from zero
+  int explore_begin() {
+    if (grow_dev(&ex.vrow, &ex_vrow_n, (size_t)pphys) || grow_dev(&ex.crow, &ex_crow_n, (size_t)tphys) ||
+        grow_dev(&ex.mlin, &ex_mlin_n, (size_t)std::max<long>(sphys, 1)))
+      return GQM_ERR_MEMORY;
+    cudaMemsetAsync(ex.vrow, 0xff, sizeof(int) * (size_t)pphys, st);
+    cudaMemsetAsync(ex.cnt, 0, sizeof(unsigned long long), st);
+    return GQM_OK;
+  }
   int refine_body() {
+    if (explore) {
+      if (capturing) return GQM_ERR_ARGUMENT;  // exploration runs are host-driven
+      int rc = explore_begin();
+      if (rc) return rc;
+    }
     refresh_points();
     refresh_tris();
     DLAUNCH(k_mark_all_encsegs, M, DevInt{&ds->last_subseg});  // last_subseg = the input's subsegments here
@@ -1447,13 +1496,8 @@ struct Refiner {
     pred_mode = opt->predicates ? 1 : 0;
     placement = opt->placement == GQM_PLACE_LEARNED ? GQM_PLACE_LEARNED : GQM_PLACE_PLAIN;
     if (placement == GQM_PLACE_LEARNED) {
-      if (!mlp_w && (dalloc(&mlp_w, kMlpW) || dalloc(&mlp_b, kMlpB))) return GQM_ERR_MEMORY;
-      std::vector<uint16_t> hw(kMlpW);
-      std::vector<float> hb(kMlpB);
-      mlp_pack(opt->mlp, hw.data(), hb.data());
-      cudaMemcpyAsync(mlp_w, hw.data(), sizeof(uint16_t) * kMlpW, cudaMemcpyHostToDevice, st);
-      cudaMemcpyAsync(mlp_b, hb.data(), sizeof(float) * kMlpB, cudaMemcpyHostToDevice, st);
-      if (cudaStreamSynchronize(st) != cudaSuccess) return GQM_ERR_CUDA;
+      int rc = set_network(opt->mlp);
+      if (rc) return rc;
     }
     max_rounds = opt->max_rounds > 0 ? opt->max_rounds : 1000000;
     offcenter = 0;
@@ -1495,11 +1539,12 @@ struct Refiner {
       // and uploaded in pieces of 32 MB, the front while the back is packed
       if (grow_pinned(need)) return GQM_ERR_MEMORY;
       const size_t bp = sizeof(double) * 2 * np, bt = sizeof(int) * 3 * nt, bs = sizeof(int) * 2 * ns;
-      host_copy_streamed({{h_stage, in->pointlist, bp}, {h_stage + bp, in->trianglelist, bt},
-                          {h_stage + bp + bt, in->neighborlist, bt}, {h_stage + bp + 2 * bt, in->segmentlist, bs}},
-                         h_stage, 32u << 20, [&](size_t off, size_t bytes) {
-                           cudaMemcpyAsync(base + off, h_stage + off, bytes, cudaMemcpyHostToDevice, st);
-                         });
+      const HostCopy parts[4] = {{h_stage, in->pointlist, bp}, {h_stage + bp, in->trianglelist, bt},
+                                 {h_stage + bp + bt, in->neighborlist, bt},
+                                 {h_stage + bp + 2 * bt, in->segmentlist, bs}};
+      host_copy_streamed(parts, h_stage, 32u << 20, [&](size_t off, size_t bytes) {
+        cudaMemcpyAsync(base + off, h_stage + off, bytes, cudaMemcpyHostToDevice, st);
+      });
       dpts = p0;
       dtri_in = t0;
       dnbr_in = n0;
@@ -1973,6 +2018,68 @@ int gqm_learn_collect(const gqm_cdt_in *in, const gqm_options *opt, float *featu
   if (r.col_cnt) cudaFree(r.col_cnt);
   r.col_feat = r.col_tgt = nullptr;
   r.col_cnt = nullptr;
+  gqm_context_destroy(ctx);
+  return rc;
+}
+int gqm_learn_explore(const gqm_cdt_in *in, const gqm_options *opt, int levels, unsigned seed, const float *mlp,
+                      float eps, float *features, int *level, float *t_used, int *parent, unsigned char *inserted,
+                      int *midpoints, long long cap, long long *count) {
+  if (!in || !opt || levels < 2 || levels > 64 || cap < 0 || cap > INT_MAX || !(eps >= 0.0f && eps <= 1.0f) ||
+      (cap > 0 && (!features || !level || !t_used || !parent || !inserted || !midpoints)))
+    return GQM_ERR_ARGUMENT;
+  gqm_options o = *opt;
+  o.placement = GQM_PLACE_PLAIN;  // the drawn points replace the off-centers
+  o.mlp = nullptr;
+  int rc = validate(in, &o);
+  if (rc) return rc;
+  gqm_context *ctx = nullptr;
+  rc = gqm_context_create(o.device, &ctx);
+  if (rc) return rc;
+  gqm::Refiner &r = ctx->r;
+  gqm::ExploreDev &E = r.ex;
+  if (mlp && (rc = r.set_network(mlp)) != GQM_OK) {
+    gqm_context_destroy(ctx);
+    return rc;
+  }
+  E.use_net = mlp ? 1 : 0;
+  E.eps = mlp ? eps : 1.0f;
+  if (mlp) E.net = gqm::mlp_dev(r.mlp_w, r.mlp_b);
+  const size_t rows = (size_t)(cap > 0 ? cap : 1);
+  if (r.dalloc(&E.feat, rows * gqm::kFeat) || r.dalloc(&E.level, rows) || r.dalloc(&E.tused, rows) ||
+      r.dalloc(&E.parent, rows) || r.dalloc(&E.ins, rows) || r.dalloc(&E.mids, rows) || r.dalloc(&E.cnt, 1)) {
+    rc = GQM_ERR_MEMORY;
+  } else {
+    E.cap = (unsigned long long)cap;
+    E.levels = levels;
+    E.seed = seed;
+    r.explore = true;
+    r.use_graph = false;
+    gqm_stats st;
+    rc = gqm_context_run(ctx, in, 0, &o, &st);
+    unsigned long long n = 0;
+    if (!rc && cudaMemcpy(&n, E.cnt, sizeof(n), cudaMemcpyDeviceToHost) != cudaSuccess) rc = GQM_ERR_CUDA;
+    if (count) *count = (long long)n;
+    if (!rc && n > (unsigned long long)cap) rc = GQM_ERR_TOO_LARGE;  // lineage would be cut: no rows returned
+    if (!rc && n > 0) {
+      const size_t m = (size_t)n;
+      if (cudaMemcpy(features, E.feat, sizeof(float) * gqm::kFeat * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMemcpy(level, E.level, sizeof(int) * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMemcpy(t_used, E.tused, sizeof(float) * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMemcpy(parent, E.parent, sizeof(int) * m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMemcpy(inserted, E.ins, m, cudaMemcpyDeviceToHost) != cudaSuccess ||
+          cudaMemcpy(midpoints, E.mids, sizeof(int) * m, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = GQM_ERR_CUDA;
+    }
+  }
+  for (void *q : {(void *)E.feat, (void *)E.level, (void *)E.tused, (void *)E.parent, (void *)E.ins, (void *)E.mids,
+                  (void *)E.cnt})
+    if (q) cudaFree(q);
+  E.feat = nullptr;
+  E.level = E.parent = E.mids = nullptr;
+  E.tused = nullptr;
+  E.ins = nullptr;
+  E.cnt = nullptr;
+  r.explore = false;
   gqm_context_destroy(ctx);
   return rc;
 }

@@ -174,6 +174,11 @@ def lib() -> ctypes.CDLL:
         L.gqm_learn_collect.argtypes = [ctypes.POINTER(CdtIn), ctypes.POINTER(Options), fp, fp, ctypes.c_longlong,
                                         ctypes.POINTER(ctypes.c_longlong)]
         L.gqm_learn_collect.restype = ctypes.c_int
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.gqm_learn_explore.argtypes = [ctypes.POINTER(CdtIn), ctypes.POINTER(Options), ctypes.c_int, ctypes.c_uint,
+                                        fp, ctypes.c_float, fp, ip, fp, ip, ctypes.POINTER(ctypes.c_ubyte), ip,
+                                        ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+        L.gqm_learn_explore.restype = ctypes.c_int
         if hasattr(L, "gqm_mlp_infer"):  # absent from the CPU emulation build of the tests
             L.gqm_mlp_infer.argtypes = [ctypes.c_int, fp, fp, ctypes.c_longlong, fp]
             L.gqm_mlp_infer.restype = ctypes.c_int
@@ -182,6 +187,8 @@ def lib() -> ctypes.CDLL:
             L.gqm_mlp_train.argtypes = [ctypes.c_int, fp, fp, fp, ctypes.c_longlong, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_float, ctypes.c_uint, fp]
             L.gqm_mlp_train.restype = ctypes.c_int
+            L.gqm_mlp_time.argtypes = [ctypes.c_int, fp, ctypes.c_longlong, ctypes.c_int, fp]
+            L.gqm_mlp_time.restype = ctypes.c_int
         L.gqm_context_set_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
         L.gqm_context_set_tuning.restype = ctypes.c_int
         L.gqm_context_get_tuning.argtypes = [ctypes.c_void_p, ctypes.POINTER(Tuning)]
@@ -249,12 +256,23 @@ class _Owner:
             pass
 
 
+class _Mem:
+    """numpy's handle on n elements of library memory at addr: the array's
+    base, so the library's memory (its owner) lives as long as the array."""
+
+    __slots__ = ("__array_interface__", "_owner")
+
+    def __init__(self, addr, n, typestr, owner):
+        self.__array_interface__ = {"data": (addr, False), "shape": (n,), "typestr": typestr, "version": 3}
+        self._owner = owner
+
+
 def _view(owner, ptr, n, ctype, dtype):
     if n == 0 or not ptr:
         return np.zeros(0, dtype)
-    buf = (ctype * n).from_address(ctypes.addressof(ptr.contents))
-    buf._owner = owner  # the library's memory lives as long as the array
-    return np.frombuffer(buf, dtype=dtype)
+    # an array interface, not a ctypes array type per length (a few times faster
+    # for the thousands of small arrays of a batch)
+    return np.asarray(_Mem(ctypes.cast(ptr, ctypes.c_void_p).value, n, np.dtype(dtype).str, owner))
 
 
 def _take(out: CdtOut, with_status=False, L=None):
@@ -424,6 +442,77 @@ def learn_collect(cdt: CDT, theta=20.0, insertpolicy=Offcenter, mode=1, device=0
     return feat[:cnt.value].copy(), tgt[:cnt.value].copy()
 
 
+def learn_explore(cdt: CDT, theta=20.0, levels=5, seed=0, insertpolicy=Offcenter, mode=1, device=0, cap=None,
+                  mlp=None, eps=1.0):
+    """Rows of an exploration run (gqm_learn_explore): a dict of per-row arrays
+    features [n, 32], level, t_used, parent, inserted, midpoints.  With a
+    network, a triangle draws a level with probability eps and otherwise takes
+    the network's t (level -2)."""
+    L = lib()
+    net = None
+    if mlp is not None:
+        net = np.ascontiguousarray(mlp, np.float32)
+        if net.shape != (MLP_PARAMS,):
+            raise ValueError("mlp must hold MLP_PARAMS values")
+    keep = []
+    cin = _cdt_in(cdt, keep)
+    opt = make_options(theta, insertpolicy, mode, PRED_REFERENCE, device)
+    cap = int(cap if cap is not None else max(1024, 4 * cdt.numberofpoints))
+    for _ in range(2):
+        feat = np.zeros((cap, MLP_FEATURES), np.float32)
+        level = np.zeros(cap, np.int32)
+        tused = np.zeros(cap, np.float32)
+        parent = np.zeros(cap, np.int32)
+        ins = np.zeros(cap, np.uint8)
+        mids = np.zeros(cap, np.int32)
+        cnt = ctypes.c_longlong(0)
+        ip = ctypes.POINTER(ctypes.c_int)
+        rc = L.gqm_learn_explore(ctypes.byref(cin), ctypes.byref(opt), int(levels), int(seed) & 0xFFFFFFFF,
+                                 _fp(net) if net is not None else None, float(eps), _fp(feat), level.ctypes.data_as(ip), _fp(tused), parent.ctypes.data_as(ip),
+                                 ins.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), mids.ctypes.data_as(ip), cap,
+                                 ctypes.byref(cnt))
+        if rc == -13 and cnt.value > cap:  # GQM_ERR_TOO_LARGE: run again with room for every row
+            cap = int(cnt.value * 1.25) + 1024
+            continue
+        if rc != 0:
+            raise RefineError(rc, "learn_explore: " + L.gqm_status_string(rc).decode())
+        n = cnt.value
+        return {"features": feat[:n].copy(), "level": level[:n].copy(), "t_used": tused[:n].copy(),
+                "parent": parent[:n].copy(), "inserted": ins[:n].copy(), "midpoints": mids[:n].copy()}
+    raise RefineError(-13, "learn_explore: rows outgrew the capacity twice")
+
+
+def descendants(parent, inserted, midpoints, depth=0):
+    """Descendant count of every row of an exploration run: the inserted rows
+    and the midpoints below it in the parent tree, down to `depth` generations
+    (0: all).  Parents precede their children (a parent row is a vertex of an
+    earlier round), so one pass from the last row back sums whole subtrees."""
+    parent = np.asarray(parent, np.int64)
+    own = np.asarray(midpoints, np.float64)
+    ins = np.asarray(inserted, np.float64)
+    n = parent.shape[0]
+    if n and parent.max(initial=-1) >= n:
+        raise ValueError("parent row out of range")
+    has = parent >= 0
+    if np.any(parent[has] >= np.arange(n)[has]):
+        raise ValueError("a parent row must precede its child")
+    if depth <= 0:
+        d = own.copy()
+        for r in range(n - 1, -1, -1):  # children before parents
+            p = parent[r]
+            if p >= 0:
+                d[p] += ins[r] + d[r]
+        return d
+    # a[r]: descendants exactly k generations below r (the row's own midpoints
+    # and inserted children are generation 1)
+    a = own + np.bincount(parent[has], weights=ins[has], minlength=n)
+    total = a.copy()
+    for _ in range(depth - 1):
+        a = np.bincount(parent[has], weights=a[has], minlength=n)
+        total += a
+    return total
+
+
 def mlp_infer(params, features, device=0):
     L = lib()
     p = np.ascontiguousarray(params, np.float32)
@@ -461,6 +550,17 @@ def mlp_train(params, features, targets, epochs=20, batch=256, lr=1e-3, seed=0, 
     if rc != 0:
         raise RefineError(rc, "mlp_train")
     return p, float(loss[0])
+
+
+def mlp_time(params, n, iters=10, device=0):
+    """Device milliseconds of one network inference launch over n rows."""
+    L = lib()
+    p = np.ascontiguousarray(params, np.float32)
+    ms = np.zeros(1, np.float32)
+    rc = L.gqm_mlp_time(int(device), _fp(p), int(n), int(iters), _fp(ms))
+    if rc != 0:
+        raise RefineError(rc, "mlp_time")
+    return float(ms[0])
 
 
 def GPU_Refine_Quality(input: CDT, theta: float, insertpolicy=Offcenter, deletepolicy=Connected, mode=1,

@@ -292,6 +292,29 @@ void gqm_batch_release(int device);
  * is strictly better); points that encroach a subsegment are excluded.  Up to `cap` rows; *count gets the number written. */
 int gqm_learn_collect(const gqm_cdt_in *in, const gqm_options *opt, float *features, float *targets,
                       long long cap, long long *count);
+/* Exploration run for descendant-count labels (opt->placement is ignored).
+ * Every bad triangle the refinement splits gets one row, in the order the
+ * rounds reach them; the candidate's point is placed at
+ * t = j / (levels - 1) of the way from the off-center to the circumcenter,
+ * j drawn per triangle from a hash of `seed` and its vertex ids (the
+ * off-center when that point would encroach a subsegment of the triangle or
+ * its neighbours).  Per row: the triangle's features (GQM_MLP_FEATURES floats,
+ * all zero where off-center and circumcenter coincide), level[] = j (-1 for
+ * those), t_used[] = the t inserted, parent[] = the row that inserted the
+ * youngest vertex of the bad triangle (-1: all its vertices are input
+ * vertices or descend from none), inserted[] = 1 when the point entered the
+ * mesh (a candidate that lost its conflict has 0 and a later row for the same
+ * triangle), midpoints[] = subsegment midpoints whose youngest neighbouring
+ * vertex the row inserted.  The descendants of a row are the rows and
+ * midpoints below it in the parent tree.  With a network `mlp` (GQM_MLP_PARAMS
+ * floats, else NULL), a triangle draws a level only with probability `eps`
+ * (from the same hash) and otherwise takes the network's t as the learned rule
+ * would, with level[] = -2.  *count gets the number of rows; more than `cap`
+ * rows returns GQM_ERR_TOO_LARGE with no rows written (2..64 levels,
+ * 0 <= eps <= 1, cap <= INT_MAX). */
+int gqm_learn_explore(const gqm_cdt_in *in, const gqm_options *opt, int levels, unsigned seed, const float *mlp,
+                      float eps, float *features, int *level, float *t_used, int *parent, unsigned char *inserted,
+                      int *midpoints, long long cap, long long *count);
 /* Network output (the unclamped t) for n feature rows. */
 int gqm_mlp_infer(int device, const float *params, const float *features, long long n, float *out);
 /* Mean squared error of the network on n rows and its gradient with respect
@@ -303,6 +326,11 @@ int gqm_mlp_grad(int device, const float *params, const float *features, const f
  * shuffled with `seed`; *loss gets the last epoch's mean loss. */
 int gqm_mlp_train(int device, float *params, const float *features, const float *targets, long long n,
                   int epochs, int batch, float lr, unsigned seed, float *loss);
+/* Device time of the network alone: the inference kernel over n rows of
+ * zero features (the work does not depend on the values), timed with CUDA
+ * events over `iters` launches after one untimed launch; *ms gets the mean
+ * per launch. */
+int gqm_mlp_time(int device, const float *params, long long n, int iters, float *ms);
 
 const char *gqm_status_string(int status);
 int gqm_version(void);

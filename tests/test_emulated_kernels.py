@@ -183,6 +183,41 @@ def test_emulated_learn_collect(emulated):
     assert np.all((tgt >= 0) & (tgt <= 1)) and np.allclose(tgt * 8, np.round(tgt * 8))
 
 
+def test_emulated_learn_explore(emulated):
+    """Exploration rows: parents precede children, drawn levels give the
+    inserted t (or the off-center), the parent tree accounts for every
+    inserted row and midpoint, and a seed gives the same run twice."""
+    cdt = inputs.plain_small(seed=334, n=3000, nseg=150)
+    r = refine.learn_explore(cdt, 20.0, levels=5, seed=7, cap=64)  # too small a cap: run again with room
+    n = r["level"].shape[0]
+    assert n > 64 and r["features"].shape == (n, refine.MLP_FEATURES)
+    rows = np.arange(n)
+    par = r["parent"]
+    assert np.all((par == -1) | ((par >= 0) & (par < rows)))
+    assert np.all(r["inserted"][par[par >= 0]] == 1)  # only inserted rows have descendants
+    lv, tu = r["level"], r["t_used"]
+    assert np.all((lv >= -1) & (lv < 5))
+    assert np.all((tu == 0) | np.isclose(tu, lv / 4.0))
+    assert np.all(tu[lv <= 0] == 0) and np.any(tu > 0)
+    assert np.all(r["features"][lv < 0] == 0) and np.all(r["features"][lv >= 0, -1] == 1.0)
+    moved = np.unique(lv[(lv > 0)])
+    assert moved.size >= 3  # the draw reaches the levels
+    assert np.all(r["midpoints"][r["inserted"] == 0] == 0)
+    d = refine.descendants(par, r["inserted"], r["midpoints"])
+    roots = (par < 0) & (r["inserted"] == 1)
+    assert d[roots].sum() + roots.sum() == r["inserted"].sum() + r["midpoints"].sum()
+    d1 = refine.descendants(par, r["inserted"], r["midpoints"], depth=1)
+    assert np.all(d1 <= d) and np.all(d1 >= r["midpoints"])
+    r2 = refine.learn_explore(cdt, 20.0, levels=5, seed=7)
+    for k in r:
+        assert np.array_equal(r[k], r2[k]), k
+    # around a network answering t = 0.5: every candidate takes it (eps 0)
+    r3 = refine.learn_explore(cdt, 20.0, levels=5, seed=7, mlp=_const_net(0.5), eps=0.0)
+    cand = np.any(r3["features"] != 0, axis=1)
+    assert np.all(r3["level"][cand] == -2) and np.all(r3["level"][~cand] == -1)
+    assert np.all((r3["t_used"] == 0) | (r3["t_used"] == 0.5)) and np.any(r3["t_used"] == 0.5)
+
+
 def test_emulated_area_bound_matches_oracle(emulated):
     """With an area bound (no counterpart in the reference; Triangle's `a`
     switch) the kernels still agree with the oracle byte for byte."""

@@ -105,3 +105,21 @@ def test_trained_network_against_plain(gpu):
         gains.append((a.numberofpoints - b.numberofpoints) / a.numberofpoints)
     print(f"\nvertex reduction of the learned rule: {[f'{100 * g:.2f}%' for g in gains]}")
     assert all(abs(g) < 0.02 for g in gains)
+
+
+def test_explore_rows_form_a_parent_tree(gpu):
+    """Exploration run on the B200 (rows in the order the device claims
+    them): parents precede children and are inserted rows, the inserted t is
+    the drawn level's or the off-center, and the tree accounts for every
+    inserted row and midpoint."""
+    cdt = inputs.clustered(seed=9200, n=50_000, nseg=2500)
+    r = refine.learn_explore(cdt, 20.0, levels=5, seed=3)
+    par, ins, lv, tu = r["parent"], r["inserted"], r["level"], r["t_used"]
+    n = par.shape[0]
+    assert n > 0 and np.all((par == -1) | ((par >= 0) & (par < np.arange(n))))
+    assert np.all(ins[par[par >= 0]] == 1)
+    assert np.all((tu == 0) | np.isclose(tu, lv / 4.0)) and np.any(tu > 0)
+    assert np.isfinite(r["features"]).all()
+    d = refine.descendants(par, ins, r["midpoints"])
+    roots = (par < 0) & (ins == 1)
+    assert d[roots].sum() + roots.sum() == ins.sum() + r["midpoints"].sum()

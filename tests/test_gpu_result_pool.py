@@ -38,3 +38,29 @@ def test_results_in_reused_blocks_stay_distinct(gpu):
     gc.collect()
     e, _ = refine.refine(small, 20.0, 1, 1)  # a freed block of the larger result fits it
     assert _digests(e) == want_small
+
+
+def test_batch_results_share_one_block(gpu):
+    """A persistent batch whose outputs total 16 MB or more is downloaded into
+    one pinned block shared by its domains: every domain's arrays lie inside
+    it, the block is reused only after the last domain's result is released,
+    and reused, it holds the new results."""
+    doms, thetas = inputs.batch_domains(96, seed=20261231)
+    got, _ = refine.refine_batch_persistent(doms, thetas)
+    assert sum(g.pointlist.nbytes + 2 * g.trianglelist.nbytes for g in got) >= 16 << 20
+    want = [_digests(g) for g in got]
+    addrs = sorted(g.pointlist.ctypes.data for g in got)
+    assert addrs[-1] - addrs[0] < sum(g.pointlist.nbytes + 3 * g.trianglelist.nbytes for g in got) + (1 << 20)
+    keep = got[len(got) // 2]  # one domain still alive: the next batch takes another block
+    lo = addrs[0]
+    del got
+    gc.collect()
+    again, _ = refine.refine_batch_persistent(doms, thetas)
+    assert [_digests(g) for g in again] == want and _digests(keep) == want[len(want) // 2]
+    lo2 = min(g.pointlist.ctypes.data for g in again)
+    assert lo2 != lo
+    del keep, again
+    gc.collect()
+    third, _ = refine.refine_batch_persistent(doms, thetas)  # both blocks free: one is reused
+    assert min(g.pointlist.ctypes.data for g in third) in (lo, lo2)
+    assert [_digests(g) for g in third] == want
