@@ -1758,11 +1758,15 @@ GQM_KERNEL void k_remove_losers(Mesh M, const int *bad, const int *dn, const int
 // edge by edge from the resume point, with the region as it is then.  Nothing a
 // test reads changes during the walk (only claim markers do), so the walk takes
 // the same edges as one that tests each neighbour when it gets to it.
+__device__ __forceinline__ unsigned cavity_hash(int t) { return ((unsigned)t * 2654435761u) >> 26; }
 template <int PRED>
 __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, int badIndex, int *out,
                            int stride) {
   int region[kCavityCap], loop[kCavityCap];  // loop: (triangle << 2) | edge to resume at
   uint8_t inside[kCavityCap];                // per frame: neighbours whose circumcircle holds cc
+  // one bit per hash of the region's triangles: a clear bit proves a triangle
+  // is not in the region without scanning it (a set bit still scans)
+  unsigned long long rbits = 0;
   int rsize = 0, lsize = 0;
   int cur = sink, start = 0;
   for (int guard = 0; guard < 4 * kCavityCap * 3 + 16; ++guard) {
@@ -1770,6 +1774,7 @@ __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, i
     if (start == 0) {  // first visit (a return always resumes past the edge it left by)
       if (rsize == kCavityCap || lsize == kCavityCap) return -1;
       region[rsize++] = cur;
+      rbits |= 1ull << cavity_hash(cur);
       loop[lsize++] = cur << 2;
       atomicMin(M.tmark + cur, badIndex);
       const int4 sg = M.tsg[cur];
@@ -1805,11 +1810,12 @@ __device__ int cavity_walk(const Mesh &M, int sink, int direction, double2 cc, i
       if (!((bits >> i) & 1u)) continue;
       const int t = dtri(comp(nb, i));
       bool seen = false;
-      for (int r = 0; r < rsize; ++r)
-        if (region[r] == t) {
-          seen = true;
-          break;
-        }
+      if ((rbits >> cavity_hash(t)) & 1ull)
+        for (int r = 0; r < rsize; ++r)
+          if (region[r] == t) {
+            seen = true;
+            break;
+          }
       if (seen) continue;
       nIdx = t;
       taken = i;

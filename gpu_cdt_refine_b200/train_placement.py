@@ -16,11 +16,13 @@ Labels:
 * ``descendants`` (default): exploration runs (gqm_learn_explore) insert every
   candidate's point at a level t drawn from {0, 1/4, ..., 1} and record the
   parent tree of the inserted vertices; a row's label is its descendant count
-  (inserted rows and midpoints below it, down to --depth generations).  A
-  regression network learns the expected count from the features with the
-  inserted t in the free feature slot T_SLOT; each candidate's placement target
-  is the level with the smallest predicted count, the off-center unless another
-  level is predicted lower by more than --margin.
+  (inserted rows and midpoints below it, down to --depth generations).
+  Regression networks (--ensemble of them, averaged) learn the expected count
+  from the features with the inserted t in the free feature slot T_SLOT; each
+  candidate's placement target is the level with the smallest predicted count,
+  the off-center unless another level is predicted lower by more than
+  --margin.  With --iterations > 1, later explorations follow the last network
+  except for a fraction --eps of random levels.
 * ``one-step``: plain refinements (gqm_learn_collect) label each candidate
   with the level, of nine, whose new triangles include the fewest below theta.
 
@@ -93,15 +95,21 @@ def with_t(X, t):
     return Z
 
 
-def descendant_targets(X, T, D, epochs, batch, lr, margin, clip, device=0):
-    """Regression network of the descendant count, and the placement target of
-    every row: the level predicted lowest (the off-center unless another level
-    is lower by more than `margin`)."""
+def descendant_targets(X, T, D, epochs, batch, lr, margin, clip, device=0, seed=0, ensemble=4):
+    """Regression networks of the descendant count (`ensemble` of them, from
+    different initialisations and shuffles, their predictions averaged), and
+    the placement target of every row: the level predicted lowest (the
+    off-center unless another level is lower by more than `margin`)."""
     y = np.minimum(D, clip).astype(np.float32)
-    reg, loss = refine.mlp_train(refine.mlp_init(1, float(y.mean())), with_t(X, T), y, epochs=epochs, batch=batch,
-                                 lr=lr, device=device)
     levels = np.arange(LEVELS, dtype=np.float32) / (LEVELS - 1)
-    pred = np.stack([refine.mlp_infer(reg, with_t(X, t), device=device) for t in levels], axis=1)
+    pred, losses = 0.0, []
+    for k in range(ensemble):
+        reg, loss = refine.mlp_train(refine.mlp_init(1 + seed + k, float(y.mean())), with_t(X, T), y, epochs=epochs,
+                                     batch=batch, lr=lr, seed=seed + k, device=device)
+        losses.append(loss)
+        pred = pred + np.stack([refine.mlp_infer(reg, with_t(X, t), device=device) for t in levels], axis=1)
+    pred = pred / ensemble
+    loss = float(np.mean(losses))
     best = pred.argmin(axis=1)
     gain = pred[:, 0] - pred[np.arange(pred.shape[0]), best]
     best = np.where(gain > margin, best, 0)
@@ -112,7 +120,7 @@ def descendant_targets(X, T, D, epochs, batch, lr, margin, clip, device=0):
              "predicted_mean_by_t": {f"{t:.2f}": float(pred[:, j].mean()) for j, t in enumerate(levels)},
              "rows_moved": float((best > 0).mean()),
              "predicted_gain_per_moved_row": float(gain[best > 0].mean()) if np.any(best > 0) else 0.0}
-    return reg, tgt.astype(np.float32), stats
+    return tgt.astype(np.float32), stats
 
 
 def evaluate(params, n, points, theta, device=0):
@@ -138,13 +146,17 @@ def main(argv=None):
     ap.add_argument("--points", type=int, default=200_000)
     ap.add_argument("--theta", type=float, default=20.0)
     ap.add_argument("--rows-per-input", type=int, default=20_000, help="one-step labels: rows kept per input")
-    ap.add_argument("--depth", type=int, default=3, help="descendant labels: generations counted (0: all)")
-    ap.add_argument("--margin", type=float, default=0.05, help="descendant labels: predicted gain to leave t = 0")
+    ap.add_argument("--depth", type=int, default=5, help="descendant labels: generations counted (0: all)")
+    ap.add_argument("--margin", type=float, default=0.0, help="descendant labels: predicted gain to leave t = 0")
     ap.add_argument("--clip", type=float, default=64.0, help="descendant labels: counts clipped for the regression")
     ap.add_argument("--iterations", type=int, default=1,
                     help="descendant labels: rounds of exploration; from the second on, candidates take the last "
                          "network's t except for a fraction --eps that draw a level")
     ap.add_argument("--eps", type=float, default=0.3)
+    ap.add_argument("--train-seed", type=int, default=0,
+                    help="descendant labels: regression k starts from seed train_seed + k, the placement network "
+                         "from train_seed + 10")
+    ap.add_argument("--ensemble", type=int, default=4, help="descendant labels: regression networks averaged")
     ap.add_argument("--epochs", type=int, default=None)
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--lr", type=float, default=1e-3)
@@ -162,17 +174,19 @@ def main(argv=None):
         t1 = time.time()
     else:
         n_in = a.inputs or 128
-        epochs = a.epochs or 8
+        epochs = a.epochs or 20
         net = None
         report["iterations"] = []
         for it in range(a.iterations):
             # a fresh set of inputs per iteration (seeds 1000 + 10000 * it, ...)
             X, Tu, D, info = explore(n_in, a.points, a.theta, a.depth, seed0=1000 + 10000 * it, device=a.device,
                                      mlp=net, eps=a.eps if net is not None else 1.0)
-            reg, T, st = descendant_targets(X, Tu, D, epochs, a.batch, a.lr, a.margin, a.clip, device=a.device)
+            T, st = descendant_targets(X, Tu, D, epochs, a.batch, a.lr, a.margin, a.clip, device=a.device,
+                                       seed=a.train_seed, ensemble=a.ensemble)
             Tenc = np.where(T == 0, -0.25, T).astype(np.float32)
-            net, loss = refine.mlp_train(refine.mlp_init(0, float(Tenc.mean())), with_t(X, 0.0), Tenc,
-                                         epochs=epochs, batch=a.batch, lr=a.lr, device=a.device)
+            ps = a.train_seed + 10
+            net, loss = refine.mlp_train(refine.mlp_init(ps, float(Tenc.mean())), with_t(X, 0.0), Tenc,
+                                         epochs=epochs, batch=a.batch, lr=a.lr, seed=ps, device=a.device)
             st.update(info)
             st["placement_loss"] = loss
             if a.eval:

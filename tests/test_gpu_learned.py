@@ -85,12 +85,11 @@ def test_constant_network_places_and_certifies(gpu):
 
 
 def test_trained_network_against_plain(gpu):
-    """What the trained network (gpu_cdt_refine_b200/data/placement_mlp.npy)
-    gains over the plain off-center rule on held-out inputs: both meshes are
-    certified at theta; the vertex counts are reported.  Measured on the
-    clustered distribution the network was trained on, the learned rule is
-    within a fraction of a percent of the plain rule (it does not reach fewer
-    vertices), which this test pins."""
+    """What the trained network (gpu_cdt_refine_b200/data/placement_mlp.npy,
+    trained on descendant counts of exploration runs) gains over the plain
+    off-center rule on held-out inputs of the clustered distribution it was
+    trained on: both meshes are certified at theta, and the learned rule
+    inserts fewer vertices on every input (measured: 1.2-1.5 % fewer)."""
     import os
     p = np.load(os.path.join(os.path.dirname(refine.__file__), "data", "placement_mlp.npy")).astype(np.float32)
     gains = []
@@ -104,7 +103,7 @@ def test_trained_network_against_plain(gpu):
         assert 0 < st["learned_used"] < st["learned_candidates"]
         gains.append((a.numberofpoints - b.numberofpoints) / a.numberofpoints)
     print(f"\nvertex reduction of the learned rule: {[f'{100 * g:.2f}%' for g in gains]}")
-    assert all(abs(g) < 0.02 for g in gains)
+    assert all(g > 0.005 for g in gains)
 
 
 def test_explore_rows_form_a_parent_tree(gpu):
