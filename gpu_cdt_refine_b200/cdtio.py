@@ -26,6 +26,14 @@ class CDT:
     neighborlist: np.ndarray
     segmentlist: np.ndarray
 
+    @classmethod
+    def wrap(cls, pointlist, trianglelist, neighborlist, segmentlist):
+        """A CDT over arrays that already have the right dtypes and shapes
+        (n x 2 float64, n x 3 int32, n x 3 int32, n x 2 int32): no checks, no copies."""
+        c = cls.__new__(cls)
+        c.pointlist, c.trianglelist, c.neighborlist, c.segmentlist = pointlist, trianglelist, neighborlist, segmentlist
+        return c
+
     def __post_init__(self):
         self.pointlist = np.ascontiguousarray(self.pointlist, dtype=np.float64).reshape(-1, 2)
         self.trianglelist = np.ascontiguousarray(self.trianglelist, dtype=np.int32).reshape(-1, 3)

@@ -2126,7 +2126,8 @@ GQM_KERNEL void k_emit_pstatus(Mesh M, int np, uint8_t *pstat) {
 #endif
 
 // Learned placement over the bad triangles, after k_circumcenter has written
-// the plain centers: two warps per block, 32 candidates per warp and pass.
+// the plain centers: up to kInferWarpsMax warps per block, 32 candidates per
+// warp and pass, the network's weights staged in the block's shared memory.
 // ctr[0] counts candidates, ctr[1] the points the network placed.
 GQM_KERNEL void k_learned_place(Mesh M, const int *bad, const int *dn, MlpDev P, double2 *center,
                                 unsigned long long *ctr) {
@@ -2151,12 +2152,15 @@ GQM_KERNEL void k_learned_place(Mesh M, const int *bad, const int *dn, MlpDev P,
     }
   }
 #else
-  __shared__ MlpInferSmem sm[2];
+  __shared__ MlpInferTiles sm;
+  mlp_stage(P, sm.w);
+  __syncthreads();
   const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31u);
-  if (warp >= 2) return;
-  MlpInferSmem &s = sm[warp];
+  const int nw = min(kInferWarpsMax, (int)(blockDim.x >> 5));
+  if (warp >= nw) return;
+  uint16_t *x = sm.x[warp];
   const int n = *dn;
-  for (int g0 = (GQM_BID * 2 + warp) * 32; g0 < n; g0 += GQM_NB * 2 * 32) {
+  for (int g0 = (GQM_BID * nw + warp) * 32; g0 < n; g0 += GQM_NB * nw * 32) {
     const int k = g0 + lane;
     bool cand = false;
     int t = -1;
@@ -2177,8 +2181,10 @@ GQM_KERNEL void k_learned_place(Mesh M, const int *bad, const int *dn, MlpDev P,
     } else {
       for (int j = 0; j < kFeat; ++j) f[j] = 0.0f;
     }
-    for (int j = 0; j < kFeat; ++j) s.x[lane * kFeat + j] = f2bf(f[j]);
-    const float y = mlp_forward_warp(P, s.x, s.h, s.a1, nullptr);
+    mlp_put_row(x, lane, f);
+    __syncwarp();
+    const float y = mlp_forward_regs(sm.w, x);
+    __syncwarp();
     bool used = false;
     if (cand && y > 0.0f && y < 1.0f) {
       const double2 p = make_double2(coff.x + (double)y * (cc.x - coff.x), coff.y + (double)y * (cc.y - coff.y));

@@ -44,17 +44,41 @@ __device__ __forceinline__ void load_rows(const float *X, const int *idx, long l
   for (int j = 0; j < kFeat; ++j) x[lane * kFeat + j] = f2bf(row >= 0 ? X[(long long)row * kFeat + j] : 0.0f);
 }
 
+// inference as the placement step runs it (weights staged per block,
+// activations in registers), kInferWarpsMax warps per block
 __global__ void k_mlp_infer(MlpDev P, const float *X, long long n, float *out) {
-  __shared__ MlpInferSmem sm[kWarpsPerBlock];
-  const int warp = (int)(threadIdx.x >> 5);
-  MlpInferSmem &s = sm[warp];
+  __shared__ MlpInferTiles sm;
+  mlp_stage(P, sm.w);
+  __syncthreads();
+  const int warp = (int)(threadIdx.x >> 5), lane = (int)(threadIdx.x & 31u);
+  uint16_t *x = sm.x[warp];
   const long long nw = (n + 31) / 32;
-  for (long long gw = (long long)blockIdx.x * kWarpsPerBlock + warp; gw < nw; gw += (long long)gridDim.x * kWarpsPerBlock) {
-    int row;
-    load_rows(X, nullptr, 0, gw * 32, n, s.x, row);
-    const float y = mlp_forward_warp(P, s.x, s.h, s.a1, nullptr);
-    if (row >= 0) out[row] = y;
+  for (long long gw = (long long)blockIdx.x * kInferWarpsMax + warp; gw < nw;
+       gw += (long long)gridDim.x * kInferWarpsMax) {
+    const long long row = gw * 32 + lane;
+    float f[kFeat];
+    if (row < n) {
+      const float4 *xr = reinterpret_cast<const float4 *>(X + row * kFeat);
+      for (int j = 0; j < kFeat / 4; ++j) {
+        const float4 v = xr[j];
+        f[4 * j] = v.x;
+        f[4 * j + 1] = v.y;
+        f[4 * j + 2] = v.z;
+        f[4 * j + 3] = v.w;
+      }
+    } else {
+      for (int j = 0; j < kFeat; ++j) f[j] = 0.0f;
+    }
+    mlp_put_row(x, lane, f);
+    __syncwarp();
+    const float y = mlp_forward_regs(sm.w, x);
+    __syncwarp();
+    if (row < n) out[row] = y;
   }
+}
+static int infer_blocks(long long n) {
+  const long long nw = (n + 31) / 32;
+  return (int)std::max<long long>(1, std::min<long long>((nw + kInferWarpsMax - 1) / kInferWarpsMax, 148 * 8));
 }
 
 // Forward and backward of rows [row0, row0 + nrows) (through idx when not
@@ -222,9 +246,7 @@ int gqm_mlp_infer(int device, const float *params, const float *features, long l
   if (!rc) rc = dmalloc(&dY, (size_t)n);
   if (!rc) {
     cudaMemcpyAsync(dX, features, sizeof(float) * kFeat * n, cudaMemcpyHostToDevice, st);
-    const long long nw = (n + 31) / 32;
-    const int blocks = (int)std::min<long long>((nw + kWarpsPerBlock - 1) / kWarpsPerBlock, 148 * 16);
-    k_mlp_infer<<<blocks, 32 * kWarpsPerBlock, 0, st>>>(B.dev(), dX, n, dY);
+    k_mlp_infer<<<infer_blocks(n), 32 * kInferWarpsMax, 0, st>>>(B.dev(), dX, n, dY);
     cudaMemcpyAsync(out, dY, sizeof(float) * n, cudaMemcpyDeviceToHost, st);
     if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess) rc = GQM_ERR_CUDA;
   }
@@ -250,11 +272,10 @@ int gqm_mlp_time(int device, const float *params, long long n, int iters, float 
   if (!rc && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)) rc = GQM_ERR_CUDA;
   if (!rc) {
     cudaMemsetAsync(dX, 0, sizeof(float) * kFeat * n, st);
-    const long long nw = (n + 31) / 32;
-    const int blocks = (int)std::min<long long>((nw + kWarpsPerBlock - 1) / kWarpsPerBlock, 148 * 16);
-    k_mlp_infer<<<blocks, 32 * kWarpsPerBlock, 0, st>>>(B.dev(), dX, n, dY);
+    const int blocks = infer_blocks(n);
+    k_mlp_infer<<<blocks, 32 * kInferWarpsMax, 0, st>>>(B.dev(), dX, n, dY);
     cudaEventRecord(e0, st);
-    for (int i = 0; i < iters; ++i) k_mlp_infer<<<blocks, 32 * kWarpsPerBlock, 0, st>>>(B.dev(), dX, n, dY);
+    for (int i = 0; i < iters; ++i) k_mlp_infer<<<blocks, 32 * kInferWarpsMax, 0, st>>>(B.dev(), dX, n, dY);
     cudaEventRecord(e1, st);
     float t = 0.0f;
     if (cudaStreamSynchronize(st) != cudaSuccess || cudaGetLastError() != cudaSuccess ||

@@ -166,6 +166,124 @@ struct MlpInferSmem {
 };
 
 // ---------------------------------------------------------------------------
+// Inference with the weights staged in shared memory once per block and the
+// activations kept in registers: the accumulator fragments of two adjacent
+// 8-column tiles of one layer are, after bias, ReLU and bf16 rounding, the A
+// fragment of a 16-column step of the next layer (mma.m16n8k16 layouts, as in
+// warp_gemm above).  Rows of the weight and input tiles are padded by 8 bf16
+// so that the fragment loads of a warp hit 32 distinct banks.  Layers 1 and 2
+// round exactly as mlp_forward_warp; layer 3 sums a lane's 16 columns and then
+// the four lanes of a quad, so its fp32 rounding order differs from the
+// sequential sum there.
+// ---------------------------------------------------------------------------
+constexpr int kW1Stride = kFeat + 8, kW2Stride = kHid + 8, kXStride = kFeat + 8;
+constexpr int kInferWarpsMax = 8;  // warps of a block that run the network
+struct MlpWSmem {
+  uint16_t w1[kHid * kW1Stride];  // [hidden][feature]
+  uint16_t w2[kHid * kW2Stride];  // [hidden][hidden]
+  float b1[kHid], b2[kHid], w3[kHid];
+  float b3;
+};
+struct MlpInferTiles {
+  MlpWSmem w;
+  uint16_t x[kInferWarpsMax][32 * kXStride];  // one tile of 32 input rows per warp
+};
+// all threads of the block; a block barrier must follow before the weights are read
+__device__ inline void mlp_stage(const MlpDev &P, MlpWSmem &W) {
+  for (int i = (int)threadIdx.x; i < kHid * kFeat; i += (int)blockDim.x)
+    W.w1[(i / kFeat) * kW1Stride + i % kFeat] = P.w1[i];
+  for (int i = (int)threadIdx.x; i < kHid * kHid; i += (int)blockDim.x)
+    W.w2[(i / kHid) * kW2Stride + i % kHid] = P.w2[i];
+  for (int i = (int)threadIdx.x; i < kHid; i += (int)blockDim.x) {
+    W.b1[i] = P.b1[i];
+    W.b2[i] = P.b2[i];
+    W.w3[i] = bf2f(P.w3[i]);
+  }
+  if (threadIdx.x == 0) W.b3 = P.b3[0];
+}
+// row r of a warp's input tile (lane r writes its own row)
+__device__ inline void mlp_put_row(uint16_t *x, int r, const float *f) {
+  uint32_t *row = reinterpret_cast<uint32_t *>(x + r * kXStride);
+  for (int j = 0; j < kFeat / 2; ++j) row[j] = (uint32_t)f2bf(f[2 * j]) | ((uint32_t)f2bf(f[2 * j + 1]) << 16);
+}
+#ifndef GQM_HOST_EMU
+__device__ __forceinline__ uint32_t lds32(const uint16_t *p) { return *reinterpret_cast<const uint32_t *>(p); }
+__device__ __forceinline__ void mma_bf16_16816(float *d, const uint32_t *a, uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+__device__ __forceinline__ uint16_t relu_bf(float v) { return f2bf(v > 0.0f ? v : 0.0f); }
+// Network output for the 32 rows of tile x (row r = lane r); called by all 32
+// lanes of a warp.
+__device__ inline float mlp_forward_regs(const MlpWSmem &W, const uint16_t *x) {
+  const int lane = (int)(threadIdx.x & 31u), g = lane >> 2, q = lane & 3;
+  float ys[2][2];  // [16-row block][row g, row g + 8]: the quad's layer-3 sums
+#pragma unroll
+  for (int ib = 0; ib < 2; ++ib) {
+    const uint16_t *xr = x + (ib * 16) * kXStride;
+    float c1[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) c1[j][0] = c1[j][1] = c1[j][2] = c1[j][3] = 0.0f;
+#pragma unroll
+    for (int k0 = 0; k0 < kFeat; k0 += 16) {
+      uint32_t a[4];
+      a[0] = lds32(xr + g * kXStride + k0 + 2 * q);
+      a[1] = lds32(xr + (g + 8) * kXStride + k0 + 2 * q);
+      a[2] = lds32(xr + g * kXStride + k0 + 2 * q + 8);
+      a[3] = lds32(xr + (g + 8) * kXStride + k0 + 2 * q + 8);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint16_t *b = W.w1 + (8 * j + g) * kW1Stride + k0 + 2 * q;
+        mma_bf16_16816(c1[j], a, lds32(b), lds32(b + 8));
+      }
+    }
+    uint32_t a2[4][4];
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk) {
+      const int ca = 16 * kk + 2 * q, cb = ca + 8;
+      const float *u = c1[2 * kk], *v = c1[2 * kk + 1];
+      a2[kk][0] = (uint32_t)relu_bf(u[0] + W.b1[ca]) | ((uint32_t)relu_bf(u[1] + W.b1[ca + 1]) << 16);
+      a2[kk][1] = (uint32_t)relu_bf(u[2] + W.b1[ca]) | ((uint32_t)relu_bf(u[3] + W.b1[ca + 1]) << 16);
+      a2[kk][2] = (uint32_t)relu_bf(v[0] + W.b1[cb]) | ((uint32_t)relu_bf(v[1] + W.b1[cb + 1]) << 16);
+      a2[kk][3] = (uint32_t)relu_bf(v[2] + W.b1[cb]) | ((uint32_t)relu_bf(v[3] + W.b1[cb + 1]) << 16);
+    }
+    float c2[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) c2[j][0] = c2[j][1] = c2[j][2] = c2[j][3] = 0.0f;
+#pragma unroll
+    for (int kk = 0; kk < 4; ++kk)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint16_t *b = W.w2 + (8 * j + g) * kW2Stride + 16 * kk + 2 * q;
+        mma_bf16_16816(c2[j], a2[kk], lds32(b), lds32(b + 8));
+      }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float sum = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int c = 8 * j + 2 * q;
+        sum += bf2f(relu_bf(c2[j][2 * h] + W.b2[c])) * W.w3[c];
+        sum += bf2f(relu_bf(c2[j][2 * h + 1] + W.b2[c + 1])) * W.w3[c + 1];
+      }
+      sum += __shfl_xor_sync(0xffffffffu, sum, 1);
+      sum += __shfl_xor_sync(0xffffffffu, sum, 2);
+      ys[ib][h] = sum;
+    }
+  }
+  // row r = lane: block r / 16, half (r % 16) / 8, held by the quad of lane 4 (r % 8)
+  const int src = 4 * (lane & 7);
+  const float y00 = __shfl_sync(0xffffffffu, ys[0][0], src), y01 = __shfl_sync(0xffffffffu, ys[0][1], src);
+  const float y10 = __shfl_sync(0xffffffffu, ys[1][0], src), y11 = __shfl_sync(0xffffffffu, ys[1][1], src);
+  const bool hi = (lane >> 3) & 1;
+  return W.b3 + ((lane >> 4) ? (hi ? y11 : y10) : (hi ? y01 : y00));
+}
+#endif
+
+// ---------------------------------------------------------------------------
 // Features of a bad triangle (scale free, bounded to [-20, 20]): angles, log
 // edge ratios, the circumcenter's position on the bisector (log and asinh),
 // the neighbours' shapes and apex positions (asinh), subsegment flags and the

@@ -1276,8 +1276,8 @@ struct Refiner {
     DLAUNCH(k_circumcenter, M, bad, dn, (double)offconstant, offcenter, center);
     if (col_feat) DLAUNCH(k_collect, M, bad, dn, center, col_feat, col_tgt, col_cnt, col_cap);
     if (explore) DLAUNCH(k_explore_place, M, bad, dn, center, ex);
-    if (placement == GQM_PLACE_LEARNED) {  // two warps of a block take 64 candidates per pass
-      KL(k_learned_place, kDevGrid, 64)(M, bad, dn, mlp_dev(mlp_w, mlp_b), center, dctr + 4);
+    if (placement == GQM_PLACE_LEARNED) {  // eight warps of a block take 256 candidates per pass
+      KL(k_learned_place, kDevGrid, 32 * kInferWarpsMax)(M, bad, dn, mlp_dev(mlp_w, mlp_b), center, dctr + 4);
       count_launch(1);
     }
     DLAUNCH(k_fill_n, M.tmark, DevInt{&ds->last_triangle}, kMaxInt);

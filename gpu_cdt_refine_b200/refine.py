@@ -36,6 +36,11 @@ class CdtOut(ctypes.Structure):
                 ("tstatus", ctypes.POINTER(ctypes.c_ubyte))]
 
 
+# the same structure with its pointers read as plain addresses (ints)
+class _CdtOutAddr(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_void_p if issubclass(t, ctypes._Pointer) else t) for n, t in CdtOut._fields_]
+
+
 class Options(ctypes.Structure):
     _fields_ = [("theta", ctypes.c_double), ("insert_policy", ctypes.c_int), ("mode", ctypes.c_int),
                 ("predicates", ctypes.c_int), ("device", ctypes.c_int), ("max_rounds", ctypes.c_longlong),
@@ -257,22 +262,26 @@ class _Owner:
 
 
 class _Mem:
-    """numpy's handle on n elements of library memory at addr: the array's
-    base, so the library's memory (its owner) lives as long as the array."""
+    """numpy's handle on library memory at addr: the array's base, so the
+    library's memory (its owner) lives as long as the array."""
 
     __slots__ = ("__array_interface__", "_owner")
 
-    def __init__(self, addr, n, typestr, owner):
-        self.__array_interface__ = {"data": (addr, False), "shape": (n,), "typestr": typestr, "version": 3}
+    def __init__(self, addr, shape, typestr, owner):
+        self.__array_interface__ = {"data": (addr, False), "shape": shape, "typestr": typestr, "version": 3}
         self._owner = owner
 
 
-def _view(owner, ptr, n, ctype, dtype):
-    if n == 0 or not ptr:
-        return np.zeros(0, dtype)
-    # an array interface, not a ctypes array type per length (a few times faster
-    # for the thousands of small arrays of a batch)
-    return np.asarray(_Mem(ctypes.cast(ptr, ctypes.c_void_p).value, n, np.dtype(dtype).str, owner))
+_F64, _I32, _U8 = np.dtype(np.float64).str, np.dtype(np.int32).str, np.dtype(np.uint8).str
+_EMPTY = {_F64: np.float64, _I32: np.int32, _U8: np.uint8}
+
+
+def _view(owner, addr, shape, typestr):
+    # an array interface over the address, not a ctypes array type per length
+    # (several times faster for the thousands of small arrays of a batch)
+    if not addr or shape[0] == 0:
+        return np.zeros(shape, _EMPTY[typestr])
+    return np.asarray(_Mem(addr, shape, typestr, owner))
 
 
 def _take(out: CdtOut, with_status=False, L=None):
@@ -282,14 +291,12 @@ def _take(out: CdtOut, with_status=False, L=None):
     np_, nt_, ns_ = out.numberofpoints, out.numberoftriangles, out.numberofsegments
     if L is not None:
         own = _Owner(L, out)
-        res = CDT(_view(own, out.pointlist, 2 * np_, ctypes.c_double, np.float64),
-                  _view(own, out.trianglelist, 3 * nt_, ctypes.c_int, np.int32),
-                  _view(own, out.neighborlist, 3 * nt_, ctypes.c_int, np.int32),
-                  _view(own, out.segmentlist, 2 * ns_, ctypes.c_int, np.int32))
+        a = _CdtOutAddr.from_buffer(out)
+        res = CDT.wrap(_view(own, a.pointlist, (np_, 2), _F64), _view(own, a.trianglelist, (nt_, 3), _I32),
+                       _view(own, a.neighborlist, (nt_, 3), _I32), _view(own, a.segmentlist, (ns_, 2), _I32))
         if not with_status:
             return res
-        return (res, _view(own, out.pstatus, np_, ctypes.c_ubyte, np.uint8),
-                _view(own, out.tstatus, nt_, ctypes.c_ubyte, np.uint8))
+        return res, _view(own, a.pstatus, (np_,), _U8), _view(own, a.tstatus, (nt_,), _U8)
     res = CDT(np.ctypeslib.as_array(out.pointlist, shape=(2 * np_,)).copy() if np_ else np.zeros(0),
               np.ctypeslib.as_array(out.trianglelist, shape=(3 * nt_,)).copy() if nt_ else np.zeros(0, np.int32),
               np.ctypeslib.as_array(out.neighborlist, shape=(3 * nt_,)).copy() if nt_ else np.zeros(0, np.int32),
@@ -350,8 +357,11 @@ def _batch_args(cdts, thetas, insertpolicy, mode, predicates, device, max_rounds
     if np.isscalar(predicates):
         predicates = [int(predicates)] * n
     ins = (CdtIn * n)(*[_cdt_in(c, keep) for c in cdts])
-    opts = (Options * n)(*[make_options(t, insertpolicy, mode, p, device, max_rounds, mlp, max_area)
-                           for t, p in zip(thetas, predicates)])
+    made = {}  # one Options per distinct (theta, predicates), copied into the array
+    for t, p in zip(thetas, predicates):
+        if (t, p) not in made:
+            made[(t, p)] = make_options(t, insertpolicy, mode, p, device, max_rounds, mlp, max_area)
+    opts = (Options * n)(*[made[(t, p)] for t, p in zip(thetas, predicates)])
     return ins, opts
 
 

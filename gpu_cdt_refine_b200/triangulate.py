@@ -72,9 +72,10 @@ def build_cdt_gpu(points: np.ndarray, segments: np.ndarray, device: int = 0, wit
         raise CdtBuildError(rc)
     own = _Owner(L, res)  # the arrays below view the library's memory and free it when gone
     t, s = res.numberoftriangles, res.numberofsegments
-    cdt = CDT(pts.copy(), refine._view(own, res.trianglelist, 3 * t, ctypes.c_int, np.int32),
-              refine._view(own, res.neighborlist, 3 * t, ctypes.c_int, np.int32),
-              refine._view(own, res.segmentlist, 2 * s, ctypes.c_int, np.int32))
+    addr = lambda p: ctypes.cast(p, ctypes.c_void_p).value  # noqa: E731
+    cdt = CDT(pts.copy(), refine._view(own, addr(res.trianglelist), (t, 3), refine._I32),
+              refine._view(own, addr(res.neighborlist), (t, 3), refine._I32),
+              refine._view(own, addr(res.segmentlist), (s, 2), refine._I32))
     return (cdt, st.as_dict()) if with_stats else cdt
 
 
