@@ -177,7 +177,14 @@ struct MlpInferSmem {
 // sequential sum there.
 // ---------------------------------------------------------------------------
 constexpr int kW1Stride = kFeat + 8, kW2Stride = kHid + 8, kXStride = kFeat + 8;
-constexpr int kInferWarpsMax = 8;  // warps of a block that run the network
+// warps of a block that run the network: eight in the grid-wide placement
+// kernel; four inside the persistent batch kernel, which keeps its shared
+// memory under 32 KB so that the L1 left to its stack is not cut
+#ifdef GQM_CTA_MODE
+constexpr int kInferWarpsMax = 4;
+#else
+constexpr int kInferWarpsMax = 8;
+#endif
 struct MlpWSmem {
   uint16_t w1[kHid * kW1Stride];  // [hidden][feature]
   uint16_t w2[kHid * kW2Stride];  // [hidden][hidden]
