@@ -43,7 +43,7 @@ from . import inputs, refine
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "data", "placement_mlp.npy")
 T_SLOT = 25  # features_of leaves slots 25..30 zero; the regression network reads t here
-LEVELS = 5
+LEVELS = 5  # default number of levels t = 0, 1/(L-1), ..., 1
 
 
 def collect(n_inputs, points, theta, rows_per_input, seed0=1000, device=0):
@@ -64,7 +64,7 @@ def collect(n_inputs, points, theta, rows_per_input, seed0=1000, device=0):
     return np.concatenate(feats), np.concatenate(tgts)
 
 
-def explore(n_inputs, points, theta, depth, seed0=1000, device=0, mlp=None, eps=1.0):
+def explore(n_inputs, points, theta, depth, seed0=1000, device=0, mlp=None, eps=1.0, levels=LEVELS):
     """Exploration rows of n_inputs seeded inputs: (features, t_used, descendant
     count) of every inserted candidate where the learned rule applies, plus
     run totals.  With a network, candidates take its t except for a fraction
@@ -75,7 +75,7 @@ def explore(n_inputs, points, theta, depth, seed0=1000, device=0, mlp=None, eps=
     with ThreadPoolExecutor(max(1, min(8, os.cpu_count() or 1))) as ex:
         futs = [ex.submit(inputs.clustered, seed0 + s, points, points // 20) for s in range(n_inputs)]
         for s, fut in enumerate(futs):
-            r = refine.learn_explore(fut.result(), theta, levels=LEVELS, seed=seed0 + s, device=device, mlp=mlp,
+            r = refine.learn_explore(fut.result(), theta, levels=levels, seed=seed0 + s, device=device, mlp=mlp,
                                      eps=eps)
             d = refine.descendants(r["parent"], r["inserted"], r["midpoints"], depth)
             keep = (r["level"] != -1) & (r["inserted"] == 1)
@@ -95,13 +95,13 @@ def with_t(X, t):
     return Z
 
 
-def descendant_targets(X, T, D, epochs, batch, lr, margin, clip, device=0, seed=0, ensemble=4):
+def descendant_targets(X, T, D, epochs, batch, lr, margin, clip, device=0, seed=0, ensemble=4, nlevels=LEVELS):
     """Regression networks of the descendant count (`ensemble` of them, from
     different initialisations and shuffles, their predictions averaged), and
     the placement target of every row: the level predicted lowest (the
     off-center unless another level is lower by more than `margin`)."""
     y = np.minimum(D, clip).astype(np.float32)
-    levels = np.arange(LEVELS, dtype=np.float32) / (LEVELS - 1)
+    levels = np.arange(nlevels, dtype=np.float32) / (nlevels - 1)
     pred, losses = 0.0, []
     for k in range(ensemble):
         reg, loss = refine.mlp_train(refine.mlp_init(1 + seed + k, float(y.mean())), with_t(X, T), y, epochs=epochs,
@@ -157,6 +157,7 @@ def main(argv=None):
                     help="descendant labels: regression k starts from seed train_seed + k, the placement network "
                          "from train_seed + 10")
     ap.add_argument("--ensemble", type=int, default=4, help="descendant labels: regression networks averaged")
+    ap.add_argument("--levels", type=int, default=LEVELS, help="descendant labels: levels of t explored and chosen")
     ap.add_argument("--epochs", type=int, default=None)
     ap.add_argument("--batch", type=int, default=1024)
     ap.add_argument("--lr", type=float, default=1e-3)
@@ -180,9 +181,9 @@ def main(argv=None):
         for it in range(a.iterations):
             # a fresh set of inputs per iteration (seeds 1000 + 10000 * it, ...)
             X, Tu, D, info = explore(n_in, a.points, a.theta, a.depth, seed0=1000 + 10000 * it, device=a.device,
-                                     mlp=net, eps=a.eps if net is not None else 1.0)
+                                     mlp=net, eps=a.eps if net is not None else 1.0, levels=a.levels)
             T, st = descendant_targets(X, Tu, D, epochs, a.batch, a.lr, a.margin, a.clip, device=a.device,
-                                       seed=a.train_seed, ensemble=a.ensemble)
+                                       seed=a.train_seed, ensemble=a.ensemble, nlevels=a.levels)
             Tenc = np.where(T == 0, -0.25, T).astype(np.float32)
             ps = a.train_seed + 10
             net, loss = refine.mlp_train(refine.mlp_init(ps, float(Tenc.mean())), with_t(X, 0.0), Tenc,
