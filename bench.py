@@ -310,8 +310,8 @@ def run_learned(cdt, args, local_rank):
     path = os.path.join(ROOT, "gpu_cdt_refine_b200", "data", "placement_mlp.npy")
     params = np.load(path).astype(np.float32)
     res = {"network": "gpu_cdt_refine_b200/data/placement_mlp.npy (descendant-count labels: exploration runs of 128 "
-                      "seeded clustered inputs of 200,000 points, theta 20, 5 generations, 4 regression networks "
-                      "averaged)"}
+                      "seeded clustered inputs of 200,000 points, theta 20, 33 levels of t, 5 generations, 4 "
+                      "regression networks averaged)"}
     plain, sp = refine.refine(cdt, 20.0, refine.Offcenter, 1, device=local_rank)
     learned, sl = refine.refine(cdt, 20.0, refine.Offcenter, 1, device=local_rank, mlp=params)
     learned, sl = refine.refine(cdt, 20.0, refine.Offcenter, 1, device=local_rank, mlp=params)

@@ -14,7 +14,7 @@ below 0, where the placement rule falls back to the off-center.
 Labels:
 
 * ``descendants`` (default): exploration runs (gqm_learn_explore) insert every
-  candidate's point at a level t drawn from {0, 1/4, ..., 1} and record the
+  candidate's point at a level t drawn from {0, 1/32, ..., 1} (--levels) and record the
   parent tree of the inserted vertices; a row's label is its descendant count
   (inserted rows and midpoints below it, down to --depth generations).
   Regression networks (--ensemble of them, averaged) learn the expected count
@@ -43,7 +43,7 @@ from . import inputs, refine
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_OUT = os.path.join(HERE, "data", "placement_mlp.npy")
 T_SLOT = 25  # features_of leaves slots 25..30 zero; the regression network reads t here
-LEVELS = 5  # default number of levels t = 0, 1/(L-1), ..., 1
+LEVELS = 33  # default number of levels t = 0, 1/(L-1), ..., 1
 
 
 def collect(n_inputs, points, theta, rows_per_input, seed0=1000, device=0):

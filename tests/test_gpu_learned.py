@@ -89,7 +89,7 @@ def test_trained_network_against_plain(gpu):
     trained on descendant counts of exploration runs) gains over the plain
     off-center rule on held-out inputs of the clustered distribution it was
     trained on: both meshes are certified at theta, and the learned rule
-    inserts fewer vertices on every input (measured: 1.2-1.5 % fewer)."""
+    inserts fewer vertices on every input (measured: 1.8-2.1 % fewer)."""
     import os
     p = np.load(os.path.join(os.path.dirname(refine.__file__), "data", "placement_mlp.npy")).astype(np.float32)
     gains = []
