@@ -65,8 +65,9 @@ typedef struct {
 /* Output CDT.  Arrays are allocated by the library and released with
  * gqm_free_result() (never free() them one by one): a result of 16 MB or more
  * lives in one block of pinned host memory that the library downloads into
- * directly and reuses for a later result once it is released (at most 2 GB of
- * such blocks); a smaller one is malloc()ed.  pstatus / tstatus hold the
+ * directly and reuses for a later result once it is released (the domains of
+ * a persistent batch share one block, free again once every domain's result is
+ * released; at most 8 GB of such blocks); a smaller one is malloc()ed.  pstatus / tstatus hold the
  * reference's PStatus / TStatus bytes of the compacted points / triangles
  * (refine.h:36-205). */
 typedef struct {
