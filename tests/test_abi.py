@@ -3,6 +3,7 @@ import ctypes
 import os
 import re
 
+import numpy as np
 import pytest
 
 from gpu_cdt_refine_b200 import _native
@@ -82,3 +83,39 @@ def test_refine_rejects_invalid_arguments_before_touching_a_device(case):
     """Argument checks run on the host before any CUDA call, so they answer the
     same on a machine without a GPU: GQM_ERR_ARGUMENT, and no output arrays."""
     assert _bad_call(case) == -1
+
+
+@pytest.mark.parametrize("case", ["null_input", "one_level", "many_levels", "eps_negative", "eps_above_one",
+                                  "negative_cap", "null_rows", "theta_zero"])
+def test_learn_explore_rejects_invalid_arguments_before_touching_a_device(case):
+    """gqm_learn_explore checks its arguments and options on the host first."""
+    from gpu_cdt_refine_b200 import inputs, refine
+    L = refine.lib()
+    cdt = inputs.plain_small(seed=12, n=200, nseg=10)
+    keep = []
+    cin = refine._cdt_in(cdt, keep)
+    opt = refine.make_options(0.0 if case == "theta_zero" else 20.0, refine.Offcenter, 1)
+    levels = {"one_level": 1, "many_levels": 65}.get(case, 5)
+    eps = {"eps_negative": -0.1, "eps_above_one": 1.5}.get(case, 1.0)
+    cap = -1 if case == "negative_cap" else 16
+    f = np.zeros((16, refine.MLP_FEATURES), np.float32)
+    i = np.zeros(16, np.int32)
+    t = np.zeros(16, np.float32)
+    u = np.zeros(16, np.uint8)
+    ip = ctypes.POINTER(ctypes.c_int)
+    cnt = ctypes.c_longlong(0)
+    rows = (None,) * 6 if case == "null_rows" else (refine._fp(f), i.ctypes.data_as(ip), refine._fp(t),
+                                                    i.ctypes.data_as(ip), u.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                                                    i.ctypes.data_as(ip))
+    rc = L.gqm_learn_explore(None if case == "null_input" else ctypes.byref(cin), ctypes.byref(opt), levels, 1, None,
+                             eps, *rows, cap, ctypes.byref(cnt))
+    assert rc == -1
+
+
+@pytest.mark.parametrize("n,iters,null", [(0, 5, False), (100, 0, False), (100, 5, True)])
+def test_mlp_time_rejects_invalid_arguments_before_touching_a_device(n, iters, null):
+    from gpu_cdt_refine_b200 import refine
+    L = refine.lib()
+    p = np.zeros(refine.MLP_PARAMS, np.float32)
+    ms = np.zeros(1, np.float32)
+    assert L.gqm_mlp_time(0, None if null else refine._fp(p), n, iters, refine._fp(ms)) == -1
