@@ -33,7 +33,6 @@ no data-path collective), timed as the slowest rank's engine call.
 from __future__ import annotations
 
 import argparse
-import ctypes
 import json
 import os
 import subprocess
